@@ -1,0 +1,414 @@
+"""MPMSolver: drop-in for the reference simulator's hot path.
+
+Keeps the method names and semantics of mpm_exps/engine/mpm_solver.py
+(MPMSolver, :17-1912) that the experiment drivers call: initialize,
+add_cube, substep, run_forward_only, compute_loss / loss, set_bits_and_ranges,
+reshape_params, detect_bound / get_limits, fetch_data_np / push_data_np.
+The substep itself runs in libaq.so (sm_100a kernels behind include/aq.h);
+this module only builds the record layout and moves buffers.  PyTorch is used
+for device buffers and the current stream.
+"""
+import ctypes as C
+
+import numpy as np
+
+from . import _lib
+from . import quant as Q
+
+FIELD_NAMES = ("x", "v", "C", "F", "J")
+
+
+class _Loss:
+    """Stand-in for the reference's `loss` field: loss[None]."""
+
+    def __init__(self):
+        self.value = 0.0
+
+    def __getitem__(self, k):
+        return self.value
+
+    def __setitem__(self, k, v):
+        self.value = float(v)
+
+
+def lame(E, nu, softer=False):
+    mu = E / (2 * (1 + nu))
+    la = E * nu / ((1 + nu) * (1 - 2 * nu))
+    if softer:
+        mu, la = mu * 0.3, la * 0.3
+    return mu, la
+
+
+class MPMSolver:
+    def __init__(self, mpm_param):
+        self.param = p = mpm_param
+        self.dim = p.dim
+        self.n_timestep = int(p.n_timesteps)
+        self.n_particles, self.n_grid = int(p.n_particles), p.n_grid
+        self.dx = 1 / self.n_grid
+        self.inv_dx = 1.0 / self.dx
+        self.p_rho, self.p_vol = p.p_rho, p.p_vol
+        self.p_mass = self.p_vol * self.p_rho
+        self.la = p.la
+        self.E, self.nu = p.E, p.nu
+        self.mu_0, self.la_0 = lame(self.E, self.nu, p.softer)
+        self.dt, self.steps, self.g = p.dt, p.steps, p.g
+        self.use_fluid = p.use_fluid
+        self.use_quantaichi = p.use_quantaichi
+        self.use_difftaichi = p.use_difftaichi
+        self.use_bitpack = p.use_bitpack
+        self.use_dithering = p.use_dithering
+        self.use_bound_clip = p.use_bound_clip
+        self.use_friction = p.use_friction
+        self.size = p.size
+        self.bound = list(p.bound) if p.bound is not None else [3] * self.dim
+        self.offset = [0] * self.dim
+        # mpm_solver.py:97-105
+        self.lb = [b + o for b, o in zip(self.bound, self.offset)]
+        self.ub = [self.n_grid * self.size - b for b in self.bound]
+        if p.ub is not None:
+            self.ub = list(p.ub)
+        if p.lb is not None:
+            self.lb = list(p.lb)
+        if p.quant_bits is not None:
+            self.bits = self.reshape_params(p.quant_bits)
+            self.ranges = self.reshape_params(p.quant_ranges)
+        self.loss = _Loss()
+        self.current_idx = 0
+        self._host = None  # staged particle values (n x n_slots, float64)
+        self._sim = None
+        self._dirty = True
+        self._layout = None
+        self.materials = p.materials
+        self.initialize()
+
+    # ------------------------------------------------------------ layout
+
+    @property
+    def has_F(self):
+        return not self.use_fluid
+
+    @property
+    def has_mat(self):
+        return bool(self.materials)
+
+    def n_slots(self):
+        d = self.dim
+        return 2 * d + d * d + (d * d if self.has_F else 1) + (1 if self.has_mat else 0)
+
+    def slot_range(self, name):
+        d = self.dim
+        return {"x": (0, d), "v": (d, 2 * d), "C": (2 * d, 2 * d + d * d),
+                "F": (2 * d + d * d, 2 * d + 2 * d * d), "J": (2 * d + d * d, 2 * d + d * d + 1),
+                "mat": (self.n_slots() - 1, self.n_slots())}[name]
+
+    def record(self):
+        """The particle record as a BitPack, in the reference's place order
+        x, v, C, F|J (init_quantaichi, mpm_solver.py:364-455)."""
+        p, d = self.param, self.dim
+        rec = Q.BitPack()
+        qp = p.quantized_properties or {}
+        if not self.use_quantaichi:
+            raw = Q.Raw(f64=(p.precision == "f64"))
+            rec.place(*[raw] * (self.n_slots() - (1 if self.has_mat else 0)))
+        else:
+            comp = "f32" if p.compute_fp == "f32" else "f64"
+            bits = [int(b) for b in np.asarray(p.quant_bits).ravel()]
+            rngs = [float(r) for r in np.asarray(p.quant_ranges).ravel()]
+            nfj = d * d if self.has_F else 1
+            if len(bits) != 2 * d + d * d + nfj:
+                raise ValueError("quant_bits must list x, v, C and F|J scalars (%d)" % (2 * d + d * d + nfj))
+
+            def fx(i, offset=0.0):
+                return Q.fixed(bits[i], True, rngs[i], offset, comp, p.use_dithering)
+
+            rec.place(*[fx(i) for i in range(d)])
+            if p.v_exp_bits:
+                rec.place(*[Q.qfloat(bits[d + i], p.v_exp_bits, True) for i in range(d)], shared_exponent=True)
+            else:
+                rec.place(*[fx(d + i) for i in range(d)])
+            if "C" in qp or not qp:
+                rec.place(*[fx(2 * d + i) for i in range(d * d)])
+            else:
+                rec.place(*[Q.Raw(f64=(p.precision == "f64"))] * (d * d))
+            if self.has_F:
+                rec.place(*[fx(2 * d + d * d + i) for i in range(d * d)])
+            else:
+                rec.place(fx(2 * d + d * d, offset=1.0))
+        if self.has_mat:
+            rec.place(Q.qint(max(1, int(np.ceil(np.log2(max(2, len(self.materials)))))), False))
+        return rec
+
+    def layout(self):
+        if self._layout is None:
+            self._layout = self.record().build()
+        return self._layout
+
+    def bytes_per_particle(self):
+        return 8 * self.layout().n_words
+
+    def _params(self):
+        p, d = self.param, self.dim
+        P = _lib.Params()
+        P.dim = d
+        P.precision = 1 if p.precision == "f64" else 0
+        res = p.grid_res if p.grid_res is not None else [int(round(self.n_grid * self.size))] * d
+        for k in range(3):
+            P.res[k] = int(res[k]) if k < d else 1
+            P.lb[k] = float(self.lb[k]) if k < d else 0.0
+            P.ub[k] = float(self.ub[k]) if k < d else 0.0
+        P.has_F = int(self.has_F)
+        P.has_mat = int(self.has_mat)
+        if self.has_mat:
+            P.n_materials = len(self.materials)
+            for i, (kind, E, nu, la) in enumerate(self.materials):
+                mu, lam = lame(E, nu, p.softer)
+                P.mat[i].kind = kind
+                P.mat[i].mu, P.mat[i].lam = (0.0, la) if kind == _lib.AQ_MAT_FLUID else (mu, lam)
+        else:
+            P.n_materials = 1
+            if self.use_fluid:
+                P.mat[0].kind, P.mat[0].mu, P.mat[0].lam = _lib.AQ_MAT_FLUID, 0.0, self.la
+            else:
+                P.mat[0].kind, P.mat[0].mu, P.mat[0].lam = _lib.AQ_MAT_ELASTIC, self.mu_0, self.la_0
+        P.use_friction = int(self.use_friction)
+        P.use_bound_clip = int(self.use_bound_clip)
+        P.sort_interval = int(p.sort_interval)
+        P.dx, P.dt, P.p_vol, P.p_mass, P.gravity = self.dx, self.dt, self.p_vol, self.p_mass, self.g
+        P.n_particles = self.current_idx
+        P.seed = int(p.seed)
+        return P
+
+    # ----------------------------------------------------- scene set-up
+
+    def initialize(self):
+        """mpm_solver.py:564-576: F = I (or J = 1), C = 0, no particles."""
+        n, d = self.n_particles, self.dim
+        self._host = np.zeros((n, self.n_slots()), dtype=np.float64)
+        a, b = self.slot_range("F" if self.has_F else "J")
+        if self.has_F:
+            self._host[:, a:b] = np.eye(d).ravel()
+        else:
+            self._host[:, a] = 1.0
+        self.current_idx = 0
+        self.loss[None] = 0.0
+        self._drop_sim()
+
+    def _drop_sim(self):
+        if self._sim is not None:
+            _lib.lib().aq_sim_destroy(self._sim)
+            self._sim = None
+        self._dirty = True
+
+    def _pull(self):
+        """Copy the simulator's state back into the host staging array."""
+        if self._sim is not None and not self._dirty:
+            self._host[: self.current_idx] = self.state_values()
+
+    def add_cube(self, low_corner, box_size, num, material=0):
+        """3D: uniform random positions (fill_in_box, :1573-1590); 2D: the
+        deterministic lattice of fill_in_box_2duniform (:1561-1571)."""
+        self._pull()
+        d = self.dim
+        st = self.current_idx
+        if d == 3 or len(low_corner) == 3:
+            rng = np.random.default_rng((int(self.param.seed), st))
+            x = np.asarray(low_corner)[None, :] + rng.random((num, d)) * np.asarray(box_size)[None, :]
+            cnt = num
+        else:
+            n = int(np.sqrt(num))
+            i, j = np.meshgrid(np.arange(n), np.arange(n), indexing="ij")
+            x = np.stack([low_corner[0] + 1.0 / n * j.ravel() * box_size[0],
+                          low_corner[1] + 1.0 / n * i.ravel() * box_size[1]], axis=1)
+            cnt = n * n
+        if st + cnt > self.n_particles:
+            raise ValueError("add_cube: %d particles exceed n_particles=%d" % (st + cnt, self.n_particles))
+        a, b = self.slot_range("x")
+        self._host[st:st + cnt, a:b] = x
+        va, vb = self.slot_range("v")
+        self._host[st:st + cnt, va:vb] = 0.0
+        if self.has_mat:
+            self._host[st:st + cnt, self.slot_range("mat")[0]] = material
+        self.current_idx = st + cnt
+        self._drop_sim()
+
+    def set_particles(self, values):
+        """Set all active particles from an (n x n_slots) array."""
+        v = np.asarray(values, dtype=np.float64)
+        self._host[: v.shape[0]] = v
+        self.current_idx = v.shape[0]
+        self._drop_sim()
+
+    # ------------------------------------------------------------ running
+
+    def _ensure_sim(self):
+        import torch
+
+        if not torch.cuda.is_available():
+            raise RuntimeError("MPMSolver needs a CUDA device (sm_100a); there is no CPU fallback")
+        if self._sim is not None and not self._dirty:
+            return
+        if self._sim is None:
+            sim = C.c_void_p()
+            _lib.check(_lib.lib().aq_sim_create(C.byref(self._params()), C.byref(self.layout()), C.byref(sim)),
+                       "aq_sim_create")
+            self._sim = sim
+        vals = torch.from_numpy(np.ascontiguousarray(self._host[: self.current_idx])).cuda()
+        _lib.check(_lib.lib().aq_sim_set_state(self._sim, C.c_void_p(vals.data_ptr()), 1, _lib.stream_ptr()),
+                   "aq_sim_set_state")
+        torch.cuda.current_stream().synchronize()
+        self._dirty = False
+
+    def substeps(self, n):
+        self._ensure_sim()
+        _lib.check(_lib.lib().aq_sim_substeps(self._sim, int(n), _lib.stream_ptr()), "aq_sim_substeps")
+
+    def substep(self, s=0, t=None):
+        """One substep (mpm_solver.py:624-631)."""
+        self.substeps(1)
+
+    def run_forward_only(self, save_pics=False, save_states=False):
+        """run_forward_only of the drivers: n_timestep-1 substeps, then the loss."""
+        self.substeps(self.n_timestep - 1)
+        self.compute_loss()
+        return self.loss[None]
+
+    def compute_loss(self):
+        self._ensure_sim()
+        out = C.c_double()
+        _lib.check(_lib.lib().aq_sim_loss(self._sim, 0, C.byref(out), _lib.stream_ptr()), "aq_sim_loss")
+        self.loss[None] = out.value
+        return out.value
+
+    # ------------------------------------------------------------- state
+
+    def state_values(self, f64=True):
+        """Decoded state, particle order, (n x n_slots) numpy array."""
+        t = self.state_tensor(f64)
+        return t.cpu().numpy()
+
+    def state_tensor(self, f64=True):
+        import torch
+
+        self._ensure_sim()
+        out = torch.empty((self.current_idx, self.n_slots()), dtype=torch.float64 if f64 else torch.float32,
+                          device="cuda")
+        _lib.check(_lib.lib().aq_sim_get_state(self._sim, C.c_void_p(out.data_ptr()), int(f64), _lib.stream_ptr()),
+                   "aq_sim_get_state")
+        return out
+
+    def words(self):
+        import torch
+
+        self._ensure_sim()
+        out = torch.empty((self.current_idx, self.layout().n_words), dtype=torch.int64, device="cuda")
+        _lib.check(_lib.lib().aq_sim_get_words(self._sim, C.c_void_p(out.data_ptr()), _lib.stream_ptr()),
+                   "aq_sim_get_words")
+        return out.cpu().numpy().view(np.uint64)
+
+    def set_words(self, words):
+        import torch
+
+        self._ensure_sim()
+        w = torch.from_numpy(np.ascontiguousarray(words).view(np.int64)).cuda()
+        _lib.check(_lib.lib().aq_sim_set_words(self._sim, C.c_void_p(w.data_ptr()), _lib.stream_ptr()),
+                   "aq_sim_set_words")
+        torch.cuda.current_stream().synchronize()
+
+    def fetch_data_np(self, name, parts=10):
+        """mpm_solver.py:1782-1830 (x, v: n x dim; C, F: n x dim x dim; J: n)."""
+        a, b = self.slot_range(name)
+        v = self.state_values()[:, a:b]
+        if name in ("C", "F"):
+            return v.reshape(-1, self.dim, self.dim).astype(np.float32)
+        if name == "J":
+            return v[:, 0].astype(np.float32)
+        return v.astype(np.float32)
+
+    def push_data_np(self, name, data):
+        """mpm_solver.py:1832-1867."""
+        self._pull()
+        a, b = self.slot_range(name)
+        self._host[: len(data), a:b] = np.asarray(data, dtype=np.float64).reshape(len(data), b - a)
+        self._dirty = True
+        if self._sim is not None:
+            self._ensure_sim()
+        return data
+
+    def status(self, clear=False):
+        self._ensure_sim()
+        f = C.c_uint32()
+        fb = C.c_int64()
+        _lib.check(_lib.lib().aq_sim_status(self._sim, C.byref(f), C.byref(fb), int(clear), _lib.stream_ptr()),
+                   "aq_sim_status")
+        return f.value, fb.value
+
+    def launches(self):
+        n = C.c_int64()
+        if self._sim is None:
+            return 0
+        _lib.check(_lib.lib().aq_sim_launches(self._sim, C.byref(n)), "aq_sim_launches")
+        return n.value
+
+    # ------------------------------------------------- scheme parameters
+
+    def reshape_params(self, ranges):
+        """mpm_solver.py:522-535: flat x, v, C, J|F list -> per-field arrays."""
+        d, qp = self.dim, self.param.quantized_properties or {"x": 1, "v": 1, "C": 1, ("J" if self.use_fluid else "F"): 1}
+        ranges = np.asarray(ranges)
+        r = []
+        if "x" in qp:
+            r.append(np.array(ranges[:d]))
+        if "v" in qp:
+            r.append(np.array(ranges[d:2 * d]))
+        if "C" in qp:
+            r.append(np.array(ranges[2 * d:2 * d + d * d]))
+        if "J" in qp:
+            r.append(np.array(ranges[-1:]))
+        if "F" in qp:
+            r.append(np.array(ranges[-d * d:]))
+        return r
+
+    def set_bits_and_ranges(self, bits, ranges):
+        """mpm_solver.py:494-520: clamp bits to [1, 32] and rebuild the layout."""
+        bits = [max(min(int(b), 32), 1) for b in bits]
+        self.param.quant_bits = np.array(bits)
+        self.param.quant_ranges = np.asarray(ranges, dtype=np.float64)
+        self.bits = self.reshape_params(bits)
+        self.ranges = self.reshape_params(ranges)
+        self._pull()
+        self._layout = None
+        self._drop_sim()
+
+    # ------------------------------------------------- range detection
+
+    def run_forward_detect_ranges(self, n=None):
+        """Range detection (run_forward_detect_ranges, mpm_solver.py:933-945):
+        running max/min of every scalar after each substep."""
+        self._ensure_sim()
+        _lib.check(_lib.lib().aq_sim_ranges_enable(self._sim, 1, _lib.stream_ptr()), "aq_sim_ranges_enable")
+        self.substeps(self.n_timestep - 1 if n is None else n)
+        _lib.check(_lib.lib().aq_sim_ranges_enable(self._sim, 0, _lib.stream_ptr()), "aq_sim_ranges_enable")
+        self.detect_bound()
+        return self.get_limits()
+
+    def detect_bound(self, s=0):
+        ns = self.n_slots()
+        mx = (C.c_double * ns)()
+        mn = (C.c_double * ns)()
+        _lib.check(_lib.lib().aq_sim_ranges_get(self._sim, mx, mn, _lib.stream_ptr()), "aq_sim_ranges_get")
+        self._rmax, self._rmin = np.array(mx[:]), np.array(mn[:])
+
+    def get_limits(self):
+        """mpm_solver.py:981-992: [2]*dim for x, then max(|max|, |min|) of
+        v, C and J|F."""
+        d = self.dim
+        lim = np.maximum(np.abs(self._rmax), np.abs(self._rmin))
+        end = self.n_slots() - (1 if self.has_mat else 0)
+        return np.hstack([[2.0] * d, lim[d:end]])
+
+    def __del__(self):
+        try:
+            self._drop_sim()
+        except Exception:
+            pass

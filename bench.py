@@ -1,0 +1,392 @@
+"""Benchmark of the quantized MLS-MPM substep on B200.
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
+
+Workload (one "step" = one substep over all particles): the 3D mixed scene,
+128^3 grid, 2,097,152 particles in 4 random boxes (2 fixed-corotated
+elastic, 2 fluid), dt 2e-5, quantized records of 395 bits (7 words, 56 B):
+x 3x21 fixed, v 3x12 digits + shared 6-bit exponent, C 9x16 fixed, F 9x16
+fixed, 2-bit material id; dithering on.  Synthetic seeded input (numpy
+default_rng), no dataset.  Particle records (117 MB) and grids (67 MB) exceed
+the 126 MB L2, so no flush is needed between steps.
+
+Reported: particle-substeps/s of the quantized state (`value`), the same
+scene with FP32 particle state, position error of both against an FP64 GPU
+run, the fused kernel's roofline (CUDA-event time per launch vs. the
+measured HBM copy bandwidth), an end-to-end number through the public API
+with host buffers, and the oracle CPU port as baseline.
+
+--impl reference times the CPU restatement of the reference's substep
+(oracle/, C + OpenMP, all host cores) on a bounded sample of the same scene:
+the reference's Taichi build cannot run here (it needs LLVM >= 10 and
+Python < 3.10), so the oracle port stands in for it.
+
+With torchrun (N>1) each rank runs an independent replica (the path does not
+shard across GPUs without a halo exchange); value = all ranks' particle-
+substeps / max over ranks of the timed region.
+"""
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import threading
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+METRIC = "particle-substeps/s quantized vs FP32 on 1 B200 at stated error; HBM GB/s"
+UNIT = "particle-substeps/s"
+WORKLOAD = "mixed_boxes_3d: 3D MLS-MPM, 128^3 grid, 2,097,152 particles, 4 boxes (2 corotated elastic, 2 fluid), dt 2e-5"
+
+
+def host_cores():
+    try:
+        return len(os.sched_getaffinity(0))
+    except Exception:
+        return os.cpu_count() or 1
+
+
+def measured_peaks():
+    p = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    if os.path.exists(p):
+        with open(p) as f:
+            d = json.load(f)
+        return float(d["hbm_gbs"]), "measured"
+    return 6650.0, "fallback"
+
+
+def ncu_traffic():
+    """DRAM bytes per launch of the fused kernel from the committed ncu summary."""
+    p = os.path.join(ROOT, "profiles", "k_step_mixed_boxes_3d.md")
+    if not os.path.exists(p):
+        return None
+    for line in open(p):
+        if line.startswith("dram_bytes_per_launch_full_size:"):
+            try:
+                return float(line.split(":", 1)[1].strip().split()[0])
+            except ValueError:
+                return None
+    return None
+
+
+class Clocks:
+    """nvidia-smi sampler running during the timed region."""
+
+    Q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,clocks_event_reasons.hw_slowdown,"
+         "clocks_event_reasons.hw_thermal_slowdown,clocks_event_reasons.sw_thermal_slowdown,"
+         "clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, index):
+        self.index = index
+        self.proc = None
+        self.lines = []
+
+    def start(self):
+        try:
+            self.proc = subprocess.Popen(["nvidia-smi", "-i", str(self.index), "--query-gpu=" + self.Q,
+                                          "--format=csv,noheader,nounits", "-lms", "200"],
+                                         stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+            self.t = threading.Thread(target=self._read, daemon=True)
+            self.t.start()
+        except Exception:
+            self.proc = None
+
+    def _read(self):
+        for line in self.proc.stdout:
+            self.lines.append(line.strip())
+
+    def stop(self):
+        if not self.proc:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
+        self.proc.terminate()
+        try:
+            self.proc.wait(5)
+        except Exception:
+            self.proc.kill()
+        sm, smax, reasons = [], [], set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for ln in self.lines:
+            f = [x.strip() for x in ln.split(",")]
+            if len(f) < 9:
+                continue
+            try:
+                sm.append(float(f[1]))
+                smax.append(float(f[2]))
+            except ValueError:
+                continue
+            for nm, v in zip(names, f[5:9]):
+                if v.lower() == "active":
+                    reasons.add(nm)
+        return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": max(smax) if smax else None,
+                "reasons": sorted(reasons), "samples": len(sm)}
+
+
+def dist_init():
+    ws = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    if ws > 1:
+        import datetime
+
+        import torch
+        import torch.distributed as dist
+
+        torch.cuda.set_device(local)
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=300),
+                                device_id=torch.device("cuda", local))
+    return ws, rank, local
+
+
+def barrier(ws):
+    if ws > 1:
+        import torch.distributed as dist
+
+        dist.barrier()
+
+
+def max_over_ranks(x, ws):
+    if ws == 1:
+        return x
+    import torch
+    import torch.distributed as dist
+
+    t = torch.tensor([x], dtype=torch.float64, device="cuda")
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
+def cpu_oracle_rate(cfg, vals, seconds=15.0, stride=16, threads=None):
+    """Oracle port (C + OpenMP) on every `stride`-th particle of the scene:
+    substeps until `seconds` of wall time; particle-substeps/s."""
+    sys.path.insert(0, os.path.join(ROOT, "oracle"))
+    import oracle as O
+    from tests.helpers import oracle_layout_from, oracle_params_from
+    from autoquantizer_b200.mpm_solver import MPMSolver
+
+    sub = vals[::stride]
+    s = MPMSolver(cfg)
+    s.set_particles(sub)
+    L = oracle_layout_from(s.record())
+    P = oracle_params_from(s._params())
+    th = threads or host_cores()
+    o = O.Sim(P, L, threads=th)
+    o.set_state(sub)
+    o.substeps(1)  # warm-up
+    t0 = time.perf_counter()
+    k = 0
+    while True:
+        o.substeps(1)
+        k += 1
+        if time.perf_counter() - t0 > seconds or k >= 1000:
+            break
+    dt = time.perf_counter() - t0
+    del s
+    return sub.shape[0] * k / dt, th, "every %d-th particle of the scene (%d particles) x %d substeps, %.1f s" % (
+        stride, sub.shape[0], k, dt)
+
+
+def run_reference(args, ws, rank):
+    if rank != 0:
+        return
+    from autoquantizer_b200 import scenes
+
+    cfg, vals = scenes.mixed_boxes_3d(seed=0)
+    sys.path.insert(0, os.path.join(ROOT, "oracle"))
+    import oracle as O
+    from tests.helpers import oracle_layout_from, oracle_params_from
+    from autoquantizer_b200 import quant as Q  # noqa: F401
+    from autoquantizer_b200.mpm_solver import MPMSolver
+
+    stride = 16
+    sub = vals[::stride]
+    s = MPMSolver(cfg)  # layout only; no device state is created
+    s.set_particles(sub)
+    L = oracle_layout_from(s.record())
+    P = oracle_params_from(s._params())
+    th = host_cores()
+    o = O.Sim(P, L, threads=th)
+    o.set_state(sub)
+    for _ in range(args.warmup):
+        o.substeps(1)
+    t0 = time.perf_counter()
+    o.substeps(args.steps)
+    dt = time.perf_counter() - t0
+    v = sub.shape[0] * args.steps / dt
+    sample = "every %d-th particle of the scene (%d particles), one substep per step" % (stride, sub.shape[0])
+    line = {"impl": "reference", "metric": METRIC, "value": v, "unit": UNIT, "n_gpus": ws, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": 1e3 * dt / args.steps, "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
+            "config": {"workload": WORKLOAD, "sample": sample, "l2": "inputs larger than L2 not applicable (CPU)"},
+            "cpu_baseline": {"value": v, "unit": UNIT, "cores": th, "kind": "port", "sample": sample},
+            "e2e": {"value": v, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+    print(json.dumps(line), flush=True)
+
+
+def run_ours(args, ws, rank, local):
+    import ctypes as C
+
+    import torch
+
+    from autoquantizer_b200 import _lib, scenes
+    from autoquantizer_b200.mpm_solver import MPMSolver
+
+    torch.cuda.set_device(local)
+    cfg, vals = scenes.mixed_boxes_3d(seed=rank)
+    n = vals.shape[0]
+    K, W = args.steps, args.warmup
+    L = _lib.lib()
+
+    def timed(solver, k, prof=False):
+        if prof:
+            _lib.check(L.aq_sim_profile_enable(solver._sim, 1))
+        barrier(ws)
+        torch.cuda.synchronize()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        l0 = solver.launches()
+        e0.record()
+        solver.substeps(k)
+        e1.record()
+        torch.cuda.synchronize()
+        barrier(ws)
+        return e0.elapsed_time(e1), solver.launches() - l0
+
+    # ---- quantized state (the headline)
+    q = MPMSolver(cfg)
+    q.set_particles(vals)
+    q.substeps(W)
+    clocks = Clocks(local)
+    clocks.start()
+    ms, launches = timed(q, K, prof=True)
+    ck = clocks.stop()
+    ms = max_over_ranks(ms, ws)
+    value = ws * n * K / (ms * 1e-3)
+    tot = C.c_double()
+    cnt = C.c_int64()
+    _lib.check(L.aq_sim_profile_get(q._sim, 0, C.byref(tot), C.byref(cnt)))
+    step_ms = tot.value / max(1, cnt.value)
+    _lib.check(L.aq_sim_profile_get(q._sim, 1, C.byref(tot), C.byref(cnt)))
+    grid_ms = tot.value / max(1, cnt.value)
+    _lib.check(L.aq_sim_profile_enable(q._sim, 0))
+    S = q.bytes_per_particle()
+    alg_bytes = 2.0 * S * n  # one read + one write of every record per fused launch
+    peak, peak_kind = measured_peaks()
+    achieved = alg_bytes / (step_ms * 1e-3) / 1e9
+    flags, fallbacks = q.status()
+
+    # ---- FP32 particle state, same scene and code path
+    cfg32, _ = scenes.mixed_boxes_3d(seed=rank, quantized=False)
+    f = MPMSolver(cfg32)
+    f.set_particles(vals)
+    f.substeps(W)
+    ms32, _ = timed(f, K)
+    ms32 = max_over_ranks(ms32, ws)
+    value32 = ws * n * K / (ms32 * 1e-3)
+
+    # ---- FP64 oracle run on the GPU and position errors after W+K substeps
+    cfg64, _ = scenes.mixed_boxes_3d(seed=rank, quantized=False, precision="f64")
+    d = MPMSolver(cfg64)
+    d.set_particles(vals)
+    d.substeps(W + K)
+    x64 = d.state_tensor(True)[:, :3]
+    errs = {}
+    for name, sol in (("quantized", q), ("fp32_state", f)):
+        dx_ = sol.state_tensor(True)[:, :3] - x64
+        errs[name] = {"x_rms": float(dx_.pow(2).sum(1).mean().sqrt()), "x_max": float(dx_.abs().max())}
+    del d, f
+
+    # ---- end to end through the public API with host buffers: per step the
+    # packed records come from pinned host memory, one frame of substeps
+    # runs, the records and the loss go back to the host.
+    frame = args.frame
+    words = q.words()
+    h_in = torch.from_numpy(words.view(np.int64)).pin_memory()
+    h_out = torch.empty_like(h_in).pin_memory()
+    d_words = torch.empty_like(h_in, device="cuda")
+    e2e_steps = max(1, args.e2e_steps)
+
+    def e2e_step():
+        d_words.copy_(h_in, non_blocking=True)
+        _lib.check(L.aq_sim_set_words(q._sim, C.c_void_p(d_words.data_ptr()), _lib.stream_ptr()))
+        q.substeps(frame)
+        _lib.check(L.aq_sim_get_words(q._sim, C.c_void_p(d_words.data_ptr()), _lib.stream_ptr()))
+        h_out.copy_(d_words, non_blocking=True)
+        return q.compute_loss()  # device->host read of the step's result
+
+    e2e_step()
+    barrier(ws)
+    torch.cuda.synchronize()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record()
+    for _ in range(e2e_steps):
+        e2e_step()
+    e1.record()
+    torch.cuda.synchronize()
+    e2e_ms = max_over_ranks(e0.elapsed_time(e1), ws)
+    e2e_val = ws * n * frame * e2e_steps / (e2e_ms * 1e-3)
+
+    # ---- CPU baseline (rank 0, N=1 only)
+    cpu = None
+    if rank == 0 and ws == 1 and not args.no_cpu:
+        v, th, sample = cpu_oracle_rate(cfg, vals, seconds=args.cpu_seconds)
+        cpu = {"value": v, "unit": UNIT, "cores": th, "kind": "port", "sample": sample}
+
+    if rank == 0:
+        line = {
+            "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": ws, "steps": K, "warmup": W,
+            "ms_per_step": ms / K, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+            "dtype": "f32", "data": "synthetic (numpy default_rng seeded scene)",
+            "config": {"workload": WORKLOAD, "record_bits": q.layout().total_bits, "bytes_per_particle": S,
+                       "fp32_bytes_per_particle": 4 * 24, "particles_per_gpu": n, "grid": [128, 128, 128],
+                       "l2": "inputs larger than L2 (117 MB records + 67 MB grids), no flush",
+                       "parallelism": "replicas" if ws > 1 else "single"},
+            "fp32_state": {"value": value32, "unit": UNIT, "ms_per_step": ms32 / K,
+                           "quantized_speedup": value / value32},
+            "compression": 96.0 / S,
+            "error_vs_fp64": {"substeps": W + K, **errs},
+            "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
+                         "frac": achieved / peak, "traffic": ncu_traffic(), "peak_kind": peak_kind,
+                         "kernel": "k_step (fused G2P+P2G)", "avg_launch_ms": step_ms,
+                         "alg_bytes_per_launch": alg_bytes, "k_grid_avg_ms": grid_ms},
+            "cpu_baseline": cpu,
+            "e2e": {"value": e2e_val, "unit": UNIT, "h2d_bytes_per_step": int(h_in.numel() * 8),
+                    "d2h_bytes_per_step": int(h_out.numel() * 8 + 8), "substeps_per_step": frame,
+                    "steps": e2e_steps},
+            "gpu_launches": int(launches),
+            "status": {"flags": flags, "tile_fallbacks": fallbacks},
+            "clocks": ck,
+        }
+        print(json.dumps(line), flush=True)
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=200)
+    ap.add_argument("--warmup", type=int, default=20)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--frame", type=int, default=100)
+    ap.add_argument("--e2e-steps", type=int, default=3)
+    ap.add_argument("--cpu-seconds", type=float, default=15.0)
+    ap.add_argument("--no-cpu", action="store_true")
+    args = ap.parse_args()
+    args.warmup = max(3, args.warmup)
+    ws, rank, local = dist_init()
+    try:
+        if args.impl == "reference":
+            run_reference(args, ws, rank)
+        else:
+            run_ours(args, ws, rank, local)
+    finally:
+        if ws > 1:
+            import torch.distributed as dist
+
+            dist.destroy_process_group()
+
+
+if __name__ == "__main__":
+    main()

@@ -1,0 +1,222 @@
+/*
+ * aq.h - C ABI of libaq.so, the B200 (sm_100a) implementation of the quantized
+ * MLS-MPM substep (P2G -> grid update -> G2P) over bit_pack particle records.
+ *
+ * Conventions
+ *   - Every entry point returns int: 0 = ok, negative = error (see AQ_E_*).
+ *     No entry point aborts the process.
+ *   - Pointers named d_* are CUDA device pointers; h_* are host pointers.
+ *   - `stream` is a cudaStream_t passed as void* (NULL = legacy default
+ *     stream).  Calls are stream-ordered; a handle is not thread-safe.
+ *   - Buffers passed in are caller-owned.  An aq_sim owns its particle
+ *     records, grids and binning scratch and frees them in aq_sim_destroy.
+ *
+ * Each declaration names the reference interface it replaces (path inside the
+ * AutoQuantizer repository, file:line).
+ */
+#ifndef AQ_H_
+#define AQ_H_
+
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define AQ_ABI_VERSION 1
+#define AQ_MAX_SLOTS 32  /* scalars per particle record */
+#define AQ_MAX_GROUPS 4  /* shared-exponent groups per record */
+#define AQ_MAX_MATERIALS 4
+
+/* error codes */
+#define AQ_OK 0
+#define AQ_E_ARG (-1)      /* bad argument (null pointer, size, bit width) */
+#define AQ_E_LAYOUT (-2)   /* layout does not fit the simulator schema */
+#define AQ_E_CUDA (-3)     /* a CUDA runtime call failed */
+#define AQ_E_NOMEM (-4)    /* device allocation failed */
+#define AQ_E_STATE (-5)    /* call not valid in the current state */
+#define AQ_E_LIMIT (-6)    /* size above a documented maximum */
+
+/* device status flags (aq_sim_status) */
+#define AQ_ST_OUT_OF_DOMAIN 0x1u  /* a particle stencil left the grid; base clamped */
+#define AQ_ST_NAN 0x2u            /* a NaN position was met; base clamped */
+#define AQ_ST_FALLBACK 0x4u       /* a particle left its shared-memory tile (informational) */
+
+/* scalar kinds: quantized types of the reference
+ *   AQ_FIXED      ti.quant.fixed(frac=bits, signed, range, offset)
+ *                 (taichi_submission/python/taichi/lang/quant_impl.py:28-50)
+ *   AQ_INT        ti.quant.int(bits, signed)          (quant_impl.py:12-26)
+ *   AQ_FLOAT_EXP  ti.quant.float(exp, frac, signed): own exponent
+ *                 (quant_impl.py:52-73, codegen_llvm_quant.cpp:229-305)
+ *   AQ_SHARED_EXP custom float whose exponent is shared by its group
+ *                 (snode.py place(..., shared_exponent=True), :151-180;
+ *                 codegen_llvm_quant.cpp:347-499)
+ *   AQ_RAW_F32 / AQ_RAW_F64  unquantized IEEE value stored in the record */
+enum {
+  AQ_FIXED = 0,
+  AQ_INT = 1,
+  AQ_FLOAT_EXP = 2,
+  AQ_SHARED_EXP = 3,
+  AQ_RAW_F32 = 4,
+  AQ_RAW_F64 = 5
+};
+
+/* One scalar of a particle record, in place order. */
+typedef struct aq_scalar_spec {
+  int32_t kind;
+  int32_t bits;      /* digits incl. sign bit, 1..32 (RAW: ignored) */
+  int32_t is_signed;
+  int32_t exp_bits;  /* FLOAT_EXP / SHARED_EXP: exponent bits, 1..8 */
+  int32_t group;     /* SHARED_EXP: members with equal id share one exponent */
+  int32_t _pad;
+  double range;      /* FIXED: scale = range/2^(bits-1) (signed) or range/2^bits */
+  double offset;     /* FIXED: value = code*scale + offset */
+} aq_scalar_spec;
+
+/* Resolved slot: bit positions inside the record and derived constants. */
+typedef struct aq_slot {
+  int32_t kind, bits, is_signed, exp_bits;
+  int32_t bit_offset;  /* first bit of the digits (little-endian bit stream) */
+  int32_t exp_offset;  /* first bit of the exponent (FLOAT_EXP, SHARED_EXP) */
+  int32_t group;       /* SHARED_EXP: dense group index */
+  int32_t exp_first;   /* SHARED_EXP: the group exponent precedes this slot */
+  float scale_f32, inv_scale_f32, offset_f32, _pad2;
+  double scale_f64, inv_scale_f64, offset_f64, _pad3;
+} aq_slot;
+
+typedef struct aq_layout {
+  int32_t n_slots, n_words, total_bits, compute_f64, use_dithering, n_groups;
+  int32_t _pad[2];
+  aq_slot slot[AQ_MAX_SLOTS];
+} aq_layout;
+
+/* Build a bit_pack record layout: fields are packed in place order into a
+ * little-endian stream of 64-bit words; a field may straddle two words; a
+ * shared exponent is placed right before the first member of its group.
+ * Replaces the bit_pack layout pass taichi_submission/taichi/struct/
+ * struct_llvm.cpp:77-116 and place_child in
+ * taichi_submission/taichi/program/snode_expr_utils.cpp:30-92. */
+int aq_layout_build(int32_t n_scalars, const aq_scalar_spec* h_specs,
+                    int32_t compute_f64, int32_t use_dithering,
+                    aq_layout* h_out);
+
+/* Encode n records.  d_values is n x n_slots (f32, or f64 if values_f64).
+ * Dithering (layout.use_dithering) draws the uniform of slot s of particle
+ * d_pid[i] (or i when d_pid is NULL) at substep `step` from the counter-based
+ * generator keyed on (seed, step, pid, slot); d_uniforms (n x n_slots, compute
+ * type), when non-NULL, supplies the uniforms instead.
+ * Replaces ti.bit_pack_assign (taichi_submission/python/taichi/lang/
+ * impl.py:753-756) lowered by CodeGenLLVM::visit(BitPackAssignStmt)
+ * (codegen_llvm_quant.cpp:884-952), float_to_custom_int (:44-80),
+ * custom_type_to_bits (:166-184) and rounding_prepare_f{32,64}[_with_dithering]
+ * (taichi_submission/taichi/runtime/llvm/runtime.cpp:1732-1762). */
+int aq_encode(const aq_layout* h_layout, const void* d_values, int32_t values_f64,
+              uint64_t* d_words, int64_t n, const int32_t* d_pid, uint64_t seed,
+              int64_t step, const void* d_uniforms, void* stream);
+
+/* Decode n records into d_values (n x n_slots).
+ * Replaces load_custom_float / load_as_custom_int / load_split /
+ * reconstruct_custom_float[_with_exponent] (codegen_llvm_quant.cpp:529-878). */
+int aq_decode(const aq_layout* h_layout, const uint64_t* d_words, void* d_values,
+              int32_t values_f64, int64_t n, void* stream);
+
+/* ---------------------------------------------------------------- simulator */
+
+enum { AQ_MAT_FLUID = 0, AQ_MAT_ELASTIC = 1, AQ_MAT_COROTATED = 2 };
+
+/* AQ_MAT_FLUID:     cauchy = diag(lam*(J-1))
+ * AQ_MAT_ELASTIC:   the reference's elastic law: 2D fixed-corotated
+ *                   2mu(F-R)F^T + lam J(J-1) I; 3D mu(FF^T-I) + lam log J
+ *                   added to every entry (mpm_solver.py:1012-1031)
+ * AQ_MAT_COROTATED: fixed-corotated in 2D and 3D (3D via a 3x3 polar
+ *                   decomposition); not a reference material */
+typedef struct aq_material {
+  int32_t kind, _pad;
+  double mu, lam;
+} aq_material;
+
+typedef struct aq_params {
+  int32_t dim;         /* 2 or 3 */
+  int32_t precision;   /* 0: f32 grid and arithmetic, 1: f64 */
+  int32_t res[3];      /* grid cells per axis */
+  int32_t has_F;       /* record holds F (dim*dim) after C, else J (1) */
+  int32_t has_mat;     /* record holds a material-id INT slot last */
+  int32_t n_materials;
+  int32_t use_friction, use_bound_clip;
+  int32_t sort_interval; /* re-bin particles every k substeps (>=1) */
+  int32_t _pad;
+  double dx, dt, p_vol, p_mass, gravity;
+  double lb[3], ub[3]; /* grid-index walls, as MPMSolver.lb/ub */
+  aq_material mat[AQ_MAX_MATERIALS];
+  int64_t n_particles;
+  uint64_t seed;
+} aq_params;
+
+typedef struct aq_sim aq_sim;
+
+/* Create a simulator for n_particles records of `layout`.  Record slots must
+ * follow the reference place order x(dim), v(dim), C(dim*dim), F(dim*dim) | J,
+ * [material id] (mpm_solver.py:445-452).
+ * Replaces MPMSolver.__init__ (mpm_exps/engine/mpm_solver.py:19-122) with its
+ * init_quantaichi (:364-455) and init_sparse_grids (:216-253). */
+int aq_sim_create(const aq_params* h_params, const aq_layout* h_layout, aq_sim** out);
+int aq_sim_destroy(aq_sim* sim);
+
+/* Quantize and store all particle values (d_values: n x n_slots, particle
+ * order).  Replaces the per-field initial stores of fill_in_box*
+ * (mpm_solver.py:1561-1597) through store_custom_int (codegen_llvm.cpp:1266-1300). */
+int aq_sim_set_state(aq_sim* sim, const void* d_values, int32_t values_f64, void* stream);
+/* Decode all particle values in particle order.
+ * Replaces fetch_data_np / fetch_*_data (mpm_solver.py:1782-1830). */
+int aq_sim_get_state(aq_sim* sim, void* d_values, int32_t values_f64, void* stream);
+/* Raw packed records in particle order (n x n_words). */
+int aq_sim_set_words(aq_sim* sim, const uint64_t* d_words, void* stream);
+int aq_sim_get_words(aq_sim* sim, uint64_t* d_words, void* stream);
+
+/* Advance n substeps.  Replaces MPMSolver.substep (mpm_solver.py:624-631):
+ * deactivate + build_pid (:578-588) + p2g_bls (:590-622) + grid_op (:633-665)
+ * + g2p_bls (:667-758).  Consecutive substeps are fused: G2P of substep k and
+ * P2G of substep k+1 run in one kernel. */
+int aq_sim_substeps(aq_sim* sim, int32_t n, void* stream);
+
+/* Loss of the current state (written to *h_out, synchronizes the stream).
+ * kind 0: compute_ek (mpm_solver.py:1043-1052): 3D sum 0.5 m|v|^2 + g m x_y,
+ * 2D sum |v|^2. */
+int aq_sim_loss(aq_sim* sim, int32_t kind, double* h_out, void* stream);
+
+/* Per-slot running max/min of the state (range detection), accumulated on
+ * the device after every substep once enabled.
+ * Replaces update_limits_* / get_limits (mpm_solver.py:944-997). */
+int aq_sim_ranges_enable(aq_sim* sim, int32_t on, void* stream);
+int aq_sim_ranges_get(aq_sim* sim, double* h_max, double* h_min, void* stream);
+
+/* Status flags (AQ_ST_*) and tile-fallback counter; synchronizes the
+ * stream.  clear != 0 resets them. */
+int aq_sim_status(aq_sim* sim, uint32_t* h_flags, int64_t* h_fallbacks,
+                  int32_t clear, void* stream);
+int aq_sim_step_count(const aq_sim* sim, int64_t* h_out);
+/* Launch counters of this simulator's own kernels (for accounting). */
+int aq_sim_launches(const aq_sim* sim, int64_t* h_out);
+
+/* Kernel timing with CUDA events recorded around each launch of the fused
+ * substep kernel (k_step) and of the grid kernel (k_grid) on the stream they
+ * run on.  No reference counterpart (the reference profiles through CUPTI,
+ * taichi_submission/taichi/program/kernel_profiler.h:46).  which: 0 = k_step,
+ * 1 = k_grid.  profile_get synchronizes and resets the accumulators. */
+int aq_sim_profile_enable(aq_sim* sim, int32_t on);
+int aq_sim_profile_get(aq_sim* sim, int32_t which, double* h_total_ms, int64_t* h_launches);
+
+/* Per-slot error of a (n x n_slots) against b: h_sq[s] = sum (a-b)^2,
+ * h_max[s] = max |a-b|, accumulated in f64.  Used for the error report
+ * against the f64 oracle run. */
+int aq_state_error(const void* d_a, int32_t a_f64, const void* d_b, int32_t b_f64,
+                   int64_t n, int32_t n_slots, double* h_sq, double* h_max,
+                   void* stream);
+
+const char* aq_error_string(int32_t code);
+int32_t aq_abi_version(void);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* AQ_H_ */
