@@ -28,6 +28,7 @@ EXPORTS = [
     "aq_sim_get_state", "aq_sim_set_words", "aq_sim_get_words", "aq_sim_substeps", "aq_sim_loss",
     "aq_sim_ranges_enable", "aq_sim_ranges_get", "aq_sim_status", "aq_sim_step_count", "aq_sim_launches",
     "aq_state_error", "aq_error_string", "aq_abi_version", "aq_sim_profile_enable", "aq_sim_profile_get",
+    "aq_sim_kernel_is_jit",
 ]
 
 
@@ -57,7 +58,7 @@ class Material(C.Structure):
 class Params(C.Structure):
     _fields_ = [("dim", C.c_int32), ("precision", C.c_int32), ("res", C.c_int32 * 3), ("has_F", C.c_int32),
                 ("has_mat", C.c_int32), ("n_materials", C.c_int32), ("use_friction", C.c_int32),
-                ("use_bound_clip", C.c_int32), ("sort_interval", C.c_int32), ("_pad", C.c_int32),
+                ("use_bound_clip", C.c_int32), ("sort_interval", C.c_int32), ("jit", C.c_int32),
                 ("dx", C.c_double), ("dt", C.c_double), ("p_vol", C.c_double), ("p_mass", C.c_double),
                 ("gravity", C.c_double), ("lb", C.c_double * 3), ("ub", C.c_double * 3),
                 ("mat", Material * AQ_MAX_MATERIALS), ("n_particles", C.c_int64), ("seed", C.c_uint64)]
@@ -99,6 +100,7 @@ def lib():
         "aq_sim_status": ([vp, C.POINTER(C.c_uint32), C.POINTER(C.c_int64), i32, vp], C.c_int),
         "aq_sim_step_count": ([vp, C.POINTER(C.c_int64)], C.c_int),
         "aq_sim_launches": ([vp, C.POINTER(C.c_int64)], C.c_int),
+        "aq_sim_kernel_is_jit": ([vp, C.POINTER(C.c_int32)], C.c_int),
         "aq_state_error": ([vp, i32, vp, i32, i64, i32, C.POINTER(C.c_double), C.POINTER(C.c_double), vp],
                            C.c_int),
         "aq_sim_profile_enable": ([vp, i32], C.c_int),

@@ -44,12 +44,40 @@ def stale():
     return any(os.path.getmtime(f) > t for f in files)
 
 
+# headers compiled again at run time by NVRTC (layout-specialized k_step);
+# the names are the include strings the sources use
+JIT_HEADERS = [("aq_kernels.cuh", os.path.join(CSRC, "aq_kernels.cuh")),
+               ("aq_codec.cuh", os.path.join(CSRC, "aq_codec.cuh")),
+               ("../../include/aq.h", os.path.join(ROOT, "include", "aq.h"))]
+
+
+def write_jit_sources():
+    """Embed the kernel headers into the library as C string literals."""
+    out = ["// generated by autoquantizer_b200/build.py: headers for NVRTC", ""]
+    names, srcs = [], []
+    for i, (name, path) in enumerate(JIT_HEADERS):
+        text = open(path).read()
+        assert ")AQSRC" not in text
+        out.append('static const char kAqJitSrc%d[] = R"AQSRC(%s)AQSRC";' % (i, text))
+        names.append('"%s"' % name)
+        srcs.append("kAqJitSrc%d" % i)
+    out.append("static const int kAqJitHeaderCount = %d;" % len(JIT_HEADERS))
+    out.append("static const char* const kAqJitHeaderName[] = {%s};" % ", ".join(names))
+    out.append("static const char* const kAqJitHeaderSrc[] = {%s};" % ", ".join(srcs))
+    path = os.path.join(OUT, "aq_jit_sources.inc")
+    text = "\n".join(out) + "\n"
+    if not os.path.exists(path) or open(path).read() != text:
+        with open(path, "w") as f:
+            f.write(text)
+
+
 def build(force=False, verbose=False, extra=()):
     if not force and not stale():
         return LIB
     os.makedirs(OUT, exist_ok=True)
+    write_jit_sources()
     flags = [GENCODE, "-O3", "-lineinfo", "-std=c++17", "-Xcompiler", "-fPIC", "--expt-relaxed-constexpr",
-             "-I" + os.path.join(ROOT, "include"), *extra]
+             "-I" + os.path.join(ROOT, "include"), "-I" + OUT, *extra]
     if verbose:
         flags += ["-Xptxas", "-v"]
 
@@ -68,7 +96,7 @@ def build(force=False, verbose=False, extra=()):
             if err:
                 print(err)
     tmp = LIB + ".tmp"
-    cmd = [nvcc(), GENCODE, "-shared", "-o", tmp, *[r[0] for r in results], "-lcudart"]
+    cmd = [nvcc(), GENCODE, "-shared", "-o", tmp, *[r[0] for r in results], "-lcudart", "-ldl"]
     subprocess.check_call(cmd)
     os.replace(tmp, LIB)
     return LIB

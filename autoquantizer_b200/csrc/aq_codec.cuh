@@ -14,8 +14,10 @@
 // that nvcc cannot contract it into an FMA, which would change the codes.
 #pragma once
 
+#ifndef __CUDACC_RTC__
 #include <cuda_runtime.h>
 #include <stdint.h>
+#endif
 
 #include "../../include/aq.h"
 

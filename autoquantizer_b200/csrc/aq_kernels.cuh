@@ -1,0 +1,583 @@
+// Device code of the quantized MLS-MPM substep (sm_100a).
+//
+// This header is compiled twice: by nvcc into libaq.so with the record
+// layout read from the kernel parameter (RtLayout), and at simulator
+// creation by NVRTC with the layout as a constexpr (a JitLayout generated
+// by aq_jit.cu), so that bit offsets, scales and slot kinds fold into the
+// instruction stream the way the reference's per-field LLVM codegen does
+// (codegen_llvm_quant.cpp).
+//
+// Data layout in HBM
+//   records  : n x W u64 bit_pack records, ordered by 4^3 (3D) or 8^2 (2D)
+//              cell block and cells inside a block; each block is cut into
+//              chunks of <= 256 records (the work items) and inside a chunk
+//              records are slot-major: the first record of every cell, then
+//              the second of every cell, ...  The 32 lanes of a warp then
+//              hold particles of 32 different cells.
+//              A particle-id array moves with the records.
+//   grids    : two dense grids of R4 nodes, row-major; one receives P2G
+//              sums (m, m v), the other holds grid_op output (m, v).
+//   binning  : per-cell counts/offsets, per-particle key and rank, and work
+//              items (block, first record, count <= 256).
+//
+// k_step, one CTA of 256 threads per work item (persistent loop):
+//   1. thread t loads record t of the item into shared memory (odd word
+//      stride: conflict-free) and stages the block's grid tile (G2P source);
+//   2. G2P of substep k: gather 3^d nodes, new v, C, x, F|J;
+//      bit_pack_assign into the shared record, which also yields the values
+//      a later decode returns; records written back to HBM;
+//   3. P2G of substep k+1 from those values into a per-warp private tile
+//      of float4 nodes with plain shared-memory adds (lanes that share a
+//      cell take turns, found with __match_any_sync), then the 8 warp tiles
+//      are summed (and re-zeroed) and flushed with one red.global.add.v4.f32
+//      per touched node.
+// Either phase may be off (first / last substep of a run).
+#pragma once
+
+#include "aq_codec.cuh"
+
+#ifdef __CUDACC_RTC__
+#define AQ_POS_INF __int_as_float(0x7f800000)
+#else
+#include <math.h>
+#define AQ_POS_INF INFINITY
+#endif
+
+namespace aq {
+
+constexpr int CH = 256;  // particles per work item = threads per CTA
+constexpr int NWARP = CH / 32;
+
+template <int D>
+struct Geo {
+  static constexpr int BS = D == 3 ? 4 : 8;          // block edge (cells)
+  static constexpr int T = BS + 4;                   // tile edge: one cell of drift each side + stencil
+  static constexpr int XS = D == 3 ? T * T + 4 : T;  // stride of the slowest tile axis (padded)
+  static constexpr int TNP = D == 3 ? T * XS : T * T;  // nodes per tile plane incl. padding
+};
+
+template <int D, bool HF, bool HM>
+struct Sch {
+  static constexpr int X = 0, V = D, C = 2 * D, FJ = 2 * D + D * D;
+  static constexpr int NFJ = HF ? D * D : 1;
+  static constexpr int MAT = FJ + NFJ;
+  static constexpr int NS = MAT + (HM ? 1 : 0);
+};
+
+template <class R>
+struct R4T;
+template <>
+struct R4T<float> {
+  typedef float4 type;
+};
+template <>
+struct R4T<double> {
+  typedef double4 type;
+};
+
+template <class R>
+struct SimK {
+  int res[3], nb[3];
+  int W, WS, friction, bound_clip, n_mat, _pad;
+  R inv_dx, dx, dt, p_mass, stress_coef, four_inv_dx, grav;
+  double lb[3], ub[3];
+  R clip_lo[3], clip_hi[3];
+  int mat_kind[AQ_MAX_MATERIALS];
+  R mu[AQ_MAX_MATERIALS], lam[AQ_MAX_MATERIALS];
+};
+
+struct StepArgs {
+  uint64_t* words;
+  const int32_t* pid;
+  const int4* items;
+  const int32_t* n_items;
+  const void* grid_in;  // G2P source (after grid_op)
+  void* grid_out;       // P2G target (zeroed)
+  unsigned* status;
+  unsigned long long* fallbacks;
+  double* rmax;
+  double* rmin;
+  uint64_t sk;          // dithering key of the G2P substep
+  int do_g2p, do_p2g, ranges, _pad;
+};
+
+// Layout from the kernel parameter (nvcc build).
+struct RtLayout {
+  static __device__ __forceinline__ const aq_layout& get(const aq_layout& p) { return p; }
+};
+
+// ---------------------------------------------------------------- helpers
+
+template <class R>
+__device__ __forceinline__ int base_of(R x, const SimK<R>& K, int d, unsigned& fl) {
+  const R t = x * K.inv_dx - (R)0.5;
+  if (t != t) {
+    fl |= AQ_ST_NAN;
+    return 0;
+  }
+  if (t < (R)0) {
+    fl |= AQ_ST_OUT_OF_DOMAIN;
+    return 0;
+  }
+  if (t >= (R)(K.res[d] - 2)) {
+    fl |= AQ_ST_OUT_OF_DOMAIN;
+    return K.res[d] - 3;
+  }
+  return (int)floor(t);
+}
+
+template <int D>
+__device__ __forceinline__ int64_t cell_index(const int (&res)[3], int i, int j, int k) {
+  return D == 3 ? ((int64_t)i * res[1] + j) * res[2] + k : (int64_t)i * res[1] + j;
+}
+
+__device__ __forceinline__ void red_add_node(float4* g, float m, float a, float b, float c) {
+  asm volatile("red.global.add.v4.f32 [%0], {%1, %2, %3, %4};" ::"l"(g), "f"(m), "f"(a), "f"(b), "f"(c)
+               : "memory");
+}
+
+__device__ __forceinline__ void red_add_node(double4* g, double m, double a, double b, double c) {
+  double* p = reinterpret_cast<double*>(g);
+  atomicAdd(p, m);
+  atomicAdd(p + 1, a);
+  atomicAdd(p + 2, b);
+  atomicAdd(p + 3, c);
+}
+
+__device__ __forceinline__ void atomic_max_d(double* a, double v) {
+  unsigned long long* p = reinterpret_cast<unsigned long long*>(a);
+  unsigned long long old = *p;
+  while (v > __longlong_as_double((long long)old)) {
+    const unsigned long long prev = atomicCAS(p, old, (unsigned long long)__double_as_longlong(v));
+    if (prev == old) break;
+    old = prev;
+  }
+}
+
+__device__ __forceinline__ void atomic_min_d(double* a, double v) {
+  unsigned long long* p = reinterpret_cast<unsigned long long*>(a);
+  unsigned long long old = *p;
+  while (v < __longlong_as_double((long long)old)) {
+    const unsigned long long prev = atomicCAS(p, old, (unsigned long long)__double_as_longlong(v));
+    if (prev == old) break;
+    old = prev;
+  }
+}
+
+// ------------------------------------------------------------- materials
+
+template <int D, class R>
+__device__ __forceinline__ R det(const R* F) {
+  if (D == 2) return F[0] * F[3] - F[1] * F[2];
+  return F[0] * (F[4] * F[8] - F[5] * F[7]) - F[1] * (F[3] * F[8] - F[5] * F[6]) +
+         F[2] * (F[3] * F[7] - F[4] * F[6]);
+}
+
+// Rotation of the polar decomposition: 2D closed form (linalg_impl.py:9-26);
+// 3D by Newton's iteration X <- (X + X^-T)/2 (Higham 1986).
+template <int D, class R>
+__device__ __forceinline__ void polar_rot(const R* F, R* Rm) {
+  if (D == 2) {
+    const R x = F[0] + F[3], y = F[2] - F[1];
+    const R sc = (R)1 / sqrt(x * x + y * y);
+    const R c = x * sc, s = y * sc;
+    Rm[0] = c;
+    Rm[1] = -s;
+    Rm[2] = s;
+    Rm[3] = c;
+  } else {
+    R X[9];
+#pragma unroll
+    for (int k = 0; k < 9; ++k) X[k] = F[k];
+    const R tol = sizeof(R) == 4 ? (R)1e-6 : (R)1e-12;
+    for (int it = 0; it < 20; ++it) {
+      const R c00 = X[4] * X[8] - X[5] * X[7], c01 = X[5] * X[6] - X[3] * X[8], c02 = X[3] * X[7] - X[4] * X[6];
+      const R c10 = X[2] * X[7] - X[1] * X[8], c11 = X[0] * X[8] - X[2] * X[6], c12 = X[1] * X[6] - X[0] * X[7];
+      const R c20 = X[1] * X[5] - X[2] * X[4], c21 = X[2] * X[3] - X[0] * X[5], c22 = X[0] * X[4] - X[1] * X[3];
+      const R id = (R)1 / (X[0] * c00 + X[1] * c01 + X[2] * c02);
+      const R Y[9] = {c00 * id, c01 * id, c02 * id, c10 * id, c11 * id, c12 * id, c20 * id, c21 * id, c22 * id};
+      R diff = 0;
+#pragma unroll
+      for (int k = 0; k < 9; ++k) {
+        const R nx = (R)0.5 * (X[k] + Y[k]);
+        diff += (nx - X[k]) * (nx - X[k]);
+        X[k] = nx;
+      }
+      if (diff < tol * tol) break;
+    }
+#pragma unroll
+    for (int k = 0; k < 9; ++k) Rm[k] = X[k];
+  }
+}
+
+// compute_cauchy (mpm_solver.py:1012-1031), plus the fixed-corotated 3D law.
+template <int D, bool HF, class R>
+__device__ __forceinline__ void cauchy(const SimK<R>& K, int mat, const R* F, R J, R* out) {
+  const int mk = K.mat_kind[mat];
+  const R mu = K.mu[mat], lam = K.lam[mat];
+#pragma unroll
+  for (int k = 0; k < D * D; ++k) out[k] = 0;
+  if (mk == AQ_MAT_FLUID) {
+    const R Jf = HF ? det<D, R>(F) : J;
+#pragma unroll
+    for (int d = 0; d < D; ++d) out[d * D + d] = lam * (Jf - (R)1);
+    return;
+  }
+  if (!HF) return;
+  const R Jd = det<D, R>(F);
+  if (D == 2 || mk == AQ_MAT_COROTATED) {
+    R Rm[D * D];
+    polar_rot<D, R>(F, Rm);
+#pragma unroll
+    for (int i = 0; i < D; ++i)
+#pragma unroll
+      for (int j = 0; j < D; ++j) {
+        R s = 0;
+#pragma unroll
+        for (int k = 0; k < D; ++k) s += (F[i * D + k] - Rm[i * D + k]) * F[j * D + k];
+        out[i * D + j] = (R)2 * mu * s + (i == j ? lam * Jd * (Jd - (R)1) : (R)0);
+      }
+  } else {
+    const R lj = lam * log(Jd);
+#pragma unroll
+    for (int i = 0; i < D; ++i)
+#pragma unroll
+      for (int j = 0; j < D; ++j) {
+        R s = 0;
+#pragma unroll
+        for (int k = 0; k < D; ++k) s += F[i * D + k] * F[j * D + k];
+        out[i * D + j] = mu * (s - (i == j ? (R)1 : (R)0)) + lj;
+      }
+  }
+}
+
+template <int D, class R>
+__device__ __forceinline__ void bspline(const R* x, const SimK<R>& K, int* base, R* fx, R (&w)[3][3], unsigned& fl) {
+#pragma unroll
+  for (int d = 0; d < D; ++d) {
+    base[d] = base_of<R>(x[d], K, d, fl);
+    fx[d] = x[d] * K.inv_dx - (R)base[d];
+    w[0][d] = (R)0.5 * ((R)1.5 - fx[d]) * ((R)1.5 - fx[d]);
+    w[1][d] = (R)0.75 - (fx[d] - (R)1) * (fx[d] - (R)1);
+    w[2][d] = (R)0.5 * (fx[d] - (R)0.5) * (fx[d] - (R)0.5);
+  }
+}
+
+// ------------------------------------------------------------ the step
+
+template <int D, bool HF, bool HM, class R, class LA>
+__global__ void __launch_bounds__(CH, 2) k_step(const __grid_constant__ aq_layout Lp, const SimK<R> K,
+                                                const StepArgs A) {
+  typedef Sch<D, HF, HM> S;
+  typedef Geo<D> G;
+  typedef typename R4T<R>::type R4;
+  constexpr int NS = S::NS;
+  constexpr int T = G::T;
+  constexpr int TNP = G::TNP;
+  auto&& L = LA::get(Lp);  // a reference (RtLayout) or a folded constant (JitLayout)
+  const int W = L.n_words;
+  const int WS = K.WS;
+
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  R4* gtile = reinterpret_cast<R4*>(smem_raw);                      // TNP nodes (m, v): G2P source
+  R4* ptile = gtile + TNP;                                           // NWARP x TNP (m, m v): P2G, per warp
+  int32_t* spid = reinterpret_cast<int32_t*>(ptile + NWARP * TNP);  // CH
+  uint64_t* srec = reinterpret_cast<uint64_t*>(spid + CH);          // CH x WS
+
+  const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+  const int nitems = *A.n_items;
+  const R4* gin = reinterpret_cast<const R4*>(A.grid_in);
+  R4* gout = reinterpret_cast<R4*>(A.grid_out);
+  unsigned fl = 0, nfall = 0;
+  uint64_t* myrec = srec + tid * WS;
+  R4 zero4;
+  zero4.x = zero4.y = zero4.z = zero4.w = 0;
+  if (A.do_p2g)  // private tiles start at zero; the flush of every item re-zeroes them
+    for (int j = tid; j < NWARP * TNP; j += CH) ptile[j] = zero4;
+
+  for (int it = blockIdx.x; it < nitems; it += gridDim.x) {
+    const int4 item = A.items[it];
+    const int cnt = item.z;
+    const int64_t first = item.y;
+    const bool active = tid < cnt;
+    int o[3] = {0, 0, 0};  // tile origin (node coordinates)
+    {
+      int blk = item.x;
+      if (D == 3) {
+        o[2] = (blk % K.nb[2]) * G::BS - 1;
+        blk /= K.nb[2];
+      }
+      o[1] = (blk % K.nb[1]) * G::BS - 1;
+      o[0] = (blk / K.nb[1]) * G::BS - 1;
+    }
+    if (active) {
+      const uint64_t* src = A.words + (first + tid) * W;
+      for (int k = 0; k < W; ++k) myrec[k] = __ldg(src + k);
+      spid[tid] = A.pid[first + tid];
+    }
+    if (A.do_g2p) {  // stage the grid tile (m, v after grid_op)
+      for (int j = tid; j < TNP; j += CH) {
+        int l0, l1, l2 = 0;
+        if (D == 3) {
+          l0 = j / G::XS;
+          const int r = j - l0 * G::XS;
+          l1 = r / T;
+          l2 = r - l1 * T;
+        } else {
+          l0 = j / T;
+          l1 = j - l0 * T;
+        }
+        const int g0 = o[0] + l0, g1 = o[1] + l1, g2 = o[2] + l2;
+        const bool ok = (D == 3 ? l1 < T : true) && g0 >= 0 && g0 < K.res[0] && g1 >= 0 && g1 < K.res[1] &&
+                        (D == 2 || (g2 >= 0 && g2 < K.res[2]));
+        gtile[j] = ok ? gin[cell_index<D>(K.res, g0, g1, g2)] : zero4;
+      }
+    }
+    __syncthreads();
+
+    R vals[NS];
+    if (active) decode_record<NS, R>(L, myrec, vals);
+
+    // ---------------------------------------------------------------- G2P
+    if (A.do_g2p && active) {
+      int base[3] = {0, 0, 0};
+      R fx[3] = {0, 0, 0}, w[3][3];
+      bspline<D, R>(vals + S::X, K, base, fx, w, fl);
+      bool in_tile = true;
+#pragma unroll
+      for (int d = 0; d < D; ++d) {
+        const int l = base[d] - o[d];
+        in_tile = in_tile && l >= 0 && l <= T - 3;
+      }
+      R nv[D], Sm[D][D];
+#pragma unroll
+      for (int d = 0; d < D; ++d) {
+        nv[d] = 0;
+#pragma unroll
+        for (int e = 0; e < D; ++e) Sm[d][e] = 0;
+      }
+      const int lb = in_tile ? (D == 3 ? (base[0] - o[0]) * G::XS + (base[1] - o[1]) * T + (base[2] - o[2])
+                                       : (base[0] - o[0]) * T + (base[1] - o[1]))
+                             : 0;
+      if (!in_tile) ++nfall;
+#pragma unroll
+      for (int a = 0; a < 3; ++a)
+#pragma unroll
+        for (int b = 0; b < 3; ++b) {
+          const R wab = w[a][0] * w[b][1];
+#pragma unroll
+          for (int c = 0; c < (D == 3 ? 3 : 1); ++c) {
+            const R weight = D == 3 ? wab * w[c][2] : wab;
+            const R4 g = in_tile ? gtile[lb + (D == 3 ? a * G::XS + b * T + c : a * T + b)]
+                                 : gin[cell_index<D>(K.res, base[0] + a, base[1] + b, D == 3 ? base[2] + c : 0)];
+            const R gv[3] = {g.y, g.z, g.w};
+            const int off[3] = {a, b, c};
+#pragma unroll
+            for (int d = 0; d < D; ++d) {
+              const R wg = weight * gv[d];
+              nv[d] += wg;
+#pragma unroll
+              for (int e = 0; e < D; ++e) {
+                if (off[e] == 1) Sm[d][e] += wg;
+                if (off[e] == 2) Sm[d][e] += (R)2 * wg;
+              }
+            }
+          }
+        }
+      // new_C = 4 inv_dx sum w g_v (off - fx)^T;  new_x = x + dt new_v
+      R nC[D * D];
+#pragma unroll
+      for (int d = 0; d < D; ++d)
+#pragma unroll
+        for (int e = 0; e < D; ++e) nC[d * D + e] = K.four_inv_dx * (Sm[d][e] - nv[d] * fx[e]);
+#pragma unroll
+      for (int d = 0; d < D; ++d) {
+        R nx = vals[S::X + d] + K.dt * nv[d];
+        if (K.bound_clip) nx = fmax(fmin(nx, K.clip_hi[d]), K.clip_lo[d]);
+        vals[S::X + d] = nx;
+        vals[S::V + d] = nv[d];
+      }
+      const int mat = HM ? min(max((int)vals[S::MAT], 0), K.n_mat - 1) : 0;
+      if (HF) {
+        R nF[D * D];
+#pragma unroll
+        for (int i = 0; i < D; ++i)
+#pragma unroll
+          for (int j = 0; j < D; ++j) {
+            R acc = 0;
+#pragma unroll
+            for (int k = 0; k < D; ++k)
+              acc += ((i == k ? (R)1 : (R)0) + K.dt * nC[i * D + k]) * vals[S::FJ + k * D + j];
+            nF[i * D + j] = acc;
+          }
+        if (HM && K.mat_kind[mat] == AQ_MAT_FLUID) {  // fluid in an F record keeps only J
+          const R Jn = det<D, R>(nF);
+          const R sj = D == 3 ? cbrt(Jn) : sqrt(Jn);
+#pragma unroll
+          for (int i = 0; i < D; ++i)
+#pragma unroll
+            for (int j = 0; j < D; ++j) nF[i * D + j] = i == j ? sj : (R)0;
+        }
+#pragma unroll
+        for (int k = 0; k < D * D; ++k) vals[S::FJ + k] = nF[k];
+      } else {
+        R tr = 0;
+#pragma unroll
+        for (int d = 0; d < D; ++d) tr += nC[d * D + d];
+        vals[S::FJ] = ((R)1 + K.dt * tr) * vals[S::FJ];
+      }
+#pragma unroll
+      for (int k = 0; k < D * D; ++k) vals[S::C + k] = nC[k];
+      // bit_pack_assign of the new state; vals become the values a later
+      // read of the record returns (input of the next P2G)
+      encode_record<NS, R>(L, vals, myrec, particle_key(A.sk, spid[tid]), (const float*)0, (const double*)0);
+      uint64_t* dst = A.words + (first + tid) * W;
+      for (int k = 0; k < W; ++k) dst[k] = myrec[k];
+    }
+
+    // -------------------------------------------- range detection (opt)
+    if (A.ranges && A.do_g2p) {
+#pragma unroll
+      for (int s = 0; s < NS; ++s) {
+        double mx = active ? (double)vals[s] : -(double)AQ_POS_INF, mn = active ? (double)vals[s] : (double)AQ_POS_INF;
+#pragma unroll
+        for (int k = 16; k; k >>= 1) {
+          mx = fmax(mx, __shfl_xor_sync(0xffffffffu, mx, k));
+          mn = fmin(mn, __shfl_xor_sync(0xffffffffu, mn, k));
+        }
+        if (lane == 0) {
+          atomic_max_d(A.rmax + s, mx);
+          atomic_min_d(A.rmin + s, mn);
+        }
+      }
+    }
+
+    // ---------------------------------------------------------------- P2G
+    if (A.do_p2g) {
+      int base[3] = {0, 0, 0};
+      R fx[3] = {0, 0, 0}, w[3][3];
+      R Aff[D * D], q[D];
+      bool in_tile = false;
+      int lb = 0;
+      if (active) {
+        const int mat = HM ? min(max((int)vals[S::MAT], 0), K.n_mat - 1) : 0;
+        bspline<D, R>(vals + S::X, K, base, fx, w, fl);
+        in_tile = true;
+#pragma unroll
+        for (int d = 0; d < D; ++d) {
+          const int l = base[d] - o[d];
+          in_tile = in_tile && l >= 0 && l <= T - 3;
+        }
+        R cau[D * D];
+        cauchy<D, HF, R>(K, mat, vals + S::FJ, vals[S::FJ], cau);
+        // node value = m v + affine (off - fx) dx = q + Aff off,
+        // q = m v - affine fx dx, Aff = (stress + m C) dx
+#pragma unroll
+        for (int k = 0; k < D * D; ++k) Aff[k] = (K.stress_coef * cau[k] + K.p_mass * vals[S::C + k]) * K.dx;
+#pragma unroll
+        for (int d = 0; d < D; ++d) {
+          R s = K.p_mass * vals[S::V + d];
+#pragma unroll
+          for (int e = 0; e < D; ++e) s -= Aff[d * D + e] * fx[e];
+          q[d] = s;
+        }
+        if (in_tile) {
+          lb = D == 3 ? (base[0] - o[0]) * G::XS + (base[1] - o[1]) * T + (base[2] - o[2])
+                      : (base[0] - o[0]) * T + (base[1] - o[1]);
+        } else {
+          ++nfall;
+        }
+      }
+      // Lanes of a warp with the same base cell add into the same nodes and
+      // take turns (rank among peers); lanes of different base cells never
+      // share a node for the same stencil offset.  Binning orders records so
+      // that a warp's lanes are in different cells: one turn is the norm.
+      const int key = (active && in_tile) ? lb : -1 - lane;
+      const unsigned peers = __match_any_sync(0xffffffffu, key);
+      const int rank = __popc(peers & ((1u << lane) - 1u));
+      const int rounds = __reduce_max_sync(0xffffffffu, (unsigned)__popc(peers));
+      R4* mytile = ptile + warp * TNP;
+      for (int r = 0; r < rounds; ++r) {
+        if (active && rank == r) {
+#pragma unroll
+          for (int a = 0; a < 3; ++a)
+#pragma unroll
+            for (int b = 0; b < 3; ++b) {
+              const R wab = w[a][0] * w[b][1];
+              R qab[3];
+#pragma unroll
+              for (int d = 0; d < D; ++d) {
+                R s = q[d];
+                if (a == 1) s += Aff[d * D + 0];
+                if (a == 2) s += (R)2 * Aff[d * D + 0];
+                if (b == 1) s += Aff[d * D + 1];
+                if (b == 2) s += (R)2 * Aff[d * D + 1];
+                qab[d] = s;
+              }
+#pragma unroll
+              for (int c = 0; c < (D == 3 ? 3 : 1); ++c) {
+                const R weight = D == 3 ? wab * w[c][2] : wab;
+                R mv[3] = {0, 0, 0};
+#pragma unroll
+                for (int d = 0; d < D; ++d) {
+                  R s = qab[d];
+                  if (D == 3 && c == 1) s += Aff[d * D + 2];
+                  if (D == 3 && c == 2) s += (R)2 * Aff[d * D + 2];
+                  mv[d] = weight * s;
+                }
+                const R m = weight * K.p_mass;
+                if (in_tile) {
+                  R4& t = mytile[lb + (D == 3 ? a * G::XS + b * T + c : a * T + b)];
+                  R4 v = t;
+                  v.x += m;
+                  v.y += mv[0];
+                  v.z += mv[1];
+                  v.w += mv[2];
+                  t = v;
+                } else {
+                  R4* g = gout + cell_index<D>(K.res, base[0] + a, base[1] + b, D == 3 ? base[2] + c : 0);
+                  red_add_node(g, m, mv[0], mv[1], mv[2]);
+                }
+              }
+            }
+        }
+        __syncwarp();
+      }
+      __syncthreads();
+      // sum the warp tiles, re-zero them, flush: one vector reduction per
+      // touched node
+      for (int j = tid; j < TNP; j += CH) {
+        R4 sum = zero4;
+#pragma unroll
+        for (int k = 0; k < NWARP; ++k) {
+          const R4 v = ptile[k * TNP + j];
+          sum.x += v.x;
+          sum.y += v.y;
+          sum.z += v.z;
+          sum.w += v.w;
+          ptile[k * TNP + j] = zero4;
+        }
+        if (sum.x == (R)0) continue;
+        int l0, l1, l2 = 0;
+        if (D == 3) {
+          l0 = j / G::XS;
+          const int rr = j - l0 * G::XS;
+          l1 = rr / T;
+          l2 = rr - l1 * T;
+        } else {
+          l0 = j / T;
+          l1 = j - l0 * T;
+        }
+        const int g0 = o[0] + l0, g1 = o[1] + l1, g2 = o[2] + l2;
+        if (g0 < 0 || g0 >= K.res[0] || g1 < 0 || g1 >= K.res[1] || (D == 3 && (g2 < 0 || g2 >= K.res[2])))
+          continue;
+        red_add_node(gout + cell_index<D>(K.res, g0, g1, g2), sum.x, sum.y, sum.z, sum.w);
+      }
+    }
+    __syncthreads();
+  }
+  if (fl) atomicOr(A.status, fl);
+  if (nfall) atomicAdd(A.fallbacks, (unsigned long long)nfall);
+}
+
+}  // namespace aq

@@ -1,238 +1,24 @@
-// libaq.so: the quantized MLS-MPM substep on sm_100a.
+// libaq.so: the simulator object, binning and grid kernels, and the C ABI
+// of the substep (include/aq.h).  The fused substep kernel k_step lives in
+// aq_kernels.cuh (see there for the data layout and the algorithm).
 //
-// Data layout in HBM
-//   records  : n x W u64 bit_pack records, kept sorted by grid cell (blocks
-//              of 4^3 cells in 3D, 8^2 in 2D, cells inside a block), with a
-//              particle-id array that moves with them.
-//   grids    : two dense grids of R4 nodes (m, m*v) / (m, v), row-major,
-//              used alternately as P2G target and G2P source.
-//   binning  : per-cell counts/offsets, per-particle key and rank, and a list
-//              of work items (block, first record, count <= 256).
-//
-// Kernels per substep
-//   k_step   : one CTA per work item (persistent loop).  Loads the item's
-//              records into shared memory, stages the block's grid tile,
-//              G2P (gather, F/J/C/x update) of substep k, encodes the new
-//              record (bit_pack_assign), decodes it and P2G of substep k+1
-//              into a shared-memory tile, flushed to the grid with
-//              vector reductions.  Either phase may be off (first / last
-//              substep of a run).
-//   k_grid   : grid_op (normalise, gravity, walls) on the accumulated grid
-//              and clear of the other grid.
-// Binning (k_bin, scan, k_scatter, k_items) runs every sort_interval
-// substeps; between re-binnings particles may drift one cell out of their
-// block's tile and fall back to global atomics beyond that.
+// Per substep: k_step (G2P of substep k + P2G of substep k+1) and k_grid
+// (grid_op of the accumulated grid, clear of the other).  Every
+// sort_interval substeps the records are re-binned: k_bin (cell key and
+// rank), an exclusive scan of the per-cell counts, k_scatter (move records
+// and ids into slot-major chunks), k_items (work items).
 #include <math.h>
 #include <stdio.h>
 #include <string.h>
 
 #include <new>
+#include <string>
 
-#include "aq_codec.cuh"
 #include "aq_common.cuh"
+#include "aq_jit.h"
+#include "aq_kernels.cuh"
 
 namespace aq {
-
-constexpr int CH = 256;  // particles per work item = threads per CTA
-constexpr int NW = CH / 32;
-
-template <int D>
-struct Geo {
-  static constexpr int BS = D == 3 ? 4 : 8;  // block edge (cells)
-  static constexpr int T = BS + 4;           // tile edge (nodes): 1-cell drift each side + stencil
-  static constexpr int XS = D == 3 ? T * T + 4 : T;  // stride of the slowest tile axis (padded)
-  static constexpr int TNP = D == 3 ? T * XS : T * T;  // nodes per tile plane incl. padding
-  static constexpr int NOFF = D == 3 ? 27 : 9;
-};
-
-template <int D, bool HF, bool HM>
-struct Sch {
-  static constexpr int X = 0, V = D, C = 2 * D, FJ = 2 * D + D * D;
-  static constexpr int NFJ = HF ? D * D : 1;
-  static constexpr int MAT = FJ + NFJ;
-  static constexpr int NS = MAT + (HM ? 1 : 0);
-};
-
-template <class R>
-struct R4T;
-template <>
-struct R4T<float> {
-  using type = float4;
-};
-template <>
-struct R4T<double> {
-  using type = double4;
-};
-
-template <class R>
-struct SimK {
-  int res[3], nb[3];
-  int W, friction, bound_clip, n_mat;
-  R inv_dx, dx, dt, p_mass, stress_coef, four_inv_dx, grav;
-  double lb[3], ub[3];
-  R clip_lo[3], clip_hi[3];
-  int mat_kind[AQ_MAX_MATERIALS];
-  R mu[AQ_MAX_MATERIALS], lam[AQ_MAX_MATERIALS];
-};
-
-// ---------------------------------------------------------------- helpers
-
-template <class R>
-__device__ __forceinline__ int base_of(R x, const SimK<R>& K, int d, unsigned& fl) {
-  const R t = x * K.inv_dx - (R)0.5;
-  if (t != t) {
-    fl |= AQ_ST_NAN;
-    return 0;
-  }
-  const R lim = (R)(K.res[d] - 3);
-  if (t < (R)0) {
-    fl |= AQ_ST_OUT_OF_DOMAIN;
-    return 0;
-  }
-  if (t >= lim + (R)1) {
-    fl |= AQ_ST_OUT_OF_DOMAIN;
-    return K.res[d] - 3;
-  }
-  return (int)floor(t);
-}
-
-template <int D>
-__device__ __forceinline__ int64_t cell_index(const int (&res)[3], int i, int j, int k) {
-  return D == 3 ? ((int64_t)i * res[1] + j) * res[2] + k : (int64_t)i * res[1] + j;
-}
-
-__device__ __forceinline__ void red_add_v4(float4* addr, float a, float b, float c, float d) {
-  asm volatile("red.global.add.v4.f32 [%0], {%1, %2, %3, %4};" ::"l"(addr), "f"(a), "f"(b), "f"(c), "f"(d)
-               : "memory");
-}
-
-__device__ __forceinline__ void red_add_node(float4* g, float m, float a, float b, float c) { red_add_v4(g, m, a, b, c); }
-
-__device__ __forceinline__ void red_add_node(double4* g, double m, double a, double b, double c) {
-  double* p = reinterpret_cast<double*>(g);
-  atomicAdd(p, m);
-  atomicAdd(p + 1, a);
-  atomicAdd(p + 2, b);
-  atomicAdd(p + 3, c);
-}
-
-__device__ __forceinline__ void atomic_max_d(double* a, double v) {
-  unsigned long long* p = reinterpret_cast<unsigned long long*>(a);
-  unsigned long long old = *p;
-  while (v > __longlong_as_double((long long)old)) {
-    const unsigned long long prev = atomicCAS(p, old, (unsigned long long)__double_as_longlong(v));
-    if (prev == old) break;
-    old = prev;
-  }
-}
-
-__device__ __forceinline__ void atomic_min_d(double* a, double v) {
-  unsigned long long* p = reinterpret_cast<unsigned long long*>(a);
-  unsigned long long old = *p;
-  while (v < __longlong_as_double((long long)old)) {
-    const unsigned long long prev = atomicCAS(p, old, (unsigned long long)__double_as_longlong(v));
-    if (prev == old) break;
-    old = prev;
-  }
-}
-
-// ------------------------------------------------------------- materials
-
-template <int D, class R>
-__device__ __forceinline__ R det(const R* F) {
-  if (D == 2) return F[0] * F[3] - F[1] * F[2];
-  return F[0] * (F[4] * F[8] - F[5] * F[7]) - F[1] * (F[3] * F[8] - F[5] * F[6]) +
-         F[2] * (F[3] * F[7] - F[4] * F[6]);
-}
-
-template <class R>
-__device__ __forceinline__ R rsqrt_r(R v);
-template <>
-__device__ __forceinline__ float rsqrt_r<float>(float v) {
-  return 1.0f / sqrtf(v);
-}
-template <>
-__device__ __forceinline__ double rsqrt_r<double>(double v) {
-  return 1.0 / sqrt(v);
-}
-
-// Rotation of the polar decomposition: 2D closed form (linalg_impl.py:9-26);
-// 3D by Newton's iteration X <- (X + X^-T)/2.
-template <int D, class R>
-__device__ __forceinline__ void polar_rot(const R* F, R* Rm) {
-  if (D == 2) {
-    const R x = F[0] + F[3], y = F[2] - F[1];
-    const R sc = rsqrt_r<R>(x * x + y * y);
-    const R c = x * sc, s = y * sc;
-    Rm[0] = c;
-    Rm[1] = -s;
-    Rm[2] = s;
-    Rm[3] = c;
-  } else {
-    R X[9];
-#pragma unroll
-    for (int k = 0; k < 9; ++k) X[k] = F[k];
-    const R tol = sizeof(R) == 4 ? (R)1e-6 : (R)1e-12;
-    for (int it = 0; it < 20; ++it) {
-      const R c00 = X[4] * X[8] - X[5] * X[7], c01 = X[5] * X[6] - X[3] * X[8], c02 = X[3] * X[7] - X[4] * X[6];
-      const R c10 = X[2] * X[7] - X[1] * X[8], c11 = X[0] * X[8] - X[2] * X[6], c12 = X[1] * X[6] - X[0] * X[7];
-      const R c20 = X[1] * X[5] - X[2] * X[4], c21 = X[2] * X[3] - X[0] * X[5], c22 = X[0] * X[4] - X[1] * X[3];
-      const R id = (R)1 / (X[0] * c00 + X[1] * c01 + X[2] * c02);
-      const R Y[9] = {c00 * id, c01 * id, c02 * id, c10 * id, c11 * id, c12 * id, c20 * id, c21 * id, c22 * id};
-      R diff = 0;
-#pragma unroll
-      for (int k = 0; k < 9; ++k) {
-        const R nx = (R)0.5 * (X[k] + Y[k]);
-        diff += (nx - X[k]) * (nx - X[k]);
-        X[k] = nx;
-      }
-      if (diff < tol * tol) break;
-    }
-#pragma unroll
-    for (int k = 0; k < 9; ++k) Rm[k] = X[k];
-  }
-}
-
-// compute_cauchy (mpm_solver.py:1012-1031), plus the fixed-corotated 3D law.
-template <int D, bool HF, class R>
-__device__ __forceinline__ void cauchy(const SimK<R>& K, int mat, const R* F, R J, R* out) {
-  const int mk = K.mat_kind[mat];
-  const R mu = K.mu[mat], lam = K.lam[mat];
-#pragma unroll
-  for (int k = 0; k < D * D; ++k) out[k] = 0;
-  if (mk == AQ_MAT_FLUID) {
-    const R Jf = HF ? det<D, R>(F) : J;
-#pragma unroll
-    for (int d = 0; d < D; ++d) out[d * D + d] = lam * (Jf - (R)1);
-    return;
-  }
-  if (!HF) return;
-  const R Jd = det<D, R>(F);
-  if (D == 2 || mk == AQ_MAT_COROTATED) {
-    R Rm[D * D];
-    polar_rot<D, R>(F, Rm);
-#pragma unroll
-    for (int i = 0; i < D; ++i)
-#pragma unroll
-      for (int j = 0; j < D; ++j) {
-        R s = 0;
-#pragma unroll
-        for (int k = 0; k < D; ++k) s += (F[i * D + k] - Rm[i * D + k]) * F[j * D + k];
-        out[i * D + j] = (R)2 * mu * s + (i == j ? lam * Jd * (Jd - (R)1) : (R)0);
-      }
-  } else {
-    const R lj = lam * log(Jd);
-#pragma unroll
-    for (int i = 0; i < D; ++i)
-#pragma unroll
-      for (int j = 0; j < D; ++j) {
-        R s = 0;
-#pragma unroll
-        for (int k = 0; k < D; ++k) s += F[i * D + k] * F[j * D + k];
-        out[i * D + j] = mu * (s - (i == j ? (R)1 : (R)0)) + lj;
-      }
-  }
-}
 
 // ------------------------------------------------------------ binning
 
@@ -262,13 +48,36 @@ __global__ void __launch_bounds__(256) k_bin(const __grid_constant__ aq_layout L
   if (fl) atomicOr(status, fl);
 }
 
+// Move record i to its sorted position.  A block's records (in cell
+// order) are cut into chunks of at most 256, the work items.  Inside a chunk
+// the order is slot-major: first the chunk's first record of every cell (in
+// cell order), then the second of every cell, and so on.  Consecutive
+// records, i.e. the lanes of a warp in k_step, are then in different cells
+// whenever the chunk spans at least 32 cells.
 __global__ void __launch_bounds__(256) k_scatter(const uint64_t* __restrict__ win, const int32_t* __restrict__ pin,
                                                  uint64_t* __restrict__ wout, int32_t* __restrict__ pout,
                                                  const int32_t* __restrict__ keys, const int32_t* __restrict__ ranks,
                                                  const int32_t* __restrict__ start, int64_t n, int W) {
   const int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
   if (i >= n) return;
-  const int64_t dst = (int64_t)start[keys[i]] + ranks[i];
+  const int key = keys[i];
+  const int64_t g = (int64_t)start[key] + ranks[i];
+  const int64_t c0 = (int64_t)(key >> 6) * 64;
+  const int64_t b0 = start[c0];
+  const int64_t be = start[c0 + 64];
+  const int64_t cs = b0 + ((g - b0) / CH) * CH;  // chunk [cs, ce)
+  const int64_t ce = min(cs + CH, be);
+  const int r = (int)(g - max((int64_t)start[key], cs));  // rank in its cell within the chunk
+  const int myc = key & 63;
+  int t = 0;
+  int64_t s0 = start[c0];
+  for (int k = 0; k < 64; ++k) {
+    const int64_t s1 = start[c0 + k + 1];
+    const int nk = (int)max((int64_t)0, min(s1, ce) - max(s0, cs));
+    t += min(nk, r) + ((k < myc && nk > r) ? 1 : 0);
+    s0 = s1;
+  }
+  const int64_t dst = cs + t;
   for (int j = 0; j < W; ++j) wout[dst * W + j] = win[i * W + j];
   pout[dst] = pin[i];
 }
@@ -365,337 +174,19 @@ __global__ void __launch_bounds__(SCAN_T) k_scan_apply(const int32_t* __restrict
   }
 }
 
-// --------------------------------------------------------------- substep
-
-struct StepArgs {
-  uint64_t* words;
-  const int32_t* pid;
-  const int4* items;
-  const int32_t* n_items;
-  const void* grid_in;   // G2P source (after grid_op)
-  void* grid_out;        // P2G target (zeroed)
-  unsigned* status;
-  unsigned long long* fallbacks;
-  double* rmax;
-  double* rmin;
-  uint64_t sk;           // dithering key of the G2P substep
-  int do_g2p, do_p2g, ranges;
-};
-
-template <int D, bool HF, bool HM, class R>
-__global__ void __launch_bounds__(CH, 2) k_step(const __grid_constant__ aq_layout L, const SimK<R> K,
-                                                const StepArgs A) {
-  using S = Sch<D, HF, HM>;
-  using G = Geo<D>;
-  using R4 = typename R4T<R>::type;
-  constexpr int NS = S::NS;
-  constexpr int T = G::T;
-  constexpr int TNP = G::TNP;
-  const int W = K.W;
-
-  extern __shared__ __align__(16) unsigned char smem_raw[];
-  R* tile = reinterpret_cast<R*>(smem_raw);                              // (D+1) planes of TNP
-  int32_t* spid = reinterpret_cast<int32_t*>(tile + (D + 1) * TNP);      // CH
-  uint64_t* srec = reinterpret_cast<uint64_t*>(spid + CH);               // CH * W (8-byte aligned: see host)
-
-  const int tid = threadIdx.x;
-  const int p = (tid & 31) * NW + (tid >> 5);  // lane-major: a warp spans 32 distinct cells
-  const int nitems = *A.n_items;
-  const R4* gin = reinterpret_cast<const R4*>(A.grid_in);
-  R4* gout = reinterpret_cast<R4*>(A.grid_out);
-  unsigned fl = 0;
-  unsigned nfall = 0;
-
-  for (int it = blockIdx.x; it < nitems; it += gridDim.x) {
-    const int4 item = A.items[it];
-    const int cnt = item.z;
-    const int64_t first = item.y;
-    int o[3] = {0, 0, 0};  // tile origin (node coordinates)
-    {
-      int blk = item.x;
-      if (D == 3) {
-        o[2] = (blk % K.nb[2]) * G::BS - 1;
-        blk /= K.nb[2];
-      }
-      o[1] = (blk % K.nb[1]) * G::BS - 1;
-      o[0] = (blk / K.nb[1]) * G::BS - 1;
-    }
-    // ---- records and ids of the item into shared memory (coalesced)
-    {
-      const uint64_t* src = A.words + first * W;
-      for (int j = tid; j < cnt * W; j += CH) srec[j] = src[j];
-      for (int j = tid; j < cnt; j += CH) spid[j] = A.pid[first + j];
-    }
-    // ---- stage the grid tile for G2P
-    if (A.do_g2p) {
-      for (int j = tid; j < TNP; j += CH) {
-        int l0, l1, l2 = 0;
-        if (D == 3) {
-          l0 = j / G::XS;
-          const int r = j - l0 * G::XS;
-          l1 = r / T;
-          l2 = r - l1 * T;
-        } else {
-          l0 = j / T;
-          l1 = j - l0 * T;
-        }
-        const int g0 = o[0] + l0, g1 = o[1] + l1, g2 = o[2] + l2;
-        const bool ok = (D == 3 ? l1 < T : true) && g0 >= 0 && g0 < K.res[0] && g1 >= 0 && g1 < K.res[1] &&
-                        (D == 2 || (g2 >= 0 && g2 < K.res[2]));
-        R4 v = {0, 0, 0, 0};
-        if (ok) v = gin[cell_index<D>(K.res, g0, g1, g2)];
-        tile[0 * TNP + j] = v.y;
-        tile[1 * TNP + j] = v.z;
-        if (D == 3) tile[2 * TNP + j] = v.w;
-      }
-    }
-    __syncthreads();
-
-    const bool active = p < cnt;
-    R vals[NS];
-    if (active) decode_record<NS, R>(L, srec + p * W, vals);
-
-    // ---------------------------------------------------------------- G2P
-    if (A.do_g2p && active) {
-      int base[3] = {0, 0, 0};
-      R fx[3] = {0, 0, 0}, w[3][3];
-      bool in_tile = true;
-#pragma unroll
-      for (int d = 0; d < D; ++d) {
-        base[d] = base_of<R>(vals[S::X + d], K, d, fl);
-        fx[d] = vals[S::X + d] * K.inv_dx - (R)base[d];
-        w[0][d] = (R)0.5 * ((R)1.5 - fx[d]) * ((R)1.5 - fx[d]);
-        w[1][d] = (R)0.75 - (fx[d] - (R)1) * (fx[d] - (R)1);
-        w[2][d] = (R)0.5 * (fx[d] - (R)0.5) * (fx[d] - (R)0.5);
-        const int l = base[d] - o[d];
-        in_tile = in_tile && l >= 0 && l <= T - 3;
-      }
-      R nv[D], Sm[D][D];
-#pragma unroll
-      for (int d = 0; d < D; ++d) {
-        nv[d] = 0;
-#pragma unroll
-        for (int e = 0; e < D; ++e) Sm[d][e] = 0;
-      }
-      auto accum = [&](int a, int b, int c, const R* gv) {
-        const R weight = D == 3 ? w[a][0] * w[b][1] * w[c][2] : w[a][0] * w[b][1];
-        const int off[3] = {a, b, c};
-#pragma unroll
-        for (int d = 0; d < D; ++d) {
-          const R wg = weight * gv[d];
-          nv[d] += wg;
-#pragma unroll
-          for (int e = 0; e < D; ++e) {
-            if (off[e] == 1) Sm[d][e] += wg;
-            if (off[e] == 2) Sm[d][e] += (R)2 * wg;
-          }
-        }
-      };
-      if (in_tile) {
-        const int lb = D == 3 ? (base[0] - o[0]) * G::XS + (base[1] - o[1]) * T + (base[2] - o[2])
-                              : (base[0] - o[0]) * T + (base[1] - o[1]);
-#pragma unroll
-        for (int a = 0; a < 3; ++a)
-#pragma unroll
-          for (int b = 0; b < 3; ++b)
-#pragma unroll
-            for (int c = 0; c < (D == 3 ? 3 : 1); ++c) {
-              const int idx = lb + (D == 3 ? a * G::XS + b * T + c : a * T + b);
-              R gv[D];
-#pragma unroll
-              for (int d = 0; d < D; ++d) gv[d] = tile[d * TNP + idx];
-              accum(a, b, c, gv);
-            }
-      } else {
-        ++nfall;
-#pragma unroll
-        for (int a = 0; a < 3; ++a)
-#pragma unroll
-          for (int b = 0; b < 3; ++b)
-#pragma unroll
-            for (int c = 0; c < (D == 3 ? 3 : 1); ++c) {
-              const R4 g = gin[cell_index<D>(K.res, base[0] + a, base[1] + b, D == 3 ? base[2] + c : 0)];
-              const R gv[3] = {g.y, g.z, g.w};
-              accum(a, b, c, gv);
-            }
-      }
-      // new_C = 4 inv_dx sum w g_v (off - fx)^T;  new_x = x + dt new_v
-      R nC[D * D];
-#pragma unroll
-      for (int d = 0; d < D; ++d)
-#pragma unroll
-        for (int e = 0; e < D; ++e) nC[d * D + e] = K.four_inv_dx * (Sm[d][e] - nv[d] * fx[e]);
-#pragma unroll
-      for (int d = 0; d < D; ++d) {
-        R nx = vals[S::X + d] + K.dt * nv[d];
-        if (K.bound_clip) nx = fmax(fmin(nx, K.clip_hi[d]), K.clip_lo[d]);
-        vals[S::X + d] = nx;
-        vals[S::V + d] = nv[d];
-      }
-      const int mat = HM ? min(max((int)vals[S::MAT], 0), K.n_mat - 1) : 0;
-      if (HF) {
-        R nF[D * D];
-#pragma unroll
-        for (int i = 0; i < D; ++i)
-#pragma unroll
-          for (int j = 0; j < D; ++j) {
-            R acc = 0;
-#pragma unroll
-            for (int k = 0; k < D; ++k)
-              acc += ((i == k ? (R)1 : (R)0) + K.dt * nC[i * D + k]) * vals[S::FJ + k * D + j];
-            nF[i * D + j] = acc;
-          }
-        if (HM && K.mat_kind[mat] == AQ_MAT_FLUID) {  // fluid in an F record keeps only J
-          const R Jn = det<D, R>(nF);
-          const R sj = D == 3 ? cbrt(Jn) : sqrt(Jn);
-#pragma unroll
-          for (int i = 0; i < D; ++i)
-#pragma unroll
-            for (int j = 0; j < D; ++j) nF[i * D + j] = i == j ? sj : (R)0;
-        }
-#pragma unroll
-        for (int k = 0; k < D * D; ++k) vals[S::FJ + k] = nF[k];
-      } else {
-        R tr = 0;
-#pragma unroll
-        for (int d = 0; d < D; ++d) tr += nC[d * D + d];
-        vals[S::FJ] = ((R)1 + K.dt * tr) * vals[S::FJ];
-      }
-#pragma unroll
-      for (int k = 0; k < D * D; ++k) vals[S::C + k] = nC[k];
-      // bit_pack_assign of the new state; vals become the values a later
-      // read of the record returns (input of the next P2G)
-      encode_record<NS, R>(L, vals, srec + p * W, particle_key(A.sk, spid[p]), nullptr, nullptr);
-    }
-
-    // -------------------------------------------- range detection (opt)
-    if (A.ranges && A.do_g2p) {
-      const int lane = tid & 31;
-#pragma unroll
-      for (int s = 0; s < NS; ++s) {
-        double mx = active ? (double)vals[s] : -INFINITY, mn = active ? (double)vals[s] : INFINITY;
-#pragma unroll
-        for (int k = 16; k; k >>= 1) {
-          mx = fmax(mx, __shfl_xor_sync(0xffffffffu, mx, k));
-          mn = fmin(mn, __shfl_xor_sync(0xffffffffu, mn, k));
-        }
-        if (lane == 0) {
-          atomic_max_d(A.rmax + s, mx);
-          atomic_min_d(A.rmin + s, mn);
-        }
-      }
-    }
-
-    __syncthreads();
-    if (A.do_g2p) {  // write the item's records back (coalesced)
-      uint64_t* dst = A.words + first * W;
-      for (int j = tid; j < cnt * W; j += CH) dst[j] = srec[j];
-    }
-
-    // ---------------------------------------------------------------- P2G
-    if (A.do_p2g) {
-      for (int j = tid; j < (D + 1) * TNP; j += CH) tile[j] = 0;
-      __syncthreads();
-      if (active) {
-        const int mat = HM ? min(max((int)vals[S::MAT], 0), K.n_mat - 1) : 0;
-        int base[3] = {0, 0, 0};
-        R fx[3] = {0, 0, 0}, w[3][3];
-        bool in_tile = true;
-#pragma unroll
-        for (int d = 0; d < D; ++d) {
-          base[d] = base_of<R>(vals[S::X + d], K, d, fl);
-          fx[d] = vals[S::X + d] * K.inv_dx - (R)base[d];
-          w[0][d] = (R)0.5 * ((R)1.5 - fx[d]) * ((R)1.5 - fx[d]);
-          w[1][d] = (R)0.75 - (fx[d] - (R)1) * (fx[d] - (R)1);
-          w[2][d] = (R)0.5 * (fx[d] - (R)0.5) * (fx[d] - (R)0.5);
-          const int l = base[d] - o[d];
-          in_tile = in_tile && l >= 0 && l <= T - 3;
-        }
-        R cau[D * D];
-        cauchy<D, HF, R>(K, mat, vals + S::FJ, vals[S::FJ], cau);
-        // affine = stress + m C;  node value = m v + affine (off - fx) dx
-        //   = q + A off  with q = m v - affine fx dx, A = affine dx
-        R Aff[D * D], q[D];
-#pragma unroll
-        for (int k = 0; k < D * D; ++k) Aff[k] = (K.stress_coef * cau[k] + K.p_mass * vals[S::C + k]) * K.dx;
-#pragma unroll
-        for (int d = 0; d < D; ++d) {
-          R s = K.p_mass * vals[S::V + d];
-#pragma unroll
-          for (int e = 0; e < D; ++e) s -= Aff[d * D + e] * fx[e];
-          q[d] = s;
-        }
-        if (!in_tile) ++nfall;
-        const int lb = D == 3 ? (base[0] - o[0]) * G::XS + (base[1] - o[1]) * T + (base[2] - o[2])
-                              : (base[0] - o[0]) * T + (base[1] - o[1]);
-#pragma unroll
-        for (int a = 0; a < 3; ++a)
-#pragma unroll
-          for (int b = 0; b < 3; ++b)
-#pragma unroll
-            for (int c = 0; c < (D == 3 ? 3 : 1); ++c) {
-              const R weight = D == 3 ? w[a][0] * w[b][1] * w[c][2] : w[a][0] * w[b][1];
-              const int off[3] = {a, b, c};
-              R mv[3] = {0, 0, 0};
-#pragma unroll
-              for (int d = 0; d < D; ++d) {
-                R s = q[d];
-#pragma unroll
-                for (int e = 0; e < D; ++e) {
-                  if (off[e] == 1) s += Aff[d * D + e];
-                  if (off[e] == 2) s += (R)2 * Aff[d * D + e];
-                }
-                mv[d] = weight * s;
-              }
-              const R m = weight * K.p_mass;
-              if (in_tile) {
-                const int idx = lb + (D == 3 ? a * G::XS + b * T + c : a * T + b);
-                atomicAdd(&tile[idx], m);
-#pragma unroll
-                for (int d = 0; d < D; ++d) atomicAdd(&tile[(1 + d) * TNP + idx], mv[d]);
-              } else {
-                R4* g = gout + cell_index<D>(K.res, base[0] + a, base[1] + b, D == 3 ? base[2] + c : 0);
-                red_add_node(g, m, mv[0], mv[1], mv[2]);
-              }
-            }
-      }
-      __syncthreads();
-      // flush the tile: one vector reduction per touched node
-      for (int j = tid; j < TNP; j += CH) {
-        const R m = tile[j];
-        if (m == (R)0) continue;
-        int l0, l1, l2 = 0;
-        if (D == 3) {
-          l0 = j / G::XS;
-          const int r = j - l0 * G::XS;
-          l1 = r / T;
-          l2 = r - l1 * T;
-        } else {
-          l0 = j / T;
-          l1 = j - l0 * T;
-        }
-        const int g0 = o[0] + l0, g1 = o[1] + l1, g2 = o[2] + l2;
-        if (g0 < 0 || g0 >= K.res[0] || g1 < 0 || g1 >= K.res[1] || (D == 3 && (g2 < 0 || g2 >= K.res[2])))
-          continue;
-        red_add_node(gout + cell_index<D>(K.res, g0, g1, g2), m, tile[TNP + j], tile[2 * TNP + j],
-                     D == 3 ? tile[3 * TNP + j] : (R)0);
-      }
-    }
-    __syncthreads();
-  }
-  if (fl) atomicOr(A.status, fl);
-  if (nfall) atomicAdd(A.fallbacks, (unsigned long long)nfall);
-}
-
 // grid_op (mpm_solver.py:633-665) on `acc`; zero `clr`.
 template <int D, class R>
 __global__ void __launch_bounds__(256) k_grid(const SimK<R> K, void* acc_, void* clr_, int64_t ncell) {
-  using R4 = typename R4T<R>::type;
+  typedef typename R4T<R>::type R4;
   const int64_t c = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
   if (c >= ncell) return;
   R4* acc = reinterpret_cast<R4*>(acc_);
   R4* clr = reinterpret_cast<R4*>(clr_);
-  if (clr) clr[c] = R4{0, 0, 0, 0};
+  if (clr) {
+    R4 z;
+    z.x = z.y = z.z = z.w = 0;
+    clr[c] = z;
+  }
   if (!acc) return;
   int I[3];
   if (D == 3) {
@@ -721,7 +212,10 @@ __global__ void __launch_bounds__(256) k_grid(const SimK<R> K, void* acc_, void*
     if (I[k] < K.lb[k] && v[k] < (R)0) v[k] = 0;
     if (I[k] > K.ub[k] && v[k] > (R)0) v[k] = 0;
   }
-  acc[c] = R4{g.x, v[0], v[1], v[2]};
+  g.y = v[0];
+  g.z = v[1];
+  g.w = v[2];
+  acc[c] = g;
 }
 
 // decode records into particle order
@@ -795,7 +289,7 @@ struct SimBase {
 struct aq_sim {
   aq_params P;
   aq_layout L;
-  int W = 0, NS = 0, D = 0;
+  int W = 0, WS = 0, NS = 0, D = 0;
   int64_t n = 0;
   uint64_t* words[2] = {nullptr, nullptr};
   int32_t* pid[2] = {nullptr, nullptr};
@@ -818,6 +312,8 @@ struct aq_sim {
   bool sorted = false;
   int64_t launches = 0;
   int step_grid = 0;
+  void* jit_fn = nullptr;  // CUfunction of the layout-specialized k_step, or null
+  std::string jit_error;
   aq::SimBase* impl = nullptr;
   // kernel timing (aq_sim_profile_*): event pairs per kernel kind
   static constexpr int PROF_CAP = 8192;
@@ -844,6 +340,7 @@ struct SimImpl final : SimBase {
       K.clip_hi[d] = (R)(P.ub[d] * P.dx);
     }
     K.W = sim->W;
+    K.WS = sim->WS;
     K.friction = P.use_friction;
     K.bound_clip = P.use_bound_clip;
     K.n_mat = P.n_materials < 1 ? 1 : P.n_materials;
@@ -862,9 +359,8 @@ struct SimImpl final : SimBase {
   }
 
   size_t smem_bytes() const override {
-    size_t b = sizeof(R) * (D + 1) * Geo<D>::TNP + sizeof(int32_t) * CH;
-    b = (b + 15) & ~(size_t)15;
-    return b + sizeof(uint64_t) * (size_t)CH * s->W;
+    size_t b = sizeof(typename R4T<R>::type) * (NWARP + 1) * Geo<D>::TNP + sizeof(int32_t) * CH;
+    return b + sizeof(uint64_t) * (size_t)CH * s->WS;
   }
 
   int sort(cudaStream_t st) override {
@@ -893,6 +389,7 @@ struct SimImpl final : SimBase {
   int launch_step(int do_g2p, int do_p2g, void* gin, void* gout, cudaStream_t st) {
     aq_sim* S_ = s;
     StepArgs a;
+    memset(&a, 0, sizeof(a));
     a.words = S_->words[S_->cur];
     a.pid = S_->pid[S_->cur];
     a.items = S_->items;
@@ -909,8 +406,16 @@ struct SimImpl final : SimBase {
     a.ranges = S_->ranges_on;
     const bool prof = S_->prof_on && S_->prof_n[0] < aq_sim::PROF_CAP;
     if (prof) AQ_CUDA_TRY(cudaEventRecord(S_->prof_ev[0][2 * S_->prof_n[0]], st));
-    k_step<D, HF, HM, R><<<S_->step_grid, CH, smem_bytes(), st>>>(S_->L, K, a);
-    AQ_CUDA_TRY(cudaGetLastError());
+    if (S_->jit_fn) {
+      void* args[] = {(void*)&S_->L, (void*)&K, (void*)&a};
+      if (jit_launch(S_->jit_fn, S_->step_grid, CH, smem_bytes(), st, args) != AQ_OK) {
+        set_last_cuda_error(cudaErrorLaunchFailure, "cuLaunchKernel(k_step)");
+        return AQ_E_CUDA;
+      }
+    } else {
+      k_step<D, HF, HM, R, RtLayout><<<S_->step_grid, CH, smem_bytes(), st>>>(S_->L, K, a);
+      AQ_CUDA_TRY(cudaGetLastError());
+    }
     if (prof) AQ_CUDA_TRY(cudaEventRecord(S_->prof_ev[0][2 * S_->prof_n[0]++ + 1], st));
     S_->launches += 1;
     return AQ_OK;
@@ -973,9 +478,20 @@ static int make_impl(aq_sim* s) {
   if (!im) return AQ_E_NOMEM;
   s->impl = im;
   const size_t smem = im->smem_bytes();
-  AQ_CUDA_TRY(cudaFuncSetAttribute(k_step<D, HF, HM, R>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+  if (smem > 227 * 1024) return AQ_E_LIMIT;
   int occ = 0;
-  AQ_CUDA_TRY(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, k_step<D, HF, HM, R>, CH, smem));
+  if (s->P.jit) {
+    s->jit_fn = jit_k_step(D, HF, HM, sizeof(R) == 8, s->L, &s->jit_error);
+    if (s->jit_fn && (jit_set_smem(s->jit_fn, (int)smem) != AQ_OK || jit_occupancy(s->jit_fn, CH, smem, &occ) != AQ_OK)) {
+      s->jit_fn = nullptr;
+      s->jit_error = "cuFuncSetAttribute/occupancy failed";
+    }
+  }
+  if (!s->jit_fn) {
+    AQ_CUDA_TRY(cudaFuncSetAttribute(k_step<D, HF, HM, R, RtLayout>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                     (int)smem));
+    AQ_CUDA_TRY(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, k_step<D, HF, HM, R, RtLayout>, CH, smem));
+  }
   if (occ < 1) occ = 1;
   s->step_grid = occ * num_sms();
   return AQ_OK;
@@ -1038,6 +554,7 @@ int aq_sim_create(const aq_params* P, const aq_layout* L, aq_sim** out) {
   s->L = *L;
   s->D = D;
   s->W = L->n_words;
+  s->WS = L->n_words | 1;  // odd shared-memory stride: conflict-free 8-byte accesses
   s->NS = ns;
   s->n = P->n_particles;
   int nb[3] = {1, 1, 1};
@@ -1096,7 +613,6 @@ int aq_sim_create(const aq_params* P, const aq_layout* L, aq_sim** out) {
     rc = P->precision ? make_impl_d<3, double>(s) : make_impl_d<3, float>(s);
   else
     rc = P->precision ? make_impl_d<2, double>(s) : make_impl_d<2, float>(s);
-  if (rc == AQ_OK && s->impl->smem_bytes() > 227 * 1024) rc = AQ_E_LIMIT;
   if (rc == AQ_OK) {
     e = cudaDeviceSynchronize();
     if (e != cudaSuccess) {
@@ -1221,6 +737,12 @@ int aq_sim_status(aq_sim* s, uint32_t* h_flags, int64_t* h_fallbacks, int32_t cl
 int aq_sim_step_count(const aq_sim* s, int64_t* h_out) {
   if (!s || !h_out) return AQ_E_ARG;
   *h_out = s->step;
+  return AQ_OK;
+}
+
+int aq_sim_kernel_is_jit(const aq_sim* s, int32_t* h_out) {
+  if (!s || !h_out) return AQ_E_ARG;
+  *h_out = s->jit_fn ? 1 : 0;
   return AQ_OK;
 }
 

@@ -70,3 +70,6 @@ class MPMConfig(object):
         self.sort_interval = 16
         # seed of the dithering generator and of the random scene seeding
         self.seed = 0
+        # compile the substep kernel for the record layout with NVRTC
+        # (False: the generic kernel built into libaq.so)
+        self.jit = True

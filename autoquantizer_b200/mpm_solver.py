@@ -174,6 +174,7 @@ class MPMSolver:
         P.use_friction = int(self.use_friction)
         P.use_bound_clip = int(self.use_bound_clip)
         P.sort_interval = int(p.sort_interval)
+        P.jit = int(getattr(p, "jit", True))
         P.dx, P.dt, P.p_vol, P.p_mass, P.gravity = self.dx, self.dt, self.p_vol, self.p_mass, self.g
         P.n_particles = self.current_idx
         P.seed = int(p.seed)
@@ -342,6 +343,12 @@ class MPMSolver:
         _lib.check(_lib.lib().aq_sim_status(self._sim, C.byref(f), C.byref(fb), int(clear), _lib.stream_ptr()),
                    "aq_sim_status")
         return f.value, fb.value
+
+    def kernel_is_jit(self):
+        self._ensure_sim()
+        v = C.c_int32()
+        _lib.check(_lib.lib().aq_sim_kernel_is_jit(self._sim, C.byref(v)), "aq_sim_kernel_is_jit")
+        return bool(v.value)
 
     def launches(self):
         n = C.c_int64()

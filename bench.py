@@ -357,6 +357,7 @@ def run_ours(args, ws, rank, local):
                     "d2h_bytes_per_step": int(h_out.numel() * 8 + 8), "substeps_per_step": frame,
                     "steps": e2e_steps},
             "gpu_launches": int(launches),
+            "kernel_jit": q.kernel_is_jit(),
             "status": {"flags": flags, "tile_fallbacks": fallbacks},
             "clocks": ck,
         }

@@ -17,7 +17,17 @@
 #ifndef AQ_H_
 #define AQ_H_
 
+#ifdef __CUDACC_RTC__
+/* NVRTC (layout-specialized kernel compilation) has no libc headers */
+typedef signed char int8_t;
+typedef unsigned char uint8_t;
+typedef int int32_t;
+typedef unsigned int uint32_t;
+typedef long long int64_t;
+typedef unsigned long long uint64_t;
+#else
 #include <stdint.h>
+#endif
 
 #ifdef __cplusplus
 extern "C" {
@@ -90,6 +100,7 @@ typedef struct aq_layout {
   aq_slot slot[AQ_MAX_SLOTS];
 } aq_layout;
 
+#ifndef __CUDACC_RTC__ /* declarations only: NVRTC sees the types */
 /* Build a bit_pack record layout: fields are packed in place order into a
  * little-endian stream of 64-bit words; a field may straddle two words; a
  * shared exponent is placed right before the first member of its group.
@@ -119,6 +130,7 @@ int aq_encode(const aq_layout* h_layout, const void* d_values, int32_t values_f6
  * reconstruct_custom_float[_with_exponent] (codegen_llvm_quant.cpp:529-878). */
 int aq_decode(const aq_layout* h_layout, const uint64_t* d_words, void* d_values,
               int32_t values_f64, int64_t n, void* stream);
+#endif
 
 /* ---------------------------------------------------------------- simulator */
 
@@ -144,7 +156,8 @@ typedef struct aq_params {
   int32_t n_materials;
   int32_t use_friction, use_bound_clip;
   int32_t sort_interval; /* re-bin particles every k substeps (>=1) */
-  int32_t _pad;
+  int32_t jit;           /* 1: compile the substep kernel for this layout with
+                            NVRTC (default), 0: nvcc-built generic kernel */
   double dx, dt, p_vol, p_mass, gravity;
   double lb[3], ub[3]; /* grid-index walls, as MPMSolver.lb/ub */
   aq_material mat[AQ_MAX_MATERIALS];
@@ -152,6 +165,7 @@ typedef struct aq_params {
   uint64_t seed;
 } aq_params;
 
+#ifndef __CUDACC_RTC__
 typedef struct aq_sim aq_sim;
 
 /* Create a simulator for n_particles records of `layout`.  Record slots must
@@ -195,6 +209,10 @@ int aq_sim_ranges_get(aq_sim* sim, double* h_max, double* h_min, void* stream);
 int aq_sim_status(aq_sim* sim, uint32_t* h_flags, int64_t* h_fallbacks,
                   int32_t clear, void* stream);
 int aq_sim_step_count(const aq_sim* sim, int64_t* h_out);
+/* 1 if the substep kernel in use was compiled for this layout by NVRTC, 0 if
+ * it is the generic nvcc-built kernel.  No reference counterpart (Taichi
+ * always JIT-compiles, taichi_submission/taichi/backends/cuda/jit_cuda.cpp). */
+int aq_sim_kernel_is_jit(const aq_sim* sim, int32_t* h_out);
 /* Launch counters of this simulator's own kernels (for accounting). */
 int aq_sim_launches(const aq_sim* sim, int64_t* h_out);
 
@@ -215,6 +233,7 @@ int aq_state_error(const void* d_a, int32_t a_f64, const void* d_b, int32_t b_f6
 
 const char* aq_error_string(int32_t code);
 int32_t aq_abi_version(void);
+#endif /* __CUDACC_RTC__ */
 
 #ifdef __cplusplus
 }

@@ -102,7 +102,8 @@ def test_explicit_uniforms_bit_exact():
 def test_f32_values_input():
     rng = np.random.default_rng(9)
     rec = Q.BitPack()
-    rec.place(Q.fixed(21, True, 1.0, 0.0, "f32", True), Q.qfloat(12, 6), Q.qfloat(12, 6), shared_exponent=True)
+    rec.place(Q.fixed(21, True, 1.0, 0.0, "f32", True))
+    rec.place(Q.qfloat(12, 6), Q.qfloat(12, 6), shared_exponent=True)
     L = rec.build()
     Lo = O.build_layout(rec.spec_tuples(), False, True)
     vals = rng.uniform(-1, 1, (5000, 3)).astype(np.float32)
