@@ -206,13 +206,15 @@ __device__ __forceinline__ float dequant_shared(const aq_slot& S, uint32_t d_in,
 
 // --------------------------------------------------------------- records
 
-// Decode slots [0, NS) (predicated on n_slots) from record w.
-template <int NS, class R>
+// Decode slots [0, NS) (predicated on n_slots) from record w; slots whose
+// bit is clear in MASK are left untouched.
+template <int NS, class R, unsigned MASK = 0xffffffffu>
 __device__ __forceinline__ void decode_record(const aq_layout& L, const uint64_t* w, R (&vals)[NS]) {
   const bool f64 = L.compute_f64 != 0;
 #pragma unroll
   for (int s = 0; s < NS; ++s) {
     if (s >= L.n_slots) break;
+    if (!((MASK >> s) & 1u)) continue;
     const aq_slot& S = L.slot[s];
     const uint64_t code = get_bits(w, S.bit_offset, S.bits);
     R v;

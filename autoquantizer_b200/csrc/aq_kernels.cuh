@@ -203,7 +203,9 @@ __device__ __forceinline__ void polar_rot(const R* F, R* Rm) {
         diff += (nx - X[k]) * (nx - X[k]);
         X[k] = nx;
       }
-      if (diff < tol * tol) break;
+      // leave together: a converged lane's extra iteration changes X by
+      // rounding noise only, and the warp stays converged
+      if (__all_sync(__activemask(), diff < tol * tol)) break;
     }
 #pragma unroll
     for (int k = 0; k < 9; ++k) Rm[k] = X[k];
@@ -336,7 +338,16 @@ __global__ void __launch_bounds__(CH, 2) k_step(const __grid_constant__ aq_layou
     __syncthreads();
 
     R vals[NS];
-    if (active) decode_record<NS, R>(L, myrec, vals);
+    if (active) {
+      if (A.do_g2p) {  // G2P reads x, F|J and the material id; v and C are rewritten
+        constexpr unsigned XFM = ((1u << D) - 1u) | (((1u << S::NFJ) - 1u) << S::FJ) | (HM ? 1u << S::MAT : 0u);
+        decode_record<NS, R, XFM>(L, myrec, vals);
+#pragma unroll
+        for (int k = S::V; k < S::FJ; ++k) vals[k] = 0;
+      } else {
+        decode_record<NS, R>(L, myrec, vals);
+      }
+    }
 
     // ---------------------------------------------------------------- G2P
     if (A.do_g2p && active) {

@@ -37,8 +37,11 @@ __global__ void __launch_bounds__(256) k_bin(const __grid_constant__ aq_layout L
   constexpr int BS = Geo<D>::BS;
   int key;
   if (D == 3) {
+    // cells of a block ordered z fastest, then x, then y: eight consecutive
+    // cells then map to distinct 16-byte bank groups of the shared tiles
+    // (node stride 1 in z, XS = 4 mod 8 in x)
     const int blk = ((b[0] / BS) * K.nb[1] + b[1] / BS) * K.nb[2] + b[2] / BS;
-    key = blk * 64 + ((b[0] % BS) * BS + b[1] % BS) * BS + b[2] % BS;
+    key = blk * 64 + ((b[1] % BS) * BS + b[0] % BS) * BS + b[2] % BS;
   } else {
     const int blk = (b[0] / BS) * K.nb[1] + b[1] / BS;
     key = blk * 64 + (b[0] % BS) * BS + b[1] % BS;
@@ -48,8 +51,18 @@ __global__ void __launch_bounds__(256) k_bin(const __grid_constant__ aq_layout L
   if (fl) atomicOr(status, fl);
 }
 
+// A block of cnt records is cut into k = ceil(cnt/256) chunks of nearly
+// equal size (the first cnt % k chunks one record larger).
+__device__ __forceinline__ void chunk_of(int cnt, int local, int& c0, int& c1) {
+  const int k = (cnt + CH - 1) / CH, base = cnt / k, rem = cnt - base * k;
+  const int big = rem * (base + 1);
+  const int j = local < big ? local / (base + 1) : rem + (local - big) / base;
+  c0 = j * base + min(j, rem);
+  c1 = c0 + base + (j < rem ? 1 : 0);
+}
+
 // Move record i to its sorted position.  A block's records (in cell
-// order) are cut into chunks of at most 256, the work items.  Inside a chunk
+// order) are cut into chunks of at most 256 (chunk_of), the work items.  Inside a chunk
 // the order is slot-major: first the chunk's first record of every cell (in
 // cell order), then the second of every cell, and so on.  Consecutive
 // records, i.e. the lanes of a warp in k_step, are then in different cells
@@ -65,8 +78,9 @@ __global__ void __launch_bounds__(256) k_scatter(const uint64_t* __restrict__ wi
   const int64_t c0 = (int64_t)(key >> 6) * 64;
   const int64_t b0 = start[c0];
   const int64_t be = start[c0 + 64];
-  const int64_t cs = b0 + ((g - b0) / CH) * CH;  // chunk [cs, ce)
-  const int64_t ce = min(cs + CH, be);
+  int a, z;
+  chunk_of((int)(be - b0), (int)(g - b0), a, z);
+  const int64_t cs = b0 + a, ce = b0 + z;  // chunk [cs, ce)
   const int r = (int)(g - max((int64_t)start[key], cs));  // rank in its cell within the chunk
   const int myc = key & 63;
   int t = 0;
@@ -91,7 +105,12 @@ __global__ void k_items(const int32_t* __restrict__ start, int nblk, int4* __res
   if (cnt <= 0) return;
   const int k = (cnt + CH - 1) / CH;
   const int at = atomicAdd(n_items, k);
-  for (int j = 0; j < k; ++j) items[at + j] = make_int4(b, s + j * CH, min(CH, cnt - j * CH), 0);
+  for (int j = 0, c0 = 0; j < k; ++j) {
+    int a, z;
+    chunk_of(cnt, c0, a, z);
+    items[at + j] = make_int4(b, s + a, z - a, 0);
+    c0 = z;
+  }
 }
 
 // Exclusive scan of n int32 counts into out[0..n] (out[n] = total), in
