@@ -28,7 +28,7 @@ EXPORTS = [
     "aq_sim_get_state", "aq_sim_set_words", "aq_sim_get_words", "aq_sim_substeps", "aq_sim_loss",
     "aq_sim_ranges_enable", "aq_sim_ranges_get", "aq_sim_status", "aq_sim_step_count", "aq_sim_launches",
     "aq_state_error", "aq_error_string", "aq_abi_version", "aq_sim_profile_enable", "aq_sim_profile_get",
-    "aq_sim_kernel_is_jit",
+    "aq_sim_kernel_is_jit", "aq_adjoint_create", "aq_adjoint_destroy", "aq_adjoint_forward", "aq_adjoint_backward",
 ]
 
 
@@ -105,6 +105,10 @@ def lib():
                            C.c_int),
         "aq_sim_profile_enable": ([vp, i32], C.c_int),
         "aq_sim_profile_get": ([vp, i32, C.POINTER(C.c_double), C.POINTER(C.c_int64)], C.c_int),
+        "aq_adjoint_create": ([C.POINTER(Params), C.POINTER(vp)], C.c_int),
+        "aq_adjoint_destroy": ([vp], C.c_int),
+        "aq_adjoint_forward": ([vp, vp, i32, i32, vp, vp], C.c_int),
+        "aq_adjoint_backward": ([vp, vp, vp, C.POINTER(C.c_double), vp], C.c_int),
         "aq_error_string": ([i32], C.c_char_p),
         "aq_abi_version": ([], i32),
     }

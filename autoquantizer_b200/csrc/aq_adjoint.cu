@@ -1,0 +1,813 @@
+// libaq.so: hand-written adjoint of the MLS-MPM substep with segment
+// checkpointing, for the quantization sensitivities of the reference's
+// autodiff pass (MPMSolver.run_forward_with_ad_nlogn, mpm_exps/engine/
+// mpm_solver.py:1093-1302; Taichi's generated p2g.grad / grid_op.grad /
+// g2p.grad, taichi_submission/taichi/transforms/auto_diff.cpp).
+//
+// State: n x NS unquantized values per particle in the record slot order
+// x(d), v(d), C(d*d), F(d*d) | J; one material (fluid, or the reference's
+// elastic law).  Forward substep s -> s' (same formulas as k_step):
+//   P2G  m_i  = sum_p w_ip m,   P_i = sum_p w_ip (m v_p + A_p dpos_ip),
+//        A_p = k sigma(F_p) + m C_p,  k = -dt p_vol 4/dx^2,
+//        dpos_ip = x_i - x_p,  w_ip = prod_d N(x_pd/dx - i_d)
+//   grid v_i = P_i / (m_i + 1e-10) - dt g e_y, then wall masks per component
+//   G2P  v'_p = sum_i w_ip v_i,  C'_p = 4/dx^2 sum_i w_ip v_i dpos_ip^T,
+//        x'_p = x_p + dt v'_p,  F'_p = (I + dt C'_p) F_p  (J'_p = (1+dt tr C'_p) J_p)
+// Reverse (bars are adjoints), per substep:
+//   G2P^T   Fbar += (I+dt C')^T F'bar;  C'bar += dt F'bar F^T;
+//           v'bar += dt x'bar;  xbar += x'bar;
+//           vbar_i += w v'bar + (4/dx^2) w C'bar dpos;
+//           wbar_ip = v_i.v'bar + (4/dx^2) v_i^T C'bar dpos;
+//           xbar -= (4/dx^2) w C'bar^T v_i  (through dpos);  xbar += wbar grad_x w
+//   grid^T  masked components get no gradient; Pbar = vbar/(m+eps),
+//           mbar = -vbar.P/(m+eps)^2
+//   P2G^T   vbar += w m Pbar_i;  Abar += w Pbar_i dpos^T;
+//           wbar = m mbar_i + Pbar_i.(m v + A dpos);  xbar -= w A^T Pbar_i;
+//           xbar += wbar grad_x w;  Cbar += m Abar;  sigma_bar = k Abar;
+//           Fbar += dsigma/dF^T sigma_bar  (fluid: Jbar += la tr(sigma_bar);
+//           2D: fixed-corotated with the closed-form rotation derivative;
+//           3D reference law: mu (sbar + sbar^T) F + la sum(sbar) F^-T)
+// The derivative of the B-spline base index is zero almost everywhere.
+//
+// Sensitivities: sens[s] = sum over substeps t = 1..T-1 and particles of
+// (dL/d state_t[s])^2 in f64, the quantity accu_grad accumulates
+// (mpm_solver.py:1232-1271; the initial and the final state are not
+// accumulated there either, :1190-1196).
+#include <math.h>
+#include <string.h>
+
+#include <algorithm>
+#include <new>
+#include <vector>
+
+#include "aq_common.cuh"
+#include "aq_kernels.cuh"
+
+namespace aq {
+
+template <class R>
+struct AdK {
+  int res[3], D, NS, HF, mat;
+  R inv_dx, dx, dt, p_mass, kst, four_inv_dx2, grav, mu, lam;
+  double lb[3], ub[3];
+  int bound_clip, friction;
+  R clip_lo[3], clip_hi[3];
+};
+
+template <int D>
+__device__ __forceinline__ int64_t ad_cell(const int (&res)[3], const int* I) {
+  return D == 3 ? ((int64_t)I[0] * res[1] + I[1]) * res[2] + I[2] : (int64_t)I[0] * res[1] + I[1];
+}
+
+template <int D, class R>
+__device__ __forceinline__ void ad_weights(const R* x, const AdK<R>& K, int* base, R* fx, R (&w)[3][3],
+                                           R (&dw)[3][3]) {
+#pragma unroll
+  for (int d = 0; d < D; ++d) {
+    R t = x[d] * K.inv_dx - (R)0.5;
+    int b = (int)floor(t);
+    b = min(max(b, 0), K.res[d] - 3);
+    base[d] = b;
+    fx[d] = x[d] * K.inv_dx - (R)b;
+    w[0][d] = (R)0.5 * ((R)1.5 - fx[d]) * ((R)1.5 - fx[d]);
+    w[1][d] = (R)0.75 - (fx[d] - (R)1) * (fx[d] - (R)1);
+    w[2][d] = (R)0.5 * (fx[d] - (R)0.5) * (fx[d] - (R)0.5);
+    // dN/dx (per unit x: chain with inv_dx)
+    dw[0][d] = -((R)1.5 - fx[d]) * K.inv_dx;
+    dw[1][d] = (R)-2 * (fx[d] - (R)1) * K.inv_dx;
+    dw[2][d] = (fx[d] - (R)0.5) * K.inv_dx;
+  }
+}
+
+template <int D, class R>
+__device__ __forceinline__ R inv_det_cof(const R* F, R* cof) {  // cofactor matrix (dJ/dF) and J
+  if (D == 2) {
+    cof[0] = F[3];
+    cof[1] = -F[2];
+    cof[2] = -F[1];
+    cof[3] = F[0];
+    return F[0] * F[3] - F[1] * F[2];
+  }
+  cof[0] = F[4] * F[8] - F[5] * F[7];
+  cof[1] = F[5] * F[6] - F[3] * F[8];
+  cof[2] = F[3] * F[7] - F[4] * F[6];
+  cof[3] = F[2] * F[7] - F[1] * F[8];
+  cof[4] = F[0] * F[8] - F[2] * F[6];
+  cof[5] = F[1] * F[6] - F[0] * F[7];
+  cof[6] = F[1] * F[5] - F[2] * F[4];
+  cof[7] = F[2] * F[3] - F[0] * F[5];
+  cof[8] = F[0] * F[4] - F[1] * F[3];
+  return F[0] * cof[0] + F[1] * cof[1] + F[2] * cof[2];
+}
+
+// stress sigma(F) of the reference materials
+template <int D, bool HF, class R>
+__device__ __forceinline__ void ad_sigma(const AdK<R>& K, const R* s, R* sig) {
+  typedef Sch<D, HF, false> S;
+#pragma unroll
+  for (int k = 0; k < D * D; ++k) sig[k] = 0;
+  if (!HF) {
+#pragma unroll
+    for (int d = 0; d < D; ++d) sig[d * D + d] = K.lam * (s[S::FJ] - (R)1);
+    return;
+  }
+  const R* F = s + S::FJ;
+  R cof[9];
+  const R J = inv_det_cof<D, R>(F, cof);
+  if (K.mat == AQ_MAT_FLUID) {
+#pragma unroll
+    for (int d = 0; d < D; ++d) sig[d * D + d] = K.lam * (J - (R)1);
+    return;
+  }
+  if (D == 2) {
+    R Rm[4];
+    polar_rot<2, R>(F, Rm);
+#pragma unroll
+    for (int i = 0; i < 2; ++i)
+#pragma unroll
+      for (int j = 0; j < 2; ++j) {
+        R a = 0;
+#pragma unroll
+        for (int k = 0; k < 2; ++k) a += (F[i * 2 + k] - Rm[i * 2 + k]) * F[j * 2 + k];
+        sig[i * 2 + j] = (R)2 * K.mu * a + (i == j ? K.lam * J * (J - (R)1) : (R)0);
+      }
+  } else {
+    const R lj = K.lam * log(J);
+#pragma unroll
+    for (int i = 0; i < 3; ++i)
+#pragma unroll
+      for (int j = 0; j < 3; ++j) {
+        R a = 0;
+#pragma unroll
+        for (int k = 0; k < 3; ++k) a += F[i * 3 + k] * F[j * 3 + k];
+        sig[i * 3 + j] = K.mu * (a - (i == j ? (R)1 : (R)0)) + lj;
+      }
+  }
+}
+
+// Fbar (or Jbar) += dsigma/dF^T sbar
+template <int D, bool HF, class R>
+__device__ __forceinline__ void ad_sigma_bwd(const AdK<R>& K, const R* s, const R* sb, R* gb) {
+  typedef Sch<D, HF, false> S;
+  R tr = 0, sum = 0;
+#pragma unroll
+  for (int d = 0; d < D; ++d) tr += sb[d * D + d];
+#pragma unroll
+  for (int k = 0; k < D * D; ++k) sum += sb[k];
+  if (!HF) {
+    gb[S::FJ] += K.lam * tr;
+    return;
+  }
+  const R* F = s + S::FJ;
+  R* Fb = gb + S::FJ;
+  R cof[9];
+  const R J = inv_det_cof<D, R>(F, cof);
+  if (K.mat == AQ_MAT_FLUID) {
+#pragma unroll
+    for (int k = 0; k < D * D; ++k) Fb[k] += K.lam * tr * cof[k];
+    return;
+  }
+  if (D == 2) {
+    // sigma = 2 mu (F - R) F^T + la J (J-1) I,  R = [[c,-s],[s,c]]
+    R Rm[4];
+    polar_rot<2, R>(F, Rm);
+    R G[4], Gb[4];
+#pragma unroll
+    for (int k = 0; k < 4; ++k) G[k] = F[k] - Rm[k];
+    // Gbar = 2 mu sbar F ; Fbar += 2 mu sbar^T G
+#pragma unroll
+    for (int i = 0; i < 2; ++i)
+#pragma unroll
+      for (int j = 0; j < 2; ++j) {
+        R a = 0, b = 0;
+#pragma unroll
+        for (int k = 0; k < 2; ++k) {
+          a += sb[i * 2 + k] * F[k * 2 + j];
+          b += sb[k * 2 + i] * G[k * 2 + j];
+        }
+        Gb[i * 2 + j] = (R)2 * K.mu * a;
+        Fb[i * 2 + j] += (R)2 * K.mu * b + Gb[i * 2 + j];
+      }
+    const R Jb = K.lam * ((R)2 * J - (R)1) * tr;
+#pragma unroll
+    for (int k = 0; k < 4; ++k) Fb[k] += Jb * cof[k];
+    // Rbar = -Gbar ; c = x/r, s = y/r with x = F00+F11, y = F10-F01
+    const R cb = -(Gb[0] + Gb[3]);
+    const R sbb = -(-Gb[1] + Gb[2]);
+    const R x = F[0] + F[3], y = F[2] - F[1];
+    const R r2 = x * x + y * y, r = sqrt(r2), r3 = r2 * r;
+    const R xb = (cb * y * y - sbb * x * y) / r3;
+    const R yb = (-cb * x * y + sbb * x * x) / r3;
+    Fb[0] += xb;
+    Fb[3] += xb;
+    Fb[2] += yb;
+    Fb[1] -= yb;
+  } else {
+    // sigma = mu (F F^T - I) + la log J (every entry)
+#pragma unroll
+    for (int i = 0; i < 3; ++i)
+#pragma unroll
+      for (int j = 0; j < 3; ++j) {
+        R a = 0;
+#pragma unroll
+        for (int k = 0; k < 3; ++k) a += (sb[i * 3 + k] + sb[k * 3 + i]) * F[k * 3 + j];
+        Fb[i * 3 + j] += K.mu * a + K.lam * sum * cof[i * 3 + j] / J;
+      }
+  }
+}
+
+template <int D>
+__device__ __forceinline__ void offs(int o, int* off) {
+  off[0] = D == 3 ? o / 9 : o / 3;
+  off[1] = D == 3 ? (o / 3) % 3 : o % 3;
+  off[2] = D == 3 ? o % 3 : 0;
+}
+
+// ------------------------------------------------------------- forward
+
+template <int D, bool HF, class R>
+__global__ void __launch_bounds__(128) k_ad_p2g(const AdK<R> K, const R* __restrict__ st, int64_t n,
+                                                R* __restrict__ grid) {
+  typedef Sch<D, HF, false> S;
+  const int64_t p = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (p >= n) return;
+  const R* s = st + p * K.NS;
+  int base[3];
+  R fx[3], w[3][3], dw[3][3];
+  ad_weights<D, R>(s + S::X, K, base, fx, w, dw);
+  R sig[9], A[9];
+  ad_sigma<D, HF, R>(K, s, sig);
+#pragma unroll
+  for (int k = 0; k < D * D; ++k) A[k] = K.kst * sig[k] + K.p_mass * s[S::C + k];
+  for (int o = 0; o < (D == 3 ? 27 : 9); ++o) {
+    int off[3], I[3];
+    offs<D>(o, off);
+    R wt = 1, dpos[3];
+#pragma unroll
+    for (int d = 0; d < D; ++d) {
+      wt *= w[off[d]][d];
+      dpos[d] = ((R)off[d] - fx[d]) * K.dx;
+      I[d] = base[d] + off[d];
+    }
+    R* g = grid + 4 * ad_cell<D>(K.res, I);
+    atomicAdd(g, wt * K.p_mass);
+#pragma unroll
+    for (int d = 0; d < D; ++d) {
+      R a = K.p_mass * s[S::V + d];
+#pragma unroll
+      for (int e = 0; e < D; ++e) a += A[d * D + e] * dpos[e];
+      atomicAdd(g + 1 + d, wt * a);
+    }
+  }
+}
+
+// wall mask of component k at node I given the velocity sign (grid_op)
+template <class R>
+__device__ __forceinline__ bool ad_wall(const AdK<R>& K, const int* I, int k, R vk) {
+  return (I[k] < K.lb[k] && vk < (R)0) || (I[k] > K.ub[k] && vk > (R)0);
+}
+
+template <int D, class R>
+__global__ void __launch_bounds__(256) k_ad_grid(const AdK<R> K, const R* __restrict__ grid, R* __restrict__ gv,
+                                                 int64_t ncell) {
+  const int64_t c = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (c >= ncell) return;
+  int I[3] = {0, 0, 0};
+  if (D == 3) {
+    I[2] = (int)(c % K.res[2]);
+    I[1] = (int)((c / K.res[2]) % K.res[1]);
+    I[0] = (int)(c / ((int64_t)K.res[2] * K.res[1]));
+  } else {
+    I[1] = (int)(c % K.res[1]);
+    I[0] = (int)(c / K.res[1]);
+  }
+  const R* g = grid + 4 * c;
+  const R inv_m = (R)1 / (g[0] + (R)1e-10);
+  R v[3] = {0, 0, 0};
+#pragma unroll
+  for (int d = 0; d < D; ++d) v[d] = inv_m * g[1 + d];
+  v[1] -= K.dt * K.grav;
+#pragma unroll
+  for (int k = 0; k < D; ++k)
+    if (ad_wall<R>(K, I, k, v[k])) v[k] = 0;
+#pragma unroll
+  for (int d = 0; d < 3; ++d) gv[4 * c + d] = d < D ? v[d] : (R)0;
+  gv[4 * c + 3] = 0;
+}
+
+template <int D, bool HF, class R>
+__global__ void __launch_bounds__(128) k_ad_g2p(const AdK<R> K, const R* __restrict__ st, const R* __restrict__ gv,
+                                                R* __restrict__ out, int64_t n) {
+  typedef Sch<D, HF, false> S;
+  const int64_t p = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (p >= n) return;
+  const R* s = st + p * K.NS;
+  R* so = out + p * K.NS;
+  int base[3];
+  R fx[3], w[3][3], dw[3][3];
+  ad_weights<D, R>(s + S::X, K, base, fx, w, dw);
+  R nv[3] = {0, 0, 0}, nC[9] = {0, 0, 0, 0, 0, 0, 0, 0, 0};
+  for (int o = 0; o < (D == 3 ? 27 : 9); ++o) {
+    int off[3], I[3];
+    offs<D>(o, off);
+    R wt = 1, dpos[3];
+#pragma unroll
+    for (int d = 0; d < D; ++d) {
+      wt *= w[off[d]][d];
+      dpos[d] = ((R)off[d] - fx[d]) * K.dx;
+      I[d] = base[d] + off[d];
+    }
+    const R* g = gv + 4 * ad_cell<D>(K.res, I);
+#pragma unroll
+    for (int d = 0; d < D; ++d) {
+      nv[d] += wt * g[d];
+#pragma unroll
+      for (int e = 0; e < D; ++e) nC[d * D + e] += K.four_inv_dx2 * wt * g[d] * dpos[e];
+    }
+  }
+#pragma unroll
+  for (int d = 0; d < D; ++d) {
+    so[S::X + d] = s[S::X + d] + K.dt * nv[d];
+    so[S::V + d] = nv[d];
+  }
+#pragma unroll
+  for (int k = 0; k < D * D; ++k) so[S::C + k] = nC[k];
+  if (HF) {
+#pragma unroll
+    for (int i = 0; i < D; ++i)
+#pragma unroll
+      for (int j = 0; j < D; ++j) {
+        R a = 0;
+#pragma unroll
+        for (int k = 0; k < D; ++k) a += ((i == k ? (R)1 : (R)0) + K.dt * nC[i * D + k]) * s[S::FJ + k * D + j];
+        so[S::FJ + i * D + j] = a;
+      }
+  } else {
+    R tr = 0;
+#pragma unroll
+    for (int d = 0; d < D; ++d) tr += nC[d * D + d];
+    so[S::FJ] = ((R)1 + K.dt * tr) * s[S::FJ];
+  }
+}
+
+// ------------------------------------------------------------- reverse
+
+// G2P^T: from the adjoint of the new state (ab_out) to the adjoint of the
+// old state's x and F|J (ab_in, overwritten) and the grid velocity adjoint
+// (gvb, accumulated).
+template <int D, bool HF, class R>
+__global__ void __launch_bounds__(128) k_ad_g2p_bwd(const AdK<R> K, const R* __restrict__ st,
+                                                    const R* __restrict__ gv, const R* __restrict__ ab_out,
+                                                    R* __restrict__ ab_in, R* __restrict__ gvb, int64_t n) {
+  typedef Sch<D, HF, false> S;
+  const int64_t p = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (p >= n) return;
+  const R* s = st + p * K.NS;
+  const R* bo = ab_out + p * K.NS;
+  R* bi = ab_in + p * K.NS;
+  int base[3];
+  R fx[3], w[3][3], dw[3][3];
+  ad_weights<D, R>(s + S::X, K, base, fx, w, dw);
+  // recompute new C (needed for F' = (I + dt C') F)
+  R nC[9] = {0, 0, 0, 0, 0, 0, 0, 0, 0};
+  for (int o = 0; o < (D == 3 ? 27 : 9); ++o) {
+    int off[3], I[3];
+    offs<D>(o, off);
+    R wt = 1, dpos[3];
+#pragma unroll
+    for (int d = 0; d < D; ++d) {
+      wt *= w[off[d]][d];
+      dpos[d] = ((R)off[d] - fx[d]) * K.dx;
+      I[d] = base[d] + off[d];
+    }
+    const R* g = gv + 4 * ad_cell<D>(K.res, I);
+#pragma unroll
+    for (int d = 0; d < D; ++d)
+#pragma unroll
+      for (int e = 0; e < D; ++e) nC[d * D + e] += K.four_inv_dx2 * wt * g[d] * dpos[e];
+  }
+  R xb[3] = {0, 0, 0}, vpb[3] = {0, 0, 0}, Cpb[9];
+#pragma unroll
+  for (int k = 0; k < D * D; ++k) Cpb[k] = bo[S::C + k];
+  R FJb[9];
+  if (HF) {
+    // F' = (I + dt C') F
+#pragma unroll
+    for (int i = 0; i < D; ++i)
+#pragma unroll
+      for (int j = 0; j < D; ++j) {
+        R a = 0, c = 0;
+#pragma unroll
+        for (int k = 0; k < D; ++k) {
+          a += ((k == i ? (R)1 : (R)0) + K.dt * nC[k * D + i]) * bo[S::FJ + k * D + j];  // (I+dtC')^T F'bar
+          c += bo[S::FJ + i * D + k] * s[S::FJ + j * D + k];                            // F'bar F^T
+        }
+        FJb[i * D + j] = a;
+        Cpb[i * D + j] += K.dt * c;
+      }
+  } else {
+    R tr = 0;
+#pragma unroll
+    for (int d = 0; d < D; ++d) tr += nC[d * D + d];
+    FJb[0] = ((R)1 + K.dt * tr) * bo[S::FJ];
+    const R trb = K.dt * s[S::FJ] * bo[S::FJ];
+#pragma unroll
+    for (int d = 0; d < D; ++d) Cpb[d * D + d] += trb;
+  }
+#pragma unroll
+  for (int d = 0; d < D; ++d) {
+    xb[d] = bo[S::X + d];
+    vpb[d] = bo[S::V + d] + K.dt * bo[S::X + d];
+  }
+  for (int o = 0; o < (D == 3 ? 27 : 9); ++o) {
+    int off[3], I[3];
+    offs<D>(o, off);
+    R wt = 1, dpos[3];
+#pragma unroll
+    for (int d = 0; d < D; ++d) {
+      wt *= w[off[d]][d];
+      dpos[d] = ((R)off[d] - fx[d]) * K.dx;
+      I[d] = base[d] + off[d];
+    }
+    const int64_t cell = ad_cell<D>(K.res, I);
+    const R* g = gv + 4 * cell;
+    R wb = 0;
+#pragma unroll
+    for (int d = 0; d < D; ++d) {
+      R cd = 0;  // (C'bar dpos)_d
+#pragma unroll
+      for (int e = 0; e < D; ++e) cd += Cpb[d * D + e] * dpos[e];
+      const R vb = wt * (vpb[d] + K.four_inv_dx2 * cd);
+      atomicAdd(gvb + 4 * cell + d, vb);
+      wb += g[d] * (vpb[d] + K.four_inv_dx2 * cd);
+    }
+    // through dpos = x_i - x_p: xbar -= 4/dx^2 w C'bar^T v_i
+#pragma unroll
+    for (int e = 0; e < D; ++e) {
+      R a = 0;
+#pragma unroll
+      for (int d = 0; d < D; ++d) a += Cpb[d * D + e] * g[d];
+      xb[e] -= K.four_inv_dx2 * wt * a;
+    }
+    // through w
+#pragma unroll
+    for (int d = 0; d < D; ++d) {
+      R gw = dw[off[d]][d];
+#pragma unroll
+      for (int e = 0; e < D; ++e)
+        if (e != d) gw *= w[off[e]][e];
+      xb[d] += wb * gw;
+    }
+  }
+  for (int k = 0; k < K.NS; ++k) bi[k] = 0;
+#pragma unroll
+  for (int d = 0; d < D; ++d) bi[S::X + d] = xb[d];
+  if (HF) {
+#pragma unroll
+    for (int k = 0; k < D * D; ++k) bi[S::FJ + k] = FJb[k];
+  } else {
+    bi[S::FJ] = FJb[0];
+  }
+}
+
+// grid^T: from the velocity adjoint to the (m, P) adjoint, in place in gvb
+template <int D, class R>
+__global__ void __launch_bounds__(256) k_ad_grid_bwd(const AdK<R> K, const R* __restrict__ grid,
+                                                     R* __restrict__ gvb, int64_t ncell) {
+  const int64_t c = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (c >= ncell) return;
+  int I[3] = {0, 0, 0};
+  if (D == 3) {
+    I[2] = (int)(c % K.res[2]);
+    I[1] = (int)((c / K.res[2]) % K.res[1]);
+    I[0] = (int)(c / ((int64_t)K.res[2] * K.res[1]));
+  } else {
+    I[1] = (int)(c % K.res[1]);
+    I[0] = (int)(c / K.res[1]);
+  }
+  const R* g = grid + 4 * c;
+  const R me = g[0] + (R)1e-10;
+  const R inv_m = (R)1 / me;
+  R v[3] = {0, 0, 0};
+#pragma unroll
+  for (int d = 0; d < D; ++d) v[d] = inv_m * g[1 + d];
+  v[1] -= K.dt * K.grav;
+  R mb = 0, Pb[3] = {0, 0, 0};
+#pragma unroll
+  for (int d = 0; d < D; ++d) {
+    R vb = gvb[4 * c + d];
+    if (ad_wall<R>(K, I, d, v[d])) vb = 0;
+    Pb[d] = vb * inv_m;
+    mb -= vb * g[1 + d] * inv_m * inv_m;
+  }
+  gvb[4 * c + 0] = mb;
+#pragma unroll
+  for (int d = 0; d < 3; ++d) gvb[4 * c + 1 + d] = d < D ? Pb[d] : (R)0;
+}
+
+// P2G^T: adds the old-state adjoint through P2G into ab_in
+template <int D, bool HF, class R>
+__global__ void __launch_bounds__(128) k_ad_p2g_bwd(const AdK<R> K, const R* __restrict__ st,
+                                                    const R* __restrict__ gb, R* __restrict__ ab_in, int64_t n) {
+  typedef Sch<D, HF, false> S;
+  const int64_t p = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (p >= n) return;
+  const R* s = st + p * K.NS;
+  R* bi = ab_in + p * K.NS;
+  int base[3];
+  R fx[3], w[3][3], dw[3][3];
+  ad_weights<D, R>(s + S::X, K, base, fx, w, dw);
+  R sig[9], A[9];
+  ad_sigma<D, HF, R>(K, s, sig);
+#pragma unroll
+  for (int k = 0; k < D * D; ++k) A[k] = K.kst * sig[k] + K.p_mass * s[S::C + k];
+  R xb[3] = {0, 0, 0}, vb[3] = {0, 0, 0}, Ab[9] = {0, 0, 0, 0, 0, 0, 0, 0, 0};
+  for (int o = 0; o < (D == 3 ? 27 : 9); ++o) {
+    int off[3], I[3];
+    offs<D>(o, off);
+    R wt = 1, dpos[3];
+#pragma unroll
+    for (int d = 0; d < D; ++d) {
+      wt *= w[off[d]][d];
+      dpos[d] = ((R)off[d] - fx[d]) * K.dx;
+      I[d] = base[d] + off[d];
+    }
+    const R* g = gb + 4 * ad_cell<D>(K.res, I);
+    const R mb = g[0];
+    R wb = K.p_mass * mb;
+#pragma unroll
+    for (int d = 0; d < D; ++d) {
+      const R Pb = g[1 + d];
+      R a = K.p_mass * s[S::V + d];
+#pragma unroll
+      for (int e = 0; e < D; ++e) a += A[d * D + e] * dpos[e];
+      wb += Pb * a;
+      vb[d] += wt * K.p_mass * Pb;
+#pragma unroll
+      for (int e = 0; e < D; ++e) {
+        Ab[d * D + e] += wt * Pb * dpos[e];
+        xb[e] -= wt * A[d * D + e] * Pb;  // through dpos = x_i - x_p
+      }
+    }
+#pragma unroll
+    for (int d = 0; d < D; ++d) {
+      R gw = dw[off[d]][d];
+#pragma unroll
+      for (int e = 0; e < D; ++e)
+        if (e != d) gw *= w[off[e]][e];
+      xb[d] += wb * gw;
+    }
+  }
+  R sb[9];
+#pragma unroll
+  for (int k = 0; k < D * D; ++k) {
+    bi[S::C + k] += K.p_mass * Ab[k];
+    sb[k] = K.kst * Ab[k];
+  }
+#pragma unroll
+  for (int d = 0; d < D; ++d) {
+    bi[S::X + d] += xb[d];
+    bi[S::V + d] += vb[d];
+  }
+  ad_sigma_bwd<D, HF, R>(K, s, sb, bi);
+}
+
+template <class R>
+__global__ void k_ad_accum(const R* __restrict__ ab, int64_t n, int ns, double* __restrict__ sens) {
+  extern __shared__ double shs[];
+  for (int s = threadIdx.x; s < ns; s += blockDim.x) shs[s] = 0;
+  __syncthreads();
+  for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n * ns; i += (int64_t)gridDim.x * blockDim.x) {
+    const double v = (double)ab[i];
+    atomicAdd(&shs[i % ns], v * v);
+  }
+  __syncthreads();
+  for (int s = threadIdx.x; s < ns; s += blockDim.x) atomicAdd(&sens[s], shs[s]);
+}
+
+// --------------------------------------------------------------- host
+
+struct AdBase {
+  virtual ~AdBase() {}
+  virtual int step(const void* in, void* out, cudaStream_t st) = 0;
+  virtual int step_bwd(const void* s_in, const void* ab_out, void* ab_in, cudaStream_t st) = 0;
+  virtual int accum(const void* ab, double* sens, cudaStream_t st) = 0;
+};
+
+}  // namespace aq
+
+struct aq_adjoint {
+  aq_params P;
+  int D = 0, NS = 0;
+  int64_t n = 0, ncell = 0;
+  size_t rsz = 4;
+  void* grid = nullptr;  // (m, P) per node
+  void* gv = nullptr;    // grid velocity per node
+  void* gvb = nullptr;   // velocity adjoint, then (m, P) adjoint
+  std::vector<void*> ckpt;  // states at multiples of the checkpoint interval
+  std::vector<void*> seg;   // states of one segment (recomputed)
+  int T = 0, every = 0;
+  double* dsens = nullptr;
+  aq::AdBase* impl = nullptr;
+};
+
+namespace aq {
+
+template <int D, bool HF, class R>
+struct AdImpl final : AdBase {
+  aq_adjoint* a;
+  AdK<R> K;
+  explicit AdImpl(aq_adjoint* adj) : a(adj) {
+    const aq_params& P = adj->P;
+    memset(&K, 0, sizeof(K));
+    for (int d = 0; d < 3; ++d) {
+      K.res[d] = d < D ? P.res[d] : 1;
+      K.lb[d] = P.lb[d];
+      K.ub[d] = P.ub[d];
+    }
+    K.D = D;
+    K.NS = adj->NS;
+    K.HF = HF;
+    K.mat = P.mat[0].kind;
+    K.inv_dx = (R)(1.0 / P.dx);
+    K.dx = (R)P.dx;
+    K.dt = (R)P.dt;
+    K.p_mass = (R)P.p_mass;
+    K.kst = (R)(-(P.dt * P.p_vol * 4.0 * (1.0 / P.dx) * (1.0 / P.dx)));
+    K.four_inv_dx2 = (R)(4.0 / (P.dx * P.dx));
+    K.grav = (R)P.gravity;
+    K.mu = (R)P.mat[0].mu;
+    K.lam = (R)P.mat[0].lam;
+  }
+  int step(const void* in, void* out, cudaStream_t st) override {
+    const size_t gbytes = sizeof(R) * 4 * a->ncell;
+    AQ_CUDA_TRY(cudaMemsetAsync(a->grid, 0, gbytes, st));
+    k_ad_p2g<D, HF, R><<<grid_for(a->n, 128), 128, 0, st>>>(K, (const R*)in, a->n, (R*)a->grid);
+    k_ad_grid<D, R><<<grid_for(a->ncell, 256), 256, 0, st>>>(K, (const R*)a->grid, (R*)a->gv, a->ncell);
+    k_ad_g2p<D, HF, R><<<grid_for(a->n, 128), 128, 0, st>>>(K, (const R*)in, (const R*)a->gv, (R*)out, a->n);
+    AQ_CUDA_TRY(cudaGetLastError());
+    return AQ_OK;
+  }
+  int step_bwd(const void* s_in, const void* ab_out, void* ab_in, cudaStream_t st) override {
+    const size_t gbytes = sizeof(R) * 4 * a->ncell;
+    // recompute the grid of this substep
+    AQ_CUDA_TRY(cudaMemsetAsync(a->grid, 0, gbytes, st));
+    k_ad_p2g<D, HF, R><<<grid_for(a->n, 128), 128, 0, st>>>(K, (const R*)s_in, a->n, (R*)a->grid);
+    k_ad_grid<D, R><<<grid_for(a->ncell, 256), 256, 0, st>>>(K, (const R*)a->grid, (R*)a->gv, a->ncell);
+    AQ_CUDA_TRY(cudaMemsetAsync(a->gvb, 0, gbytes, st));
+    k_ad_g2p_bwd<D, HF, R><<<grid_for(a->n, 128), 128, 0, st>>>(K, (const R*)s_in, (const R*)a->gv,
+                                                                 (const R*)ab_out, (R*)ab_in, (R*)a->gvb, a->n);
+    k_ad_grid_bwd<D, R><<<grid_for(a->ncell, 256), 256, 0, st>>>(K, (const R*)a->grid, (R*)a->gvb, a->ncell);
+    k_ad_p2g_bwd<D, HF, R><<<grid_for(a->n, 128), 128, 0, st>>>(K, (const R*)s_in, (const R*)a->gvb, (R*)ab_in,
+                                                                 a->n);
+    AQ_CUDA_TRY(cudaGetLastError());
+    return AQ_OK;
+  }
+  int accum(const void* ab, double* sens, cudaStream_t st) override {
+    k_ad_accum<R><<<num_sms() * 2, 256, sizeof(double) * a->NS, st>>>((const R*)ab, a->n, a->NS, sens);
+    AQ_CUDA_TRY(cudaGetLastError());
+    return AQ_OK;
+  }
+};
+
+template <int D, class R>
+static AdBase* make_ad(aq_adjoint* a) {
+  if (a->P.has_F) return new (std::nothrow) AdImpl<D, true, R>(a);
+  return new (std::nothrow) AdImpl<D, false, R>(a);
+}
+
+static void free_ad(aq_adjoint* a) {
+  if (!a) return;
+  delete a->impl;
+  for (void* p : a->ckpt)
+    if (p) cudaFree(p);
+  for (void* p : a->seg)
+    if (p) cudaFree(p);
+  if (a->grid) cudaFree(a->grid);
+  if (a->gv) cudaFree(a->gv);
+  if (a->gvb) cudaFree(a->gvb);
+  if (a->dsens) cudaFree(a->dsens);
+  delete a;
+}
+
+}  // namespace aq
+
+using namespace aq;
+
+extern "C" {
+
+int aq_adjoint_create(const aq_params* P, aq_adjoint** out) {
+  if (!P || !out) return AQ_E_ARG;
+  *out = nullptr;
+  const int D = P->dim;
+  if (D != 2 && D != 3) return AQ_E_ARG;
+  if (P->has_mat) return AQ_E_LAYOUT;
+  if (P->n_particles < 1 || P->n_particles > 0x7fffffffLL) return AQ_E_ARG;
+  for (int d = 0; d < D; ++d)
+    if (P->res[d] < 3 || P->res[d] > 8192) return AQ_E_ARG;
+  const int mk = P->mat[0].kind;
+  if (mk != AQ_MAT_FLUID && mk != AQ_MAT_ELASTIC) return AQ_E_ARG;  // reference materials only
+  if (!P->has_F && mk != AQ_MAT_FLUID) return AQ_E_LAYOUT;
+  if (P->use_friction) return AQ_E_ARG;  // the reference's AD scenes run without friction
+  aq_adjoint* a = new (std::nothrow) aq_adjoint();
+  if (!a) return AQ_E_NOMEM;
+  a->P = *P;
+  a->D = D;
+  a->NS = 2 * D + D * D + (P->has_F ? D * D : 1);
+  a->n = P->n_particles;
+  a->rsz = P->precision ? sizeof(double) : sizeof(float);
+  a->ncell = 1;
+  for (int d = 0; d < D; ++d) a->ncell *= P->res[d];
+  cudaError_t e = cudaMalloc(&a->grid, a->rsz * 4 * a->ncell);
+  if (e == cudaSuccess) e = cudaMalloc(&a->gv, a->rsz * 4 * a->ncell);
+  if (e == cudaSuccess) e = cudaMalloc(&a->gvb, a->rsz * 4 * a->ncell);
+  if (e == cudaSuccess) e = cudaMalloc((void**)&a->dsens, sizeof(double) * a->NS);
+  if (e != cudaSuccess) {
+    set_last_cuda_error(e, "cudaMalloc");
+    free_ad(a);
+    return AQ_E_NOMEM;
+  }
+  if (D == 3)
+    a->impl = P->precision ? make_ad<3, double>(a) : make_ad<3, float>(a);
+  else
+    a->impl = P->precision ? make_ad<2, double>(a) : make_ad<2, float>(a);
+  if (!a->impl) {
+    free_ad(a);
+    return AQ_E_NOMEM;
+  }
+  *out = a;
+  return AQ_OK;
+}
+
+int aq_adjoint_destroy(aq_adjoint* a) {
+  if (!a) return AQ_E_ARG;
+  cudaDeviceSynchronize();
+  free_ad(a);
+  return AQ_OK;
+}
+
+int aq_adjoint_forward(aq_adjoint* a, const void* d_s0, int32_t n_substeps, int32_t every, void* d_sT,
+                       void* stream) {
+  if (!a || !d_s0 || !d_sT || n_substeps < 1 || every < 1) return AQ_E_ARG;
+  cudaStream_t st = as_stream(stream);
+  const size_t sbytes = a->rsz * a->NS * a->n;
+  const int nck = (n_substeps + every - 1) / every;
+  for (void* p : a->ckpt) cudaFree(p);
+  a->ckpt.assign(nck, nullptr);
+  for (int k = 0; k < nck; ++k) AQ_CUDA_TRY(cudaMalloc(&a->ckpt[k], sbytes));
+  if ((int)a->seg.size() != every + 1) {
+    for (void* p : a->seg) cudaFree(p);
+    a->seg.assign(every + 1, nullptr);
+    for (int k = 0; k <= every; ++k) AQ_CUDA_TRY(cudaMalloc(&a->seg[k], sbytes));
+  }
+  a->T = n_substeps;
+  a->every = every;
+  AQ_CUDA_TRY(cudaMemcpyAsync(a->seg[0], d_s0, sbytes, cudaMemcpyDeviceToDevice, st));
+  int cur = 0;
+  for (int t = 0; t < n_substeps; ++t) {
+    if (t % every == 0) AQ_CUDA_TRY(cudaMemcpyAsync(a->ckpt[t / every], a->seg[cur], sbytes, cudaMemcpyDeviceToDevice, st));
+    const int rc = a->impl->step(a->seg[cur], a->seg[1 - cur], st);
+    if (rc) return rc;
+    cur = 1 - cur;
+  }
+  AQ_CUDA_TRY(cudaMemcpyAsync(d_sT, a->seg[cur], sbytes, cudaMemcpyDeviceToDevice, st));
+  return AQ_OK;
+}
+
+int aq_adjoint_backward(aq_adjoint* a, const void* d_seed, void* d_grad_s0, double* h_sens, void* stream) {
+  if (!a || !d_seed || a->T < 1) return AQ_E_ARG;
+  cudaStream_t st = as_stream(stream);
+  const size_t sbytes = a->rsz * a->NS * a->n;
+  void* ab[2] = {nullptr, nullptr};
+  AQ_CUDA_TRY(cudaMallocAsync(&ab[0], sbytes, st));
+  AQ_CUDA_TRY(cudaMallocAsync(&ab[1], sbytes, st));
+  AQ_CUDA_TRY(cudaMemcpyAsync(ab[0], d_seed, sbytes, cudaMemcpyDeviceToDevice, st));
+  AQ_CUDA_TRY(cudaMemsetAsync(a->dsens, 0, sizeof(double) * a->NS, st));
+  int cur = 0;  // ab[cur] = adjoint of state t+1
+  const int T = a->T, every = a->every;
+  for (int sgi = (T - 1) / every; sgi >= 0; --sgi) {
+    const int t0 = sgi * every, t1 = std::min(T, t0 + every);
+    AQ_CUDA_TRY(cudaMemcpyAsync(a->seg[0], a->ckpt[sgi], sbytes, cudaMemcpyDeviceToDevice, st));
+    for (int t = t0; t < t1 - 1; ++t) {
+      const int rc = a->impl->step(a->seg[t - t0], a->seg[t - t0 + 1], st);
+      if (rc) return rc;
+    }
+    for (int t = t1 - 1; t >= t0; --t) {
+      const int rc = a->impl->step_bwd(a->seg[t - t0], ab[cur], ab[1 - cur], st);
+      if (rc) return rc;
+      cur = 1 - cur;  // ab[cur] = adjoint of state t
+      if (t >= 1) {
+        const int rc2 = a->impl->accum(ab[cur], a->dsens, st);
+        if (rc2) return rc2;
+      }
+    }
+  }
+  if (d_grad_s0) AQ_CUDA_TRY(cudaMemcpyAsync(d_grad_s0, ab[cur], sbytes, cudaMemcpyDeviceToDevice, st));
+  if (h_sens) AQ_CUDA_TRY(cudaMemcpyAsync(h_sens, a->dsens, sizeof(double) * a->NS, cudaMemcpyDeviceToHost, st));
+  AQ_CUDA_TRY(cudaFreeAsync(ab[0], st));
+  AQ_CUDA_TRY(cudaFreeAsync(ab[1], st));
+  AQ_CUDA_TRY(cudaStreamSynchronize(st));
+  return AQ_OK;
+}
+
+}  // extern "C"

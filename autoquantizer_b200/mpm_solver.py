@@ -387,6 +387,39 @@ class MPMSolver:
         self._layout = None
         self._drop_sim()
 
+    # ------------------------------------------------------------ adjoint
+
+    def run_forward_with_ad_nlogn(self, save_pics=False, ggui=None, every=64):
+        """The autodiff pass (mpm_solver.py:1093-1302, drivers' ad()): forward
+        n_timestep-1 substeps on unquantized state with checkpoints, loss
+        compute_ek, then the hand-written reverse pass; the per-scalar
+        sensitivities are kept for get_gradients().  Returns the loss."""
+        import torch
+
+        from .adjoint import Adjoint, ek_loss, ek_seed
+
+        if self.has_mat:
+            raise ValueError("the adjoint runs single-material scenes")
+        self._pull()
+        P = self._params()
+        n, ns = self.current_idx, self.n_slots()
+        adj = Adjoint(P)
+        dt = torch.float64 if self.param.precision == "f64" else torch.float32
+        s0 = torch.from_numpy(np.ascontiguousarray(self._host[:n, :ns])).to("cuda", dt)
+        sT = adj.forward(s0, self.n_timestep - 1, every)
+        loss = ek_loss(sT, self.dim, self.p_mass, self.g)
+        adj.backward(ek_seed(sT, self.dim, self.p_mass, self.g))
+        self._grads = adj.sens
+        self._ad_final = sT
+        adj.close()
+        self.loss[None] = loss
+        return loss
+
+    def get_gradients(self):
+        """Per-scalar sum over substeps and particles of (dL/dq)^2, in the
+        x, v, C, F|J order of get_gradients (mpm_solver.py:1273-1302)."""
+        return np.asarray(self._grads)
+
     # ------------------------------------------------- range detection
 
     def run_forward_detect_ranges(self, n=None):

@@ -231,6 +231,31 @@ int aq_state_error(const void* d_a, int32_t a_f64, const void* d_b, int32_t b_f6
                    int64_t n, int32_t n_slots, double* h_sq, double* h_max,
                    void* stream);
 
+/* ------------------------------------------------------------- adjoint */
+
+/* Hand-written reverse of the substep on unquantized state (n x n_slots,
+ * slots x, v, C, F|J; f32 or f64 per params.precision), one material
+ * (AQ_MAT_FLUID or the reference's AQ_MAT_ELASTIC), no friction; position
+ * clipping is not applied, as in the reference's differentiable g2p.
+ * Replaces the reference's autodiff pass: run_forward_with_ad_nlogn with
+ * checkpoint / rerun_from / nlogn_loop_forward_grad / accu_grad /
+ * get_gradients (mpm_exps/engine/mpm_solver.py:1093-1302) and the Taichi
+ * grad kernels of p2g, grid_op and g2p (taichi_submission/taichi/transforms/
+ * auto_diff.cpp).  Checkpoints every `every` substeps; a segment is
+ * recomputed from its checkpoint during the backward pass. */
+typedef struct aq_adjoint aq_adjoint;
+int aq_adjoint_create(const aq_params* h_params, aq_adjoint** out);
+int aq_adjoint_destroy(aq_adjoint* adj);
+/* Run n_substeps from d_s0, keeping checkpoints; d_sT receives the final
+ * state. */
+int aq_adjoint_forward(aq_adjoint* adj, const void* d_s0, int32_t n_substeps, int32_t every, void* d_sT,
+                       void* stream);
+/* Back-propagate d_seed = dL/d(final state) of the last forward run.
+ * d_grad_s0 (optional) receives dL/d(initial state); h_sens (optional,
+ * n_slots doubles) receives sum over substeps t = 1..T-1 and particles of
+ * (dL/d state_t)^2 per slot, the reference's grad_sum. */
+int aq_adjoint_backward(aq_adjoint* adj, const void* d_seed, void* d_grad_s0, double* h_sens, void* stream);
+
 const char* aq_error_string(int32_t code);
 int32_t aq_abi_version(void);
 #endif /* __CUDACC_RTC__ */
