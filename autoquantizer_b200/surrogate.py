@@ -1,0 +1,395 @@
+"""Learned sensitivity surrogate.
+
+The reference derives a bit-width scheme from per-field sensitivities
+(sum over substeps and particles of (dL/dq)^2) that a full reverse-mode run
+produces (mpm_solver.py:1093-1302), then calls the analytical solver
+(solvers/analytical_solver.py).  Here a small MLP (64-128-128-12, GELU, bf16
+weights, fp32 accumulation; libaq aq_mlp_* kernels for inference, backward
+and Adam) predicts the log10 sensitivities of 12 field groups from cheap
+statistics of a 16-substep forward window, so a scheme can be derived without
+a backward run; the adjoint (adjoint.py) produces the training labels and
+remains the fallback and the judge of the surrogate's error.
+
+Field groups: x_0..2, v_0..2, rows 0..2 of C, rows 0..2 of F (J in row 0 for
+fluids); 2D scenes leave the third entries empty (masked).
+Features (64): per group, at the end of the window, mean |.|, std, max |.|
+and mean |change over the window| (48), plus 16 scene descriptors.
+
+    python -m autoquantizer_b200.surrogate --train 512 --test 64 --out report.json
+"""
+import argparse
+import ctypes as C
+import json
+import time
+
+import numpy as np
+
+from . import _lib
+from .mpm_config import MPMConfig
+
+N_IN, N_H, N_OUT = 64, 128, 12
+WINDOW = 16
+
+
+# ------------------------------------------------------------------ scenes
+
+
+def random_scene(rng, n_min=10_000, n_max=500_000, horizon=64):
+    """A C5-style scene: 2D or 3D, box or sphere, elastic (E log-uniform in
+    [1e3, 1e5], nu in [0.2, 0.4]) or, with probability 0.3, fluid."""
+    dim = 2 if rng.random() < 0.5 else 3
+    fluid = rng.random() < 0.3
+    n = int(rng.uniform(n_min, n_max))
+    c = MPMConfig()
+    c.dim = dim
+    c.n_grid = 64 if dim == 3 else 256
+    c.grid_res = [c.n_grid] * dim
+    c.size = 1.0
+    c.bound = [3] * dim
+    c.use_friction = False
+    c.use_fluid = fluid
+    c.precision = "f32"
+    c.p_rho = 1.0
+    dx = 1.0 / c.n_grid
+    c.p_vol = (dx * 0.5) ** dim
+    c.E = float(10 ** rng.uniform(3, 5))
+    c.nu = float(rng.uniform(0.2, 0.4))
+    c.la = float(10 ** rng.uniform(2.5, 4))
+    mu = c.E / (2 * (1 + c.nu))
+    la0 = c.E * c.nu / ((1 + c.nu) * (1 - 2 * c.nu))
+    speed = np.sqrt(c.la if fluid else (la0 + 2 * mu))
+    c.dt = float(min(2e-4, 0.2 * dx / speed))
+    c.n_timesteps = horizon + 1
+    c.n_particles = n
+    # shape: box or ball near the centre, sized for about 8 particles per
+    # cell (clamped to the domain), uniform particles, random push
+    center = rng.uniform(0.45, 0.55, dim)
+    side = min(0.6, max(0.08, (n / (8.0 * c.n_grid ** dim)) ** (1.0 / dim)))
+    half = 0.5 * side * rng.uniform(0.8, 1.25, dim)
+    half = np.minimum(half, 0.3)
+    if rng.random() < 0.5:
+        x = center + (rng.random((n, dim)) * 2 - 1) * half
+    else:
+        r = min(0.3, float(half.max()) * 1.1)
+        u = rng.normal(size=(n, dim))
+        u /= np.linalg.norm(u, axis=1, keepdims=True)
+        x = center + u * r * rng.random((n, 1)) ** (1.0 / dim)
+    v0 = rng.uniform(-1.0, 1.0, dim)
+    ns = 2 * dim + dim * dim + (1 if fluid else dim * dim)
+    vals = np.zeros((n, ns))
+    vals[:, :dim] = x
+    vals[:, dim:2 * dim] = v0
+    if fluid:
+        vals[:, 2 * dim + dim * dim] = 1.0
+    else:
+        vals[:, 2 * dim + dim * dim:] = np.eye(dim).ravel()
+    return c, vals
+
+
+def groups_of(dim, fluid):
+    """Slot indices of the 12 field groups (empty lists for absent groups)."""
+    g = [[] for _ in range(N_OUT)]
+    for d in range(dim):
+        g[d] = [d]
+        g[3 + d] = [dim + d]
+        g[6 + d] = [2 * dim + d * dim + e for e in range(dim)]
+        if fluid:
+            if d == 0:
+                g[9] = [2 * dim + dim * dim]
+        else:
+            g[9 + d] = [2 * dim + dim * dim + d * dim + e for e in range(dim)]
+    return g
+
+
+def features(cfg, s_a, s_b):
+    dim, fluid = cfg.dim, cfg.use_fluid
+    f = np.zeros(N_IN)
+    for gi, slots in enumerate(groups_of(dim, fluid)):
+        if not slots:
+            continue
+        b = s_b[:, slots]
+        a = s_a[:, slots]
+        f[4 * gi + 0] = np.log10(np.mean(np.abs(b)) + 1e-12)
+        f[4 * gi + 1] = np.log10(np.std(b) + 1e-12)
+        f[4 * gi + 2] = np.log10(np.max(np.abs(b)) + 1e-12)
+        f[4 * gi + 3] = np.log10(np.mean(np.abs(b - a)) + 1e-12)
+    n = s_b.shape[0]
+    v = s_b[:, dim:2 * dim]
+    g = [dim / 3.0, float(fluid), np.log10(cfg.E) / 5, cfg.nu, np.log10(cfg.la) / 4, np.log10(n) / 6,
+         np.log10(cfg.dt) / 4, np.log10(1.0 / cfg.n_grid), np.log10(cfg.p_vol * cfg.p_rho) / 10, cfg.g / 10,
+         np.log10(np.mean(np.abs(v)) + 1e-9), np.log10(0.5 * np.sum(v * v) * cfg.p_vol + 1e-12) / 5,
+         (cfg.n_timesteps - 1) / 100.0, float(np.mean(s_b[:, 1] < 0.1)), WINDOW / 16.0, 1.0]
+    f[48:64] = g
+    return f
+
+
+def window_states(cfg, vals):
+    """Run the 16-substep feature window on the fast simulator (FP32 state)."""
+    from .mpm_solver import MPMSolver
+
+    s = MPMSolver(cfg)
+    s.set_particles(vals)
+    s.substeps(WINDOW)
+    return vals, s.state_values()
+
+
+def adjoint_sensitivities(cfg, vals, every=16):
+    """Per-slot sensitivities of compute_ek over the scene's horizon."""
+    import torch
+
+    from .adjoint import Adjoint, ek_loss, ek_seed
+    from .mpm_solver import MPMSolver
+
+    s = MPMSolver(cfg)
+    s.set_particles(vals)
+    adj = Adjoint(s._params())
+    s0 = torch.from_numpy(np.ascontiguousarray(vals)).to("cuda", torch.float32)
+    sT = adj.forward(s0, cfg.n_timesteps - 1, every)
+    loss = ek_loss(sT, cfg.dim, s.p_mass, s.g)
+    _, sens = adj.backward(ek_seed(sT, cfg.dim, s.p_mass, s.g))
+    adj.close()
+    return sens, loss
+
+
+def group_sensitivities(cfg, sens):
+    out = np.zeros(N_OUT)
+    mask = np.zeros(N_OUT)
+    for gi, slots in enumerate(groups_of(cfg.dim, cfg.use_fluid)):
+        if slots:
+            out[gi] = np.log10(np.sum(sens[slots]) + 1e-30)
+            mask[gi] = 1.0
+    return out, mask
+
+
+def group_ranges(cfg, s_b):
+    """Per-group ranges as the drivers' solve() sets them: positions 1, the
+    others twice the detected max |.| (run_mpm_elastic_2d.py:227-242)."""
+    r = np.ones(N_OUT)
+    for gi, slots in enumerate(groups_of(cfg.dim, cfg.use_fluid)):
+        if slots and gi >= 3:
+            r[gi] = 2.0 * max(np.max(np.abs(s_b[:, slots])), 1e-6)
+    return r
+
+
+def make_dataset(n_scenes, seed, n_min=10_000, n_max=500_000, horizon=64, log=None):
+    rng = np.random.default_rng(seed)
+    X, Y, M, meta = [], [], [], []
+    for i in range(n_scenes):
+        cfg, vals = random_scene(rng, n_min, n_max, horizon)
+        a, b = window_states(cfg, vals)
+        sens, loss = adjoint_sensitivities(cfg, vals)
+        y, m = group_sensitivities(cfg, sens)
+        X.append(features(cfg, a, b))
+        Y.append(y)
+        M.append(m)
+        meta.append({"dim": cfg.dim, "fluid": bool(cfg.use_fluid), "n": int(vals.shape[0]), "loss": float(loss),
+                     "ranges": group_ranges(cfg, b).tolist()})
+        if log and (i + 1) % 32 == 0:
+            log("scene %d/%d" % (i + 1, n_scenes))
+    return np.array(X), np.array(Y), np.array(M), meta
+
+
+# --------------------------------------------------------------------- MLP
+
+
+class MLP:
+    """64-128-128-12 MLP trained and run by the libaq kernels."""
+
+    def __init__(self, seed=0, n_in=N_IN, n_h=N_H, n_out=N_OUT):
+        import torch
+
+        self.dims = (n_in, n_h, n_out)
+        n = _lib.lib().aq_mlp_param_count(n_in, n_h, n_out)
+        rng = np.random.default_rng(seed)
+        p = np.zeros(n, dtype=np.float32)
+        o = 0
+        for fan_in, fan_out in ((n_in, n_h), (n_h, n_h), (n_h, n_out)):
+            w = rng.normal(0, np.sqrt(2.0 / fan_in), (fan_out, fan_in)).astype(np.float32)
+            p[o:o + w.size] = w.ravel()
+            o += w.size + fan_out  # biases start at zero
+        self.n = n
+        self.p = torch.from_numpy(p).cuda()
+        self.pb = torch.empty(n, dtype=torch.int16, device="cuda")
+        self.m = torch.zeros_like(self.p)
+        self.v = torch.zeros_like(self.p)
+        self.g = torch.zeros_like(self.p)
+        self.t = 0
+        _lib.check(_lib.lib().aq_mlp_to_bf16(C.c_void_p(self.p.data_ptr()), C.c_void_p(self.pb.data_ptr()), n,
+                                             _lib.stream_ptr()), "aq_mlp_to_bf16")
+        self.x_mean = self.x_std = self.y_mean = self.y_std = None
+
+    def _fwd(self, x, act=None):
+        import torch
+
+        B = x.shape[0]
+        y = torch.empty((B, self.dims[2]), dtype=torch.float32, device="cuda")
+        _lib.check(_lib.lib().aq_mlp_forward(*self.dims, C.c_void_p(self.p.data_ptr()), C.c_void_p(self.pb.data_ptr()),
+                                             C.c_void_p(x.data_ptr()), B, C.c_void_p(y.data_ptr()),
+                                             None if act is None else C.c_void_p(act.data_ptr()), _lib.stream_ptr()),
+                   "aq_mlp_forward")
+        return y
+
+    def forward_raw(self, x):
+        import torch
+
+        x = torch.as_tensor(x, dtype=torch.float32).cuda().contiguous()
+        return self._fwd(x)
+
+    def grad_raw(self, x, dy):
+        """(loss-agnostic) parameter gradient for output gradient dy."""
+        import torch
+
+        x = torch.as_tensor(x, dtype=torch.float32).cuda().contiguous()
+        dy = torch.as_tensor(dy, dtype=torch.float32).cuda().contiguous()
+        B = x.shape[0]
+        act = torch.empty((B, 4 * self.dims[1]), dtype=torch.float32, device="cuda")
+        self._fwd(x, act)
+        _lib.check(_lib.lib().aq_mlp_backward(*self.dims, C.c_void_p(self.pb.data_ptr()), C.c_void_p(x.data_ptr()), B,
+                                              C.c_void_p(act.data_ptr()), C.c_void_p(dy.data_ptr()),
+                                              C.c_void_p(self.g.data_ptr()), _lib.stream_ptr()), "aq_mlp_backward")
+        return self.g.clone()
+
+    def fit(self, X, Y, M, steps=3000, lr=1e-3, batch=128, seed=0):
+        import torch
+
+        X = np.asarray(X, dtype=np.float64)
+        Y = np.asarray(Y, dtype=np.float64)
+        M = np.asarray(M, dtype=np.float64)
+        self.x_mean, self.x_std = X.mean(0), X.std(0) + 1e-6
+        msum = np.maximum(M.sum(0), 1)
+        self.y_mean = (Y * M).sum(0) / msum
+        self.y_std = np.sqrt((((Y - self.y_mean) * M) ** 2).sum(0) / msum) + 1e-6
+        xs = torch.from_numpy(((X - self.x_mean) / self.x_std).astype(np.float32)).cuda()
+        ys = torch.from_numpy(((Y - self.y_mean) / self.y_std * M).astype(np.float32)).cuda()
+        ms = torch.from_numpy(M.astype(np.float32)).cuda()
+        n = xs.shape[0]
+        B = min(batch, n)
+        rng = np.random.default_rng(seed)
+        act = torch.empty((B, 4 * self.dims[1]), dtype=torch.float32, device="cuda")
+        dy = torch.empty((B, self.dims[2]), dtype=torch.float32, device="cuda")
+        loss = torch.zeros(1, dtype=torch.float32, device="cuda")
+        hist = []
+        L = _lib.lib()
+        for it in range(steps):
+            idx = torch.from_numpy(rng.choice(n, B, replace=False)).cuda()
+            xb, yb, mb = xs[idx].contiguous(), ys[idx].contiguous(), ms[idx].contiguous()
+            y = self._fwd(xb, act)
+            loss.zero_()
+            _lib.check(L.aq_mlp_mse_grad(C.c_void_p(y.data_ptr()), C.c_void_p(yb.data_ptr()),
+                                         C.c_void_p(mb.data_ptr()), C.c_void_p(dy.data_ptr()), y.numel(),
+                                         float(mb.sum().item()), C.c_void_p(loss.data_ptr()), _lib.stream_ptr()),
+                       "aq_mlp_mse_grad")
+            _lib.check(L.aq_mlp_backward(*self.dims, C.c_void_p(self.pb.data_ptr()), C.c_void_p(xb.data_ptr()), B,
+                                         C.c_void_p(act.data_ptr()), C.c_void_p(dy.data_ptr()),
+                                         C.c_void_p(self.g.data_ptr()), _lib.stream_ptr()), "aq_mlp_backward")
+            self.t += 1
+            _lib.check(L.aq_mlp_adam(C.c_void_p(self.p.data_ptr()), C.c_void_p(self.pb.data_ptr()),
+                                     C.c_void_p(self.m.data_ptr()), C.c_void_p(self.v.data_ptr()),
+                                     C.c_void_p(self.g.data_ptr()), self.n, lr, 0.9, 0.999, 1e-8, self.t,
+                                     _lib.stream_ptr()), "aq_mlp_adam")
+            if it % 100 == 0 or it == steps - 1:
+                hist.append((it, float(loss.item())))
+        return hist
+
+    def predict(self, X):
+        X = np.asarray(X, dtype=np.float64)
+        y = self.forward_raw(((X - self.x_mean) / self.x_std).astype(np.float32)).cpu().numpy()
+        return y * self.y_std + self.y_mean
+
+
+# ----------------------------------------------------------------- schemes
+
+
+def scheme_bits(log_sens, mask, ranges, loss, tol_rel=1e-3):
+    """Bits per group (incl. sign) from log10 sensitivities with the
+    reference's LagrangianEB over the present groups."""
+    from .solvers import LagrangianEB
+
+    idx = np.where(np.asarray(mask) > 0)[0]
+    g = 10.0 ** np.asarray(log_sens)[idx] * np.asarray(ranges)[idx] ** 2
+    bits, _ = LagrangianEB(g, ref=abs(loss) + 1e-30, tol_rel=tol_rel)
+    out = np.zeros(N_OUT, dtype=np.int64)
+    out[idx] = bits + 1
+    return out
+
+
+def evaluate(mlp, X, Y, M, meta, tol_rel=1e-3, baseline=None):
+    """Bit-width agreement of surrogate-derived schemes with adjoint-derived
+    ones on held-out scenes; `baseline` (log-sensitivity per group, e.g. the
+    training mean) stands for the method without the network."""
+    pred = mlp.predict(X)
+    res = {"within_1_bit": [], "mean_abs_bits": [], "log_err": []}
+    base = {"within_1_bit": [], "mean_abs_bits": [], "log_err": []}
+    for i in range(len(X)):
+        m = M[i] > 0
+        b_adj = scheme_bits(Y[i], M[i], meta[i]["ranges"], meta[i]["loss"], tol_rel)
+        for out, y_hat in ((res, pred[i]), (base, baseline if baseline is not None else None)):
+            if y_hat is None:
+                continue
+            b = scheme_bits(y_hat, M[i], meta[i]["ranges"], meta[i]["loss"], tol_rel)
+            d = np.abs(b - b_adj)[m]
+            out["within_1_bit"].append(float(np.mean(d <= 1)))
+            out["mean_abs_bits"].append(float(np.mean(d)))
+            out["log_err"].append(float(np.mean(np.abs(y_hat - Y[i])[m])))
+    summ = lambda r: {k: float(np.mean(v)) for k, v in r.items() if v}  # noqa: E731
+    return summ(res), summ(base)
+
+
+def timing_comparison(cfg, vals, mlp):
+    """Wall time of deriving a scheme with the surrogate (feature window +
+    inference + solver) vs with the adjoint (full forward + backward)."""
+    import torch
+
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
+    a, b = window_states(cfg, vals)
+    y = mlp.predict(features(cfg, a, b)[None])[0]
+    _, mask = group_sensitivities(cfg, np.ones(2 * cfg.dim + cfg.dim ** 2 + (1 if cfg.use_fluid else cfg.dim ** 2)))
+    scheme_bits(y, mask, group_ranges(cfg, b), 1.0)
+    torch.cuda.synchronize()
+    t_sur = time.perf_counter() - t0
+    t0 = time.perf_counter()
+    sens, loss = adjoint_sensitivities(cfg, vals)
+    ys, mask = group_sensitivities(cfg, sens)
+    scheme_bits(ys, mask, group_ranges(cfg, b), loss)
+    torch.cuda.synchronize()
+    t_adj = time.perf_counter() - t0
+    return t_sur, t_adj
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--train", type=int, default=512)
+    ap.add_argument("--test", type=int, default=64)
+    ap.add_argument("--n-max", type=int, default=500_000)
+    ap.add_argument("--horizon", type=int, default=64)
+    ap.add_argument("--steps", type=int, default=3000)
+    ap.add_argument("--out", default=None)
+    args = ap.parse_args()
+    t0 = time.perf_counter()
+    Xtr, Ytr, Mtr, _ = make_dataset(args.train, 1, n_max=args.n_max, horizon=args.horizon, log=print)
+    Xte, Yte, Mte, mte = make_dataset(args.test, 2, n_max=args.n_max, horizon=args.horizon, log=print)
+    t_data = time.perf_counter() - t0
+    mlp = MLP(seed=0)
+    t0 = time.perf_counter()
+    hist = mlp.fit(Xtr, Ytr, Mtr, steps=args.steps)
+    t_fit = time.perf_counter() - t0
+    base = (Ytr * Mtr).sum(0) / np.maximum(Mtr.sum(0), 1)
+    sur, bl = evaluate(mlp, Xte, Yte, Mte, mte, baseline=base)
+    rng = np.random.default_rng(3)
+    cfg, vals = random_scene(rng, args.n_max // 2, args.n_max, horizon=args.horizon)
+    t_sur, t_adj = timing_comparison(cfg, vals, mlp)
+    t_sur, t_adj = timing_comparison(cfg, vals, mlp)  # warm (JIT caches)
+    rep = {"train_scenes": args.train, "test_scenes": args.test, "horizon": args.horizon, "window": WINDOW,
+           "dataset_seconds": t_data, "fit_seconds": t_fit, "loss_history": hist, "surrogate": sur,
+           "baseline_mean_predictor": bl, "scheme_seconds": {"surrogate": t_sur, "adjoint": t_adj,
+                                                            "speedup": t_adj / t_sur},
+           "timing_scene": {"dim": cfg.dim, "fluid": bool(cfg.use_fluid), "n": int(vals.shape[0])}}
+    print(json.dumps(rep, indent=1))
+    if args.out:
+        with open(args.out, "w") as f:
+            json.dump(rep, f, indent=1)
+
+
+if __name__ == "__main__":
+    main()

@@ -256,6 +256,30 @@ int aq_adjoint_forward(aq_adjoint* adj, const void* d_s0, int32_t n_substeps, in
  * (dL/d state_t)^2 per slot, the reference's grad_sum. */
 int aq_adjoint_backward(aq_adjoint* adj, const void* d_seed, void* d_grad_s0, double* h_sens, void* stream);
 
+/* ------------------------------------------------ sensitivity surrogate */
+
+/* MLP in -> h -> h -> out (GELU on the hidden layers) predicting per-field
+ * log-sensitivities from forward-pass statistics, so that the analytical
+ * solver (solvers/analytical_solver.py) can derive a bit-width scheme without
+ * a full backward run.  No reference counterpart.  Parameters: one float32
+ * vector W1[h][in], b1[h], W2[h][h], b2[h], W3[out][h], b3[out] and its bf16
+ * copy (weights are read as bf16, every dot product accumulates in fp32).
+ * d_act: B*4*h floats of saved activations (optional for inference). */
+int64_t aq_mlp_param_count(int32_t in, int32_t h, int32_t out);
+int aq_mlp_to_bf16(const float* d_params, uint16_t* d_params_bf16, int64_t n, void* stream);
+int aq_mlp_forward(int32_t in, int32_t h, int32_t out, const float* d_params, const uint16_t* d_params_bf16,
+                   const float* d_x, int32_t batch, float* d_y, float* d_act, void* stream);
+/* Gradient of the loss w.r.t. all parameters (d_grad, same layout) given
+ * d_dy = dL/dy and the activations saved by aq_mlp_forward. */
+int aq_mlp_backward(int32_t in, int32_t h, int32_t out, const uint16_t* d_params_bf16, const float* d_x,
+                    int32_t batch, const float* d_act, const float* d_dy, float* d_grad, void* stream);
+/* Masked mean squared error: d_dy = 2 (y - t) m / count; *d_loss += loss. */
+int aq_mlp_mse_grad(const float* d_y, const float* d_target, const float* d_mask, float* d_dy, int64_t n,
+                    float count, float* d_loss, void* stream);
+/* One Adam step (t >= 1) on the fp32 parameters; refreshes the bf16 copy. */
+int aq_mlp_adam(float* d_params, uint16_t* d_params_bf16, float* d_m, float* d_v, const float* d_grad, int64_t n,
+                float lr, float beta1, float beta2, float eps, int32_t t, void* stream);
+
 const char* aq_error_string(int32_t code);
 int32_t aq_abi_version(void);
 #endif /* __CUDACC_RTC__ */

@@ -8,10 +8,10 @@ tests/golden/reference_data.json):
   * the per-scalar autodiff sensitivities of that loss that the reference
     shipped (mpm_exps/grads/elastic_2d/elastic_2d.npy).
 
-8192 substeps of a soft elastic scene amplify differences in floating-point
-summation order, so the loss is pinned to 1% and the sensitivities (which
-span 1e4..1e18) to within a factor of 3 per scalar, with the ordering of
-the fields preserved.
+The reference prints the loss to three decimals; it is pinned to that
+(5e-3 absolute, i.e. 7e-7 relative).  The sensitivities span 1e4..1e18 and
+come out of 8192 substeps whose f64 sums are accumulated in a different
+order than Taichi's, so each is pinned to 1% relative.
 """
 import json
 import os
@@ -58,17 +58,15 @@ def test_elastic_2d_f64_loss_matches_reference():
     loss = s.run_forward_only()
     print("elastic_2d f64 loss %.4f (reference %.3f)" % (loss, E2["f64_loss"]))
     assert s.status()[0] == 0
-    assert loss == pytest.approx(E2["f64_loss"], rel=1e-2)
+    assert loss == pytest.approx(E2["f64_loss"], abs=5e-3)
 
 
 def test_elastic_2d_sensitivities_match_reference_autodiff():
     s = _elastic_2d()
     loss = s.run_forward_with_ad_nlogn(every=64)
-    assert loss == pytest.approx(E2["f64_loss"], rel=1e-2)
+    assert loss == pytest.approx(E2["f64_loss"], abs=5e-3)
     ours = s.get_gradients()
     ref = np.array(GOLD["grads"]["elastic_2d/elastic_2d.npy"])
     ratio = ours / ref
     print("sensitivity ratio ours/reference per scalar:", np.array2string(ratio, precision=3))
-    assert np.all(np.abs(np.log10(ratio)) < np.log10(3.0)), ratio
-    # field ordering (which scalars matter most) is what the solver uses
-    assert np.array_equal(np.argsort(ours), np.argsort(ref)) or np.corrcoef(np.log(ours), np.log(ref))[0, 1] > 0.99
+    assert ours == pytest.approx(ref, rel=1e-2), ratio
