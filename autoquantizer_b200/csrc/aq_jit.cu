@@ -15,9 +15,12 @@
 #include <stdio.h>
 #include <string.h>
 
+#include <stdlib.h>
+
 #include <mutex>
 #include <string>
 #include <unordered_map>
+#include <vector>
 
 #include "aq_common.cuh"
 #include "aq_jit.h"
@@ -158,7 +161,8 @@ void* jit_k_step(int D, bool HF, bool HM, bool f64, const aq_layout& L, std::str
   std::string src = "#include \"aq_kernels.cuh\"\nnamespace aq {\n";
   src += jit_layout_source(L);
   src += "}\n";
-  const std::string key = std::string(name) + "\n" + src;
+  std::string key = std::string(name) + "\n" + src;
+  if (const char* e = getenv("AQ_JIT_DEFINES")) key += std::string("\n") + e;
   auto hit = g_cache.find(key);
   if (hit != g_cache.end()) return (void*)hit->second;
 
@@ -169,8 +173,23 @@ void* jit_k_step(int D, bool HF, bool HM, bool f64, const aq_layout& L, std::str
     return nullptr;
   }
   g_nv.add_name(prog, name);
-  const char* opts[] = {"--gpu-architecture=sm_100a", "-std=c++17", "-lineinfo", "-DAQ_JIT=1"};
-  const nvrtcResult rc = g_nv.compile(prog, 4, opts);
+  // AQ_JIT_DEFINES (environment): extra -D options, e.g.
+  // "AQ_STEP_MIN_BLOCKS=1", separated by spaces (tuning experiments)
+  std::vector<std::string> extra;
+  if (const char* e = getenv("AQ_JIT_DEFINES")) {
+    std::string s(e), tok;
+    for (size_t i = 0; i <= s.size(); ++i) {
+      if (i == s.size() || s[i] == ' ') {
+        if (!tok.empty()) extra.push_back("-D" + tok);
+        tok.clear();
+      } else {
+        tok += s[i];
+      }
+    }
+  }
+  std::vector<const char*> opts = {"--gpu-architecture=sm_100a", "-std=c++17", "-lineinfo", "-DAQ_JIT=1"};
+  for (const std::string& x : extra) opts.push_back(x.c_str());
+  const nvrtcResult rc = g_nv.compile(prog, (int)opts.size(), opts.data());
   if (rc != NVRTC_SUCCESS) {
     size_t n = 0;
     g_nv.log_size(prog, &n);

@@ -47,6 +47,9 @@ namespace aq {
 
 constexpr int CH = 256;  // particles per work item = threads per CTA
 constexpr int NWARP = CH / 32;
+#ifndef AQ_STEP_MIN_BLOCKS
+#define AQ_STEP_MIN_BLOCKS 2  // CTAs per SM the register allocation must allow
+#endif
 
 template <int D>
 struct Geo {
@@ -268,7 +271,7 @@ __device__ __forceinline__ void bspline(const R* x, const SimK<R>& K, int* base,
 // ------------------------------------------------------------ the step
 
 template <int D, bool HF, bool HM, class R, class LA>
-__global__ void __launch_bounds__(CH, 2) k_step(const __grid_constant__ aq_layout Lp, const SimK<R> K,
+__global__ void __launch_bounds__(CH, AQ_STEP_MIN_BLOCKS) k_step(const __grid_constant__ aq_layout Lp, const SimK<R> K,
                                                 const StepArgs A) {
   typedef Sch<D, HF, HM> S;
   typedef Geo<D> G;
