@@ -30,6 +30,7 @@ EXPORTS = [
     "aq_state_error", "aq_error_string", "aq_abi_version", "aq_sim_profile_enable", "aq_sim_profile_get",
     "aq_sim_kernel_is_jit", "aq_adjoint_create", "aq_adjoint_destroy", "aq_adjoint_forward", "aq_adjoint_backward",
     "aq_mlp_param_count", "aq_mlp_to_bf16", "aq_mlp_forward", "aq_mlp_backward", "aq_mlp_mse_grad", "aq_mlp_adam",
+    "aq_state_error_noalloc",
 ]
 
 
@@ -116,6 +117,8 @@ def lib():
         "aq_mlp_backward": ([i32, i32, i32, vp, vp, i32, vp, vp, vp, vp], C.c_int),
         "aq_mlp_mse_grad": ([vp, vp, vp, vp, i64, C.c_float, vp, vp], C.c_int),
         "aq_mlp_adam": ([vp, vp, vp, vp, vp, i64, C.c_float, C.c_float, C.c_float, C.c_float, i32, vp], C.c_int),
+        "aq_state_error_noalloc": ([vp, i32, vp, i32, i64, i32, C.POINTER(C.c_double), C.POINTER(C.c_double), vp],
+                                   C.c_int),
         "aq_error_string": ([i32], C.c_char_p),
         "aq_abi_version": ([], i32),
     }

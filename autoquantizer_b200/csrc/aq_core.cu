@@ -3,6 +3,8 @@
 #include <stdio.h>
 #include <string.h>
 
+#include <mutex>
+
 #include "aq_codec.cuh"
 #include "aq_common.cuh"
 
@@ -235,3 +237,65 @@ int aq_state_error(const void* a, int32_t a_f64, const void* b, int32_t b_f64, i
 }
 
 }  // extern "C"
+
+// ------------------------------------------ allocation-free state error
+//
+// aq_state_error_noalloc does the work of aq_state_error without allocating:
+// its per-slot sums and maxima live in g_err_scratch, a fixed array of
+// device memory that every GPU loading this library holds until the process
+// exits (2 * AQ_NOALLOC_MAX_SLOTS doubles, 4 KiB).  Host code may not hand
+// the array's name to a kernel (in host code it names a host-side stand-in);
+// its device address is looked up once per device with cudaGetSymbolAddress
+// while that device is current, and kept in g_err_addr.
+
+namespace aq {
+
+static __device__ __align__(256) double g_err_scratch[2 * AQ_NOALLOC_MAX_SLOTS];
+static std::mutex g_err_mu;
+static double* g_err_addr[AQ_NOALLOC_MAX_DEVICES];
+
+}  // namespace aq
+
+extern "C" int aq_state_error_noalloc(const void* a, int32_t a_f64, const void* b, int32_t b_f64, int64_t n,
+                                      int32_t ns, double* h_sq, double* h_max, void* stream) {
+  if (!a || !b || !h_sq || !h_max || n < 0 || ns < 1) return AQ_E_ARG;
+  if (ns > AQ_NOALLOC_MAX_SLOTS) return AQ_E_LIMIT;
+  int dev = 0;
+  AQ_CUDA_TRY(cudaGetDevice(&dev));
+  if (dev < 0 || dev >= AQ_NOALLOC_MAX_DEVICES) return AQ_E_LIMIT;
+  double* d = nullptr;
+  {
+    std::lock_guard<std::mutex> g(g_err_mu);
+    if (!g_err_addr[dev]) {
+      void* p = nullptr;
+      const cudaError_t e = cudaGetSymbolAddress(&p, g_err_scratch);
+      if (e != cudaSuccess || !p) {
+        set_last_cuda_error(e != cudaSuccess ? e : cudaErrorInvalidSymbol, "cudaGetSymbolAddress(g_err_scratch)");
+        return AQ_E_CUDA;
+      }
+      g_err_addr[dev] = static_cast<double*>(p);
+    }
+    d = g_err_addr[dev];
+  }
+  cudaStream_t st = as_stream(stream);
+  // the array keeps the previous call's sums: clear this call's part
+  AQ_CUDA_TRY(cudaMemsetAsync(d, 0, sizeof(double) * 2 * ns, st));
+  unsigned grid = (unsigned)(num_sms() * 4);
+  size_t shm = sizeof(double) * 2 * ns;
+  unsigned long long* mx = reinterpret_cast<unsigned long long*>(d + ns);
+  if (n > 0) {
+    if (a_f64 && b_f64)
+      k_state_error<<<grid, 256, shm, st>>>((const double*)a, (const double*)b, n, ns, d, mx);
+    else if (a_f64)
+      k_state_error<<<grid, 256, shm, st>>>((const double*)a, (const float*)b, n, ns, d, mx);
+    else if (b_f64)
+      k_state_error<<<grid, 256, shm, st>>>((const float*)a, (const double*)b, n, ns, d, mx);
+    else
+      k_state_error<<<grid, 256, shm, st>>>((const float*)a, (const float*)b, n, ns, d, mx);
+    AQ_CUDA_TRY(cudaGetLastError());
+  }
+  AQ_CUDA_TRY(cudaMemcpyAsync(h_sq, d, sizeof(double) * ns, cudaMemcpyDeviceToHost, st));
+  AQ_CUDA_TRY(cudaMemcpyAsync(h_max, d + ns, sizeof(double) * ns, cudaMemcpyDeviceToHost, st));
+  AQ_CUDA_TRY(cudaStreamSynchronize(st));
+  return AQ_OK;
+}

@@ -256,6 +256,25 @@ int aq_adjoint_forward(aq_adjoint* adj, const void* d_s0, int32_t n_substeps, in
  * (dL/d state_t)^2 per slot, the reference's grad_sum. */
 int aq_adjoint_backward(aq_adjoint* adj, const void* d_seed, void* d_grad_s0, double* h_sens, void* stream);
 
+/* Same result as aq_state_error, for callers that cannot allocate device
+ * memory themselves: hosts that own the device heap (an engine or an in-situ
+ * analysis plugin that hands out only its own buffers), or loops that must
+ * not take the allocator's locks and latency.  No counterpart in the
+ * reference.  It allocates nothing: its per-slot sums live in a fixed
+ * library-owned device array of 2 * AQ_NOALLOC_MAX_SLOTS doubles that every
+ * GPU loading libaq.so keeps until the process exits; n_slots above
+ * AQ_NOALLOC_MAX_SLOTS returns AQ_E_LIMIT, and a current device index at or
+ * above AQ_NOALLOC_MAX_DEVICES returns AQ_E_LIMIT.  The first call on a device
+ * looks up the array's device address (make that first call before any
+ * stream capture starts).  All calls share the one array, each clears its
+ * part first, and calls that overlap on the GPU (e.g. from two streams)
+ * race on it.  Synchronizes `stream`. */
+#define AQ_NOALLOC_MAX_SLOTS 256
+#define AQ_NOALLOC_MAX_DEVICES 64
+int aq_state_error_noalloc(const void* d_a, int32_t a_f64, const void* d_b, int32_t b_f64,
+                           int64_t n, int32_t n_slots, double* h_sq, double* h_max,
+                           void* stream);
+
 /* ------------------------------------------------ sensitivity surrogate */
 
 /* MLP in -> h -> h -> out (GELU on the hidden layers) predicting per-field
