@@ -161,14 +161,20 @@ void* jit_k_step(int D, bool HF, bool HM, bool f64, const aq_layout& L, std::str
   std::string src = "#include \"aq_kernels.cuh\"\nnamespace aq {\n";
   src += jit_layout_source(L);
   src += "}\n";
+  // AQ_JIT_SOURCE_DIR (environment, kernel development): compile from the
+  // aq_kernels.cuh found in this folder (and the headers it includes from
+  // there) instead of the copies embedded in the library at build time
+  const char* sdir = getenv("AQ_JIT_SOURCE_DIR");
+  const bool from_dir = sdir && *sdir;
   std::string key = std::string(name) + "\n" + src;
   if (const char* e = getenv("AQ_JIT_DEFINES")) key += std::string("\n") + e;
+  if (from_dir) key += std::string("\n") + sdir;
   auto hit = g_cache.find(key);
   if (hit != g_cache.end()) return (void*)hit->second;
 
   nvrtcProgram prog;
-  if (g_nv.create(&prog, src.c_str(), "aq_jit_step.cu", kAqJitHeaderCount, kAqJitHeaderSrc, kAqJitHeaderName) !=
-      NVRTC_SUCCESS) {
+  if (g_nv.create(&prog, src.c_str(), "aq_jit_step.cu", from_dir ? 0 : kAqJitHeaderCount,
+                  from_dir ? nullptr : kAqJitHeaderSrc, from_dir ? nullptr : kAqJitHeaderName) != NVRTC_SUCCESS) {
     if (err) *err = "nvrtcCreateProgram failed";
     return nullptr;
   }
@@ -187,6 +193,7 @@ void* jit_k_step(int D, bool HF, bool HM, bool f64, const aq_layout& L, std::str
       }
     }
   }
+  if (from_dir) extra.push_back(std::string("-I") + sdir);
   std::vector<const char*> opts = {"--gpu-architecture=sm_100a", "-std=c++17", "-lineinfo", "-DAQ_JIT=1"};
   for (const std::string& x : extra) opts.push_back(x.c_str());
   const nvrtcResult rc = g_nv.compile(prog, (int)opts.size(), opts.data());

@@ -11,6 +11,7 @@
 #include <stdio.h>
 #include <string.h>
 
+#include <algorithm>
 #include <new>
 #include <string>
 
@@ -293,6 +294,51 @@ __global__ void __launch_bounds__(256) k_loss(const __grid_constant__ aq_layout 
   }
 }
 
+// Per-slot statistics of the decoded state (features of the sensitivity
+// surrogate).  blockIdx.y is the slot; out[slot * 5 + k] accumulates
+// k = 0: sum |v|, 1: sum v, 2: sum v^2, 3: max |v| (as the bit pattern of a
+// non-negative double, which orders like the value), 4: sum |v - ref|
+// (ref: n x n_slots values in particle order, or null).
+template <class T>
+__global__ void __launch_bounds__(256) k_field_stats(const __grid_constant__ aq_layout L,
+                                                     const uint64_t* __restrict__ words,
+                                                     const int32_t* __restrict__ pid, const T* __restrict__ ref,
+                                                     int64_t n, double* __restrict__ out) {
+  __shared__ double sh[8][5];
+  const int s = blockIdx.y, ns = L.n_slots;
+  double a[5] = {0, 0, 0, 0, 0};
+  for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x) {
+    const double v = decode_slot<double>(L, s, words + i * L.n_words);
+    const double av = fabs(v);
+    a[0] += av;
+    a[1] += v;
+    a[2] += v * v;
+    a[3] = fmax(a[3], av);
+    if (ref) a[4] += fabs(v - (double)ref[(int64_t)pid[i] * ns + s]);
+  }
+#pragma unroll
+  for (int k = 16; k; k >>= 1) {
+#pragma unroll
+    for (int j = 0; j < 5; ++j) {
+      const double o = __shfl_xor_sync(0xffffffffu, a[j], k);
+      a[j] = j == 3 ? fmax(a[j], o) : a[j] + o;
+    }
+  }
+  const int warp = threadIdx.x >> 5;
+  if ((threadIdx.x & 31) == 0)
+    for (int j = 0; j < 5; ++j) sh[warp][j] = a[j];
+  __syncthreads();
+  if (threadIdx.x < 5) {
+    const int j = threadIdx.x;
+    double t = 0;
+    for (int w = 0; w < (int)(blockDim.x >> 5); ++w) t = j == 3 ? fmax(t, sh[w][j]) : t + sh[w][j];
+    if (j == 3)
+      atomicMax(reinterpret_cast<unsigned long long*>(out + s * 5 + 3), (unsigned long long)__double_as_longlong(t));
+    else
+      atomicAdd(out + s * 5 + j, t);
+  }
+}
+
 // ------------------------------------------------------------------ host
 
 struct SimBase {
@@ -325,6 +371,7 @@ struct aq_sim {
   unsigned long long* fallbacks = nullptr;
   double *rmax = nullptr, *rmin = nullptr;
   double* dloss = nullptr;
+  double* dstats = nullptr;  // aq_sim_field_stats accumulators, allocated on first use
   int ranges_on = 0;
   int64_t step = 0;
   int since_sort = 0;
@@ -536,7 +583,7 @@ static void free_sim(aq_sim* s) {
   }
   void* ptrs[] = {s->words[0], s->words[1], s->pid[0], s->pid[1], s->grid[0], s->grid[1], s->keys, s->ranks,
                   s->cell_count, s->cell_start, s->scan_sums, s->items, s->n_items, s->status, s->fallbacks,
-                  s->rmax, s->rmin, s->dloss};
+                  s->rmax, s->rmin, s->dloss, s->dstats};
   for (void* p : ptrs)
     if (p) cudaFree(p);
   delete s;
@@ -676,6 +723,27 @@ int aq_sim_get_state(aq_sim* s, void* values, int32_t values_f64, void* stream) 
                                                             s->n);
   AQ_CUDA_TRY(cudaGetLastError());
   s->launches += 1;
+  return AQ_OK;
+}
+
+int aq_sim_field_stats(aq_sim* s, const void* ref, int32_t ref_f64, double* h_out, void* stream) {
+  if (!s || !h_out) return AQ_E_ARG;
+  cudaStream_t st = as_stream(stream);
+  const size_t bytes = sizeof(double) * 5 * AQ_MAX_SLOTS;
+  if (!s->dstats) AQ_CUDA_TRY(cudaMalloc((void**)&s->dstats, bytes));
+  AQ_CUDA_TRY(cudaMemsetAsync(s->dstats, 0, bytes, st));
+  const unsigned nb = (unsigned)std::min<int64_t>(grid_for(s->n, 256), (int64_t)num_sms() * 4);
+  const dim3 grid(nb > 0 ? nb : 1, s->NS);
+  if (ref_f64)
+    k_field_stats<double><<<grid, 256, 0, st>>>(s->L, s->words[s->cur], s->pid[s->cur], (const double*)ref, s->n,
+                                                s->dstats);
+  else
+    k_field_stats<float><<<grid, 256, 0, st>>>(s->L, s->words[s->cur], s->pid[s->cur], (const float*)ref, s->n,
+                                               s->dstats);
+  AQ_CUDA_TRY(cudaGetLastError());
+  s->launches += 1;
+  AQ_CUDA_TRY(cudaMemcpyAsync(h_out, s->dstats, sizeof(double) * 5 * s->NS, cudaMemcpyDeviceToHost, st));
+  AQ_CUDA_TRY(cudaStreamSynchronize(st));
   return AQ_OK;
 }
 

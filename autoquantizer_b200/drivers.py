@@ -1,0 +1,324 @@
+"""The reference's experiment pipeline on libaq: range detection (-r), the
+gradient pass (-a), and scheme derivation followed by quantized forward runs
+(-f), for the deterministic 2D experiments of mpm_exps/ and a 3D elastic
+block.
+
+    python -m autoquantizer_b200.drivers elastic_2d -r            # ranges/elastic_2d/elastic_2d.npy
+    python -m autoquantizer_b200.drivers elastic_2d -a            # grads/elastic_2d/elastic_2d.npy
+    python -m autoquantizer_b200.drivers elastic_2d -f -m 1 -e 0.1 -N 20
+
+Flags follow the reference drivers (run_mpm_elastic_2d.py:18-50): -a
+gradients, -r ranges, -f solve + forward, -e epsilon, -m mode (0 compression
+rate, 1 error bound).  Additions: --root (folder holding grads/ and ranges/,
+default the working directory), -N (forward runs), --timesteps (shorter
+horizons), --json (one summary line).
+
+Experiments:
+  elastic_2d  run_mpm_elastic_2d.py:54-122 — 80,000 particles in eight
+              lattice cubes, 128^2, dt 2e-4, 8193 timesteps, E 50, f64.
+  fluid_2d    run_mpm_fluid_2d.py:185-214 — 10,000 particles in one lattice
+              cube, 128^2, dt 2e-4, 16385 timesteps, bulk modulus 500, f64;
+              compression-rate mode only, with the driver's own solver
+              variant (run_mpm_fluid_2d.py:129-145).
+  falling_block_3d  the 3D elastic block of the adjoint benchmark (262,144
+              particles, 64^3, dt 5e-5, 257 timesteps, f32); scheme recipe of
+              run_mpm_elastic_3d.py:331-341 (ranges doubled, CR, bits + 1).
+The reference's 3D letter/propeller experiments need mesh emitters and the
+SDF collider, which this package does not implement.
+
+Each forward run re-seeds the dithering generator (seed = run index), which
+plays the role of the reference's per-run random state.
+"""
+import argparse
+import json
+import os
+import sys
+
+import numpy as np
+
+from .mpm_config import MPMConfig
+from .solvers import LagrangianCR, LagrangianEB
+
+CR, EB = 0, 1
+
+
+def lagrangian_cr_fluid_2d(grads, r=0.5, a=None):
+    """The compression-rate solver as run_mpm_fluid_2d.py:129-145 defines it
+    locally: multiplier 2·ln2 inside the log and bits rounded up, with no
+    separate sign bit added afterwards."""
+    grads = np.asarray(grads, dtype=np.float64)
+    n = len(grads)
+    r = r * 32.0 - 1
+    a = np.ones(n) if a is None else np.asarray(a, dtype=np.float64)
+    b = a / grads
+    t = np.log2(b)
+    log_la = -r * 2 - t @ a / np.sum(a) + np.log2(2 * np.log(2))
+    la = np.power(2, log_la)
+    fun = (b * la) @ grads / 12.0
+    bits = np.ceil(-(t + log_la) / 2.0).astype(np.int32)
+    return bits, fun
+
+
+class Experiment:
+    name = None
+    file_name = None
+    f64_data = None  # unquantized loss the error-bound mode measures against
+    modes = (CR, EB)
+
+    def config(self):
+        raise NotImplementedError
+
+    def init(self, mpm):
+        raise NotImplementedError
+
+    def scheme(self, grads, ranges, mode, eps):
+        raise NotImplementedError
+
+
+class Elastic2D(Experiment):
+    """run_mpm_elastic_2d.py:54-122 (config, init) and :232-250 (solve)."""
+
+    name = "elastic_2d"
+    file_name = "elastic_2d.npy"
+    f64_data = 6893.409
+
+    def config(self):
+        c = MPMConfig()
+        c.dim = 2
+        c.E = 5e1
+        c.id = "elastic_2d_err_bound"
+        c.la = 1e3
+        c.bound = [3, 3]
+        c.use_friction = False
+        c.use_fluid = False
+        c.n_particles = 80000
+        c.dt = 2e-4
+        c.n_grid = 128
+        c.n_timesteps = 1024 * 8 + 1
+        c.steps = 64
+        c.size = 1
+        c.p_rho = 1.0
+        c.p_vol = (1 / c.n_grid * 0.5) ** c.dim
+        c.quantized_properties = {"x": 1, "v": 1, "C": 1, "F": 1}
+        c.quant_bits = np.array([32] * 12)
+        c.quant_ranges = np.array([2.0] * 12)
+        c.precision = "f64"  # ti.init(default_fp=ti.float64)
+        return c
+
+    def init(self, mpm):
+        mpm.initialize()
+        n = mpm.param.n_particles // 8
+        for i in range(4):
+            mpm.add_cube(((0.2 + i * 0.4) / 4, (0.2 + i * 0.8) / 4), (0.7 / 4, 0.7 / 4), n)
+        for i in range(4):
+            mpm.add_cube(((3.1 - i * 0.2) / 4, (0.2 + i * 0.8) / 4), (0.7 / 4, 0.7 / 4), n)
+
+    def scheme(self, grads, ranges, mode, eps):
+        d = 2
+        ranges = np.array(ranges, dtype=np.float64)
+        ranges[:d] = 1.0
+        ranges[d:] *= 2.0
+        if mode == CR:
+            bits, _ = LagrangianCR(grads=grads * ranges ** 2, r=eps)
+        else:
+            bits, _ = LagrangianEB(grads=grads * ranges ** 2, ref=self.f64_data, tol_rel=eps)
+        return bits + 1, ranges
+
+
+class Fluid2D(Experiment):
+    """run_mpm_fluid_2d.py:116-127 (init), :162-178 (solve), :185-214 (config)."""
+
+    name = "fluid_2d"
+    file_name = "fluid_2d_t16385_dt0.0002_p10000_g128.npy"
+    modes = (CR,)
+
+    def config(self):
+        c = MPMConfig()
+        c.dim = 2
+        c.E = 5e4
+        c.id = "fluid_2d_mem_bound"
+        c.la = 5e2
+        c.bound = [3, 3]
+        c.use_friction = False
+        c.quant_ranges = np.ones(9)
+        c.quantized_properties = {"x": 1, "v": 1, "C": 1, "J": 1}
+        c.quant_bits = np.ones(9)
+        c.n_particles = 10000
+        c.dt = 2e-4
+        c.n_grid = 128
+        c.n_timesteps = 1024 * 16 + 1
+        c.steps = 128
+        c.size = 1
+        c.precision = "f64"
+        return c
+
+    def init(self, mpm):
+        mpm.initialize()
+        dx = 1 / mpm.param.n_grid
+        b = mpm.param.bound
+        mpm.add_cube((b[0] * dx, b[1] * dx), (1.5 / 4, 1.5 / 4), mpm.param.n_particles)
+
+    def scheme(self, grads, ranges, mode, eps):
+        if mode != CR:
+            raise ValueError("fluid_2d runs the compression-rate mode only (run_mpm_fluid_2d.py:182)")
+        ranges = np.array(ranges, dtype=np.float64)
+        ranges[:2] = 1.0
+        ranges[2:] *= 2.0
+        g = np.asarray(grads, dtype=np.float64)
+        g = g / g.min()
+        bits, _ = lagrangian_cr_fluid_2d(g * ranges ** 2, r=eps)
+        return bits, ranges
+
+
+class FallingBlock3D(Experiment):
+    """The 3D elastic block of the adjoint benchmark, with the scheme recipe
+    of run_mpm_elastic_3d.py:331-341."""
+
+    name = "falling_block_3d"
+    file_name = "falling_block_3d.npy"
+
+    def config(self):
+        from . import scenes
+
+        c, vals = scenes.falling_block_3d()
+        c.n_timesteps = 257
+        c.steps = 16
+        c.quantized_properties = {"x": 1, "v": 1, "C": 1, "F": 1}
+        c.quant_bits = np.array([32] * 24)
+        c.quant_ranges = np.array([2.0] * 24)
+        c.compute_fp = "f32"
+        self._vals = vals
+        return c
+
+    def init(self, mpm):
+        mpm.initialize()
+        mpm.set_particles(self._vals)
+
+    def scheme(self, grads, ranges, mode, eps):
+        ranges = np.array(ranges, dtype=np.float64) * 2.0
+        ranges[:3] = 1.0
+        if mode == CR:
+            bits, _ = LagrangianCR(grads * ranges ** 2, r=eps)
+        else:
+            ref = self.f64_data if self.f64_data is not None else 1.0
+            bits, _ = LagrangianEB(grads * ranges ** 2, ref=ref, tol_rel=eps)
+        return bits + 1, ranges
+
+
+EXPERIMENTS = {e.name: e for e in (Elastic2D, Fluid2D, FallingBlock3D)}
+
+
+def _paths(exp, root):
+    g = os.path.join(root, "grads", exp.name)
+    r = os.path.join(root, "ranges", exp.name)
+    return os.path.join(g, exp.file_name), os.path.join(r, exp.file_name)
+
+
+def _solver(exp, cfg):
+    from .mpm_solver import MPMSolver
+
+    mpm = MPMSolver(cfg)
+    exp.init(mpm)
+    return mpm
+
+
+def ad(exp, cfg, root, every=64):
+    """The drivers' ad(): the gradient pass, saved as grads/<exp>/<file>."""
+    cfg.use_difftaichi = True
+    cfg.use_quantaichi = False
+    mpm = _solver(exp, cfg)
+    loss = mpm.run_forward_with_ad_nlogn(every=every)
+    g = mpm.get_gradients()
+    fn, _ = _paths(exp, root)
+    os.makedirs(os.path.dirname(fn), exist_ok=True)
+    np.save(fn, g)
+    return {"loss": float(loss), "grads": g.tolist(), "file": fn}
+
+
+def detect_range(exp, cfg, root):
+    """The drivers' detect_range(): unquantized forward with running
+    max/min, saved as ranges/<exp>/<file>."""
+    cfg.use_quantaichi = False
+    mpm = _solver(exp, cfg)
+    ranges = mpm.run_forward_detect_ranges()
+    _, fn = _paths(exp, root)
+    os.makedirs(os.path.dirname(fn), exist_ok=True)
+    np.save(fn, ranges)
+    return {"ranges": ranges.tolist(), "file": fn, "max": mpm._rmax.tolist(), "min": mpm._rmin.tolist()}
+
+
+def solve(exp, cfg, root, mode, eps):
+    """The drivers' solve(): bits and ranges from the saved gradients and
+    ranges, written into the config."""
+    gfn, rfn = _paths(exp, root)
+    grads, ranges = np.load(gfn), np.load(rfn)
+    bits, ranges = exp.scheme(grads, ranges, mode, eps)
+    cfg.quant_bits = np.asarray(bits)
+    cfg.quant_ranges = np.asarray(ranges)
+    return {"bits": [int(b) for b in bits], "ranges": ranges.tolist(),
+            "compression_rate": float(np.sum(bits) / (32 * len(bits)))}
+
+
+def run(exp, cfg, n_runs, quant=True):
+    """The drivers' run(N, quant=True): N forward runs, loss of each."""
+    if quant:
+        cfg.use_difftaichi = False
+        cfg.use_bls = True
+        cfg.use_bitpack = True
+        cfg.use_quantaichi = True
+    losses = []
+    for i in range(n_runs):
+        cfg.seed = i
+        mpm = _solver(exp, cfg)
+        losses.append(float(mpm.run_forward_only()))
+        if mpm.status()[0] != 0:
+            raise RuntimeError("simulator status flags 0x%x in run %d" % (mpm.status()[0], i))
+        mpm._drop_sim()
+    return np.array(losses)
+
+
+def main(argv=None):
+    ap = argparse.ArgumentParser()
+    ap.add_argument("experiment", choices=sorted(EXPERIMENTS))
+    ap.add_argument("-a", "--ad", action="store_true", help="compute gradients")
+    ap.add_argument("-r", "--ranges", action="store_true", help="detect ranges")
+    ap.add_argument("-f", "--forward", action="store_true", help="solve the scheme and run quantized")
+    ap.add_argument("-e", "--epsilon", type=float, default=0.1)
+    ap.add_argument("-m", "--mode", type=int, default=CR, help="0 compression rate, 1 error bound")
+    ap.add_argument("-N", "--runs", type=int, default=20)
+    ap.add_argument("--root", default=".")
+    ap.add_argument("--timesteps", type=int, default=None)
+    ap.add_argument("--json", action="store_true")
+    args = ap.parse_args(argv)
+
+    exp = EXPERIMENTS[args.experiment]()
+    cfg = exp.config()
+    if args.timesteps:
+        cfg.n_timesteps = args.timesteps
+    if args.ad:
+        out = ad(exp, cfg, args.root)
+    elif args.ranges:
+        out = detect_range(exp, cfg, args.root)
+    elif args.forward:
+        if args.mode not in exp.modes:
+            ap.error("%s has no mode %d" % (exp.name, args.mode))
+        out = solve(exp, cfg, args.root, args.mode, args.epsilon)
+        loss = run(exp, cfg, args.runs)
+        out.update({"loss_mean": float(loss.mean()), "loss_std": float(loss.std()),
+                    "loss_max": float(loss.max()), "loss_min": float(loss.min()), "losses": loss.tolist()})
+        if args.mode == EB and exp.f64_data is not None:
+            tar = args.epsilon * exp.f64_data
+            out["succeed"] = float(np.mean(np.abs(loss - exp.f64_data) < tar * 3))
+    else:
+        ap.error("one of -a, -r, -f")
+    out["experiment"] = exp.name
+    if args.json:
+        print(json.dumps(out))
+    else:
+        for k, v in out.items():
+            print("%s: %s" % (k, v))
+    return out
+
+
+if __name__ == "__main__":
+    main(sys.argv[1:])

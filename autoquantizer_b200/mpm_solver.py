@@ -184,16 +184,28 @@ class MPMSolver:
 
     def initialize(self):
         """mpm_solver.py:564-576: F = I (or J = 1), C = 0, no particles."""
-        n, d = self.n_particles, self.dim
-        self._host = np.zeros((n, self.n_slots()), dtype=np.float64)
-        a, b = self.slot_range("F" if self.has_F else "J")
-        if self.has_F:
-            self._host[:, a:b] = np.eye(d).ravel()
-        else:
-            self._host[:, a] = 1.0
+        self._host = None  # built on first use (_staging)
+        self._dev = None
         self.current_idx = 0
         self.loss[None] = 0.0
         self._drop_sim()
+
+    def _staging(self):
+        """Host staging array (n_particles x n_slots, float64), created on
+        first use with F = I (or J = 1); holds device-provided initial values
+        once something needs them on the host."""
+        if self._host is None:
+            n, d = self.n_particles, self.dim
+            h = np.zeros((n, self.n_slots()), dtype=np.float64)
+            a, b = self.slot_range("F" if self.has_F else "J")
+            if self.has_F:
+                h[:, a:b] = np.eye(d).ravel()
+            else:
+                h[:, a] = 1.0
+            if self._dev is not None:
+                h[: self._dev.shape[0]] = self._dev.double().cpu().numpy()
+            self._host = h
+        return self._host
 
     def _drop_sim(self):
         if self._sim is not None:
@@ -204,12 +216,15 @@ class MPMSolver:
     def _pull(self):
         """Copy the simulator's state back into the host staging array."""
         if self._sim is not None and not self._dirty:
-            self._host[: self.current_idx] = self.state_values()
+            self._staging()[: self.current_idx] = self.state_values()
+            self._dev = None
 
     def add_cube(self, low_corner, box_size, num, material=0):
         """3D: uniform random positions (fill_in_box, :1573-1590); 2D: the
         deterministic lattice of fill_in_box_2duniform (:1561-1571)."""
         self._pull()
+        self._staging()
+        self._dev = None
         d = self.dim
         st = self.current_idx
         if d == 3 or len(low_corner) == 3:
@@ -234,9 +249,20 @@ class MPMSolver:
         self._drop_sim()
 
     def set_particles(self, values):
-        """Set all active particles from an (n x n_slots) array."""
+        """Set all active particles from an (n x n_slots) array: numpy (host),
+        or a CUDA float32/float64 tensor, which the simulator then encodes
+        straight from device memory."""
+        if getattr(values, "is_cuda", False):
+            if values.dim() != 2 or values.shape[1] != self.n_slots() or values.shape[0] > self.n_particles:
+                raise ValueError("set_particles: expected (<= %d) x %d values" % (self.n_particles, self.n_slots()))
+            self._dev = values.contiguous()
+            self._host = None
+            self.current_idx = values.shape[0]
+            self._drop_sim()
+            return
         v = np.asarray(values, dtype=np.float64)
-        self._host[: v.shape[0]] = v
+        self._staging()[: v.shape[0]] = v
+        self._dev = None
         self.current_idx = v.shape[0]
         self._drop_sim()
 
@@ -254,8 +280,14 @@ class MPMSolver:
             _lib.check(_lib.lib().aq_sim_create(C.byref(self._params()), C.byref(self.layout()), C.byref(sim)),
                        "aq_sim_create")
             self._sim = sim
-        vals = torch.from_numpy(np.ascontiguousarray(self._host[: self.current_idx])).cuda()
-        _lib.check(_lib.lib().aq_sim_set_state(self._sim, C.c_void_p(vals.data_ptr()), 1, _lib.stream_ptr()),
+        if self._dev is not None and self._host is None:
+            vals = self._dev
+            if vals.dtype not in (torch.float32, torch.float64):
+                vals = vals.double()
+        else:
+            vals = torch.from_numpy(np.ascontiguousarray(self._staging()[: self.current_idx])).cuda()
+        _lib.check(_lib.lib().aq_sim_set_state(self._sim, C.c_void_p(vals.data_ptr()),
+                                               int(vals.dtype == torch.float64), _lib.stream_ptr()),
                    "aq_sim_set_state")
         torch.cuda.current_stream().synchronize()
         self._dirty = False
@@ -280,6 +312,27 @@ class MPMSolver:
         _lib.check(_lib.lib().aq_sim_loss(self._sim, 0, C.byref(out), _lib.stream_ptr()), "aq_sim_loss")
         self.loss[None] = out.value
         return out.value
+
+    def field_stats(self, reference=None):
+        """Per-slot statistics of the current state on the device
+        (aq_sim_field_stats): an (n_slots x 5) array of sum |v|, sum v,
+        sum v^2, max |v| and sum |v - reference| (reference: a CUDA tensor of
+        initial values in particle order, or None)."""
+        import torch
+
+        self._ensure_sim()
+        ns = self.n_slots()
+        out = (C.c_double * (5 * ns))()
+        if reference is not None:
+            if not reference.is_cuda or reference.dtype not in (torch.float32, torch.float64) or \
+                    tuple(reference.shape) != (self.current_idx, ns) or not reference.is_contiguous():
+                raise ValueError("field_stats: reference must be a contiguous CUDA float tensor of %d x %d"
+                                 % (self.current_idx, ns))
+            ref, f64 = C.c_void_p(reference.data_ptr()), int(reference.dtype == torch.float64)
+        else:
+            ref, f64 = None, 0
+        _lib.check(_lib.lib().aq_sim_field_stats(self._sim, ref, f64, out, _lib.stream_ptr()), "aq_sim_field_stats")
+        return np.array(out[:]).reshape(ns, 5)
 
     # ------------------------------------------------------------- state
 
@@ -330,7 +383,8 @@ class MPMSolver:
         """mpm_solver.py:1832-1867."""
         self._pull()
         a, b = self.slot_range(name)
-        self._host[: len(data), a:b] = np.asarray(data, dtype=np.float64).reshape(len(data), b - a)
+        self._staging()[: len(data), a:b] = np.asarray(data, dtype=np.float64).reshape(len(data), b - a)
+        self._dev = None
         self._dirty = True
         if self._sim is not None:
             self._ensure_sim()
@@ -405,7 +459,10 @@ class MPMSolver:
         n, ns = self.current_idx, self.n_slots()
         adj = Adjoint(P)
         dt = torch.float64 if self.param.precision == "f64" else torch.float32
-        s0 = torch.from_numpy(np.ascontiguousarray(self._host[:n, :ns])).to("cuda", dt)
+        if self._dev is not None and self._host is None:
+            s0 = self._dev[:n, :ns].to(dt).contiguous()
+        else:
+            s0 = torch.from_numpy(np.ascontiguousarray(self._staging()[:n, :ns])).to("cuda", dt)
         sT = adj.forward(s0, self.n_timestep - 1, every)
         loss = ek_loss(sT, self.dim, self.p_mass, self.g)
         adj.backward(ek_seed(sT, self.dim, self.p_mass, self.g))

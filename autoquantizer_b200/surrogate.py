@@ -101,49 +101,57 @@ def groups_of(dim, fluid):
     return g
 
 
-def features(cfg, s_a, s_b):
+def features(cfg, stats, n):
+    """64 features from the per-slot statistics of the end-of-window state
+    (MPMSolver.field_stats: sum |v|, sum v, sum v^2, max |v|, sum |v - v0|):
+    per group mean |.|, std, max |.| and mean |change over the window|
+    (48), plus 16 scene descriptors."""
     dim, fluid = cfg.dim, cfg.use_fluid
     f = np.zeros(N_IN)
     for gi, slots in enumerate(groups_of(dim, fluid)):
         if not slots:
             continue
-        b = s_b[:, slots]
-        a = s_a[:, slots]
-        f[4 * gi + 0] = np.log10(np.mean(np.abs(b)) + 1e-12)
-        f[4 * gi + 1] = np.log10(np.std(b) + 1e-12)
-        f[4 * gi + 2] = np.log10(np.max(np.abs(b)) + 1e-12)
-        f[4 * gi + 3] = np.log10(np.mean(np.abs(b - a)) + 1e-12)
-    n = s_b.shape[0]
-    v = s_b[:, dim:2 * dim]
+        st = stats[slots]
+        cnt = float(n * len(slots))
+        mean_abs = st[:, 0].sum() / cnt
+        mean = st[:, 1].sum() / cnt
+        var = max(st[:, 2].sum() / cnt - mean * mean, 0.0)
+        f[4 * gi + 0] = np.log10(mean_abs + 1e-12)
+        f[4 * gi + 1] = np.log10(np.sqrt(var) + 1e-12)
+        f[4 * gi + 2] = np.log10(st[:, 3].max() + 1e-12)
+        f[4 * gi + 3] = np.log10(st[:, 4].sum() / cnt + 1e-12)
+    vs = stats[dim:2 * dim]
     g = [dim / 3.0, float(fluid), np.log10(cfg.E) / 5, cfg.nu, np.log10(cfg.la) / 4, np.log10(n) / 6,
          np.log10(cfg.dt) / 4, np.log10(1.0 / cfg.n_grid), np.log10(cfg.p_vol * cfg.p_rho) / 10, cfg.g / 10,
-         np.log10(np.mean(np.abs(v)) + 1e-9), np.log10(0.5 * np.sum(v * v) * cfg.p_vol + 1e-12) / 5,
-         (cfg.n_timesteps - 1) / 100.0, float(np.mean(s_b[:, 1] < 0.1)), WINDOW / 16.0, 1.0]
+         np.log10(vs[:, 0].sum() / (n * dim) + 1e-9), np.log10(0.5 * vs[:, 2].sum() * cfg.p_vol + 1e-12) / 5,
+         (cfg.n_timesteps - 1) / 100.0, stats[1, 1] / n, WINDOW / 16.0, 1.0]
     f[48:64] = g
     return f
 
 
-def window_states(cfg, vals):
-    """Run the 16-substep feature window on the fast simulator (FP32 state)."""
+def window_stats(cfg, s0):
+    """Run the 16-substep feature window on the simulator from the initial
+    values s0 (CUDA tensor, particle order) and return the per-slot
+    statistics of the end state against s0."""
     from .mpm_solver import MPMSolver
 
     s = MPMSolver(cfg)
-    s.set_particles(vals)
+    s.set_particles(s0)
     s.substeps(WINDOW)
-    return vals, s.state_values()
+    st = s.field_stats(reference=s0)
+    s._drop_sim()
+    return st
 
 
-def adjoint_sensitivities(cfg, vals, every=16):
-    """Per-slot sensitivities of compute_ek over the scene's horizon."""
-    import torch
-
+def adjoint_sensitivities(cfg, s0, every=16):
+    """Per-slot sensitivities of compute_ek over the scene's horizon, from
+    the initial values s0 (CUDA float32 tensor)."""
     from .adjoint import Adjoint, ek_loss, ek_seed
     from .mpm_solver import MPMSolver
 
     s = MPMSolver(cfg)
-    s.set_particles(vals)
+    s.set_particles(s0)
     adj = Adjoint(s._params())
-    s0 = torch.from_numpy(np.ascontiguousarray(vals)).to("cuda", torch.float32)
     sT = adj.forward(s0, cfg.n_timesteps - 1, every)
     loss = ek_loss(sT, cfg.dim, s.p_mass, s.g)
     _, sens = adj.backward(ek_seed(sT, cfg.dim, s.p_mass, s.g))
@@ -161,29 +169,33 @@ def group_sensitivities(cfg, sens):
     return out, mask
 
 
-def group_ranges(cfg, s_b):
+def group_ranges(cfg, stats):
     """Per-group ranges as the drivers' solve() sets them: positions 1, the
-    others twice the detected max |.| (run_mpm_elastic_2d.py:227-242)."""
+    others twice the detected max |.| (run_mpm_elastic_2d.py:227-242), the
+    max taken from the window statistics."""
     r = np.ones(N_OUT)
     for gi, slots in enumerate(groups_of(cfg.dim, cfg.use_fluid)):
         if slots and gi >= 3:
-            r[gi] = 2.0 * max(np.max(np.abs(s_b[:, slots])), 1e-6)
+            r[gi] = 2.0 * max(float(stats[slots, 3].max()), 1e-6)
     return r
 
 
 def make_dataset(n_scenes, seed, n_min=10_000, n_max=500_000, horizon=64, log=None):
+    import torch
+
     rng = np.random.default_rng(seed)
     X, Y, M, meta = [], [], [], []
     for i in range(n_scenes):
         cfg, vals = random_scene(rng, n_min, n_max, horizon)
-        a, b = window_states(cfg, vals)
-        sens, loss = adjoint_sensitivities(cfg, vals)
+        s0 = torch.from_numpy(vals).to("cuda", torch.float32)
+        st = window_stats(cfg, s0)
+        sens, loss = adjoint_sensitivities(cfg, s0)
         y, m = group_sensitivities(cfg, sens)
-        X.append(features(cfg, a, b))
+        X.append(features(cfg, st, vals.shape[0]))
         Y.append(y)
         M.append(m)
         meta.append({"dim": cfg.dim, "fluid": bool(cfg.use_fluid), "n": int(vals.shape[0]), "loss": float(loss),
-                     "ranges": group_ranges(cfg, b).tolist()})
+                     "ranges": group_ranges(cfg, st).tolist()})
         if log and (i + 1) % 32 == 0:
             log("scene %d/%d" % (i + 1, n_scenes))
     return np.array(X), np.array(Y), np.array(M), meta
@@ -336,25 +348,28 @@ def evaluate(mlp, X, Y, M, meta, tol_rel=1e-3, baseline=None):
 
 
 def timing_comparison(cfg, vals, mlp):
-    """Wall time of deriving a scheme with the surrogate (feature window +
-    inference + solver) vs with the adjoint (full forward + backward)."""
+    """Wall time of deriving a scheme from initial values already on the
+    device, with the surrogate (feature window + statistics + inference +
+    solver) and with the adjoint (full forward + backward + solver)."""
     import torch
 
+    s0 = torch.from_numpy(vals).to("cuda", torch.float32)
+    n = vals.shape[0]
     torch.cuda.synchronize()
     t0 = time.perf_counter()
-    a, b = window_states(cfg, vals)
-    y = mlp.predict(features(cfg, a, b)[None])[0]
-    _, mask = group_sensitivities(cfg, np.ones(2 * cfg.dim + cfg.dim ** 2 + (1 if cfg.use_fluid else cfg.dim ** 2)))
-    scheme_bits(y, mask, group_ranges(cfg, b), 1.0)
+    st = window_stats(cfg, s0)
+    y = mlp.predict(features(cfg, st, n)[None])[0]
+    _, mask = group_sensitivities(cfg, np.ones(st.shape[0]))
+    b_sur = scheme_bits(y, mask, group_ranges(cfg, st), 1.0)
     torch.cuda.synchronize()
     t_sur = time.perf_counter() - t0
     t0 = time.perf_counter()
-    sens, loss = adjoint_sensitivities(cfg, vals)
+    sens, loss = adjoint_sensitivities(cfg, s0)
     ys, mask = group_sensitivities(cfg, sens)
-    scheme_bits(ys, mask, group_ranges(cfg, b), loss)
+    b_adj = scheme_bits(ys, mask, group_ranges(cfg, st), loss)
     torch.cuda.synchronize()
     t_adj = time.perf_counter() - t0
-    return t_sur, t_adj
+    return t_sur, t_adj, b_sur, b_adj
 
 
 def main():
@@ -365,10 +380,20 @@ def main():
     ap.add_argument("--horizon", type=int, default=64)
     ap.add_argument("--steps", type=int, default=3000)
     ap.add_argument("--out", default=None)
+    ap.add_argument("--save-data", default=None, help="write the generated datasets to this .npz")
+    ap.add_argument("--load-data", default=None, help="read datasets written by --save-data instead")
     args = ap.parse_args()
     t0 = time.perf_counter()
-    Xtr, Ytr, Mtr, _ = make_dataset(args.train, 1, n_max=args.n_max, horizon=args.horizon, log=print)
-    Xte, Yte, Mte, mte = make_dataset(args.test, 2, n_max=args.n_max, horizon=args.horizon, log=print)
+    if args.load_data:
+        z = np.load(args.load_data, allow_pickle=False)
+        Xtr, Ytr, Mtr, Xte, Yte, Mte = (z[k] for k in ("Xtr", "Ytr", "Mtr", "Xte", "Yte", "Mte"))
+        mte = json.loads(str(z["meta_te"]))
+    else:
+        Xtr, Ytr, Mtr, mtr = make_dataset(args.train, 1, n_max=args.n_max, horizon=args.horizon, log=print)
+        Xte, Yte, Mte, mte = make_dataset(args.test, 2, n_max=args.n_max, horizon=args.horizon, log=print)
+        if args.save_data:
+            np.savez(args.save_data, Xtr=Xtr, Ytr=Ytr, Mtr=Mtr, Xte=Xte, Yte=Yte, Mte=Mte,
+                     meta_tr=json.dumps(mtr), meta_te=json.dumps(mte))
     t_data = time.perf_counter() - t0
     mlp = MLP(seed=0)
     t0 = time.perf_counter()
@@ -378,13 +403,14 @@ def main():
     sur, bl = evaluate(mlp, Xte, Yte, Mte, mte, baseline=base)
     rng = np.random.default_rng(3)
     cfg, vals = random_scene(rng, args.n_max // 2, args.n_max, horizon=args.horizon)
-    t_sur, t_adj = timing_comparison(cfg, vals, mlp)
-    t_sur, t_adj = timing_comparison(cfg, vals, mlp)  # warm (JIT caches)
+    timing_comparison(cfg, vals, mlp)  # warm-up (kernel compilation, allocator)
+    t_sur, t_adj, b_sur, b_adj = timing_comparison(cfg, vals, mlp)
     rep = {"train_scenes": args.train, "test_scenes": args.test, "horizon": args.horizon, "window": WINDOW,
            "dataset_seconds": t_data, "fit_seconds": t_fit, "loss_history": hist, "surrogate": sur,
            "baseline_mean_predictor": bl, "scheme_seconds": {"surrogate": t_sur, "adjoint": t_adj,
                                                             "speedup": t_adj / t_sur},
-           "timing_scene": {"dim": cfg.dim, "fluid": bool(cfg.use_fluid), "n": int(vals.shape[0])}}
+           "timing_scene": {"dim": cfg.dim, "fluid": bool(cfg.use_fluid), "n": int(vals.shape[0]),
+                            "bits_surrogate": b_sur.tolist(), "bits_adjoint": b_adj.tolist()}}
     print(json.dumps(rep, indent=1))
     if args.out:
         with open(args.out, "w") as f:

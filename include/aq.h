@@ -198,6 +198,14 @@ int aq_sim_substeps(aq_sim* sim, int32_t n, void* stream);
  * 2D sum |v|^2. */
 int aq_sim_loss(aq_sim* sim, int32_t kind, double* h_out, void* stream);
 
+/* Per-slot statistics of the current decoded state, the inputs of the
+ * sensitivity surrogate's features (no counterpart in the reference).
+ * h_out receives n_slots x 5 doubles: sum |v|, sum v, sum v^2, max |v|,
+ * sum |v - ref|, where d_ref (optional, null skips the last one) holds
+ * n x n_slots values in particle order, f64 if ref_f64 else f32.
+ * Synchronizes the stream. */
+int aq_sim_field_stats(aq_sim* sim, const void* d_ref, int32_t ref_f64, double* h_out, void* stream);
+
 /* Per-slot running max/min of the state (range detection), accumulated on
  * the device after every substep once enabled.
  * Replaces update_limits_* / get_limits (mpm_solver.py:944-997). */

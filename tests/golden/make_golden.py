@@ -12,9 +12,14 @@ Writes reference_data.json:
     (solvers/analytical_solver.py, imported from the checkout) on those
     sensitivities, as the drivers' solve() calls them
     (run_mpm_elastic_2d.py:227-242), for several error bounds and
-    compression rates.
+    compression rates;
+  * outputs of the compression-rate solver that run_mpm_fluid_2d.py
+    defines locally (:129-145; only that function is taken out of the
+    script with ast and run, since the script itself imports Taichi), with
+    that driver's solve() recipe (:162-178).
 Nothing at test time reads the reference checkout; tests read the JSON.
 """
+import ast
 import glob
 import importlib.util
 import json
@@ -59,6 +64,22 @@ def main(ref):
             bits, fun = ana.LagrangianCR(grads=gw, r=rate)
             out["solver"].append({"key": key, "mode": "CR", "eps": rate, "grads_weighted": gw.tolist(),
                                   "bits": bits.tolist(), "fun": float(fun)})
+    # solve() of run_mpm_fluid_2d.py with its own LagrangianCR
+    src = open(os.path.join(ref, "mpm_exps", "run_mpm_fluid_2d.py")).read()
+    fn = [n for n in ast.parse(src).body if isinstance(n, ast.FunctionDef) and n.name == "LagrangianCR"][0]
+    ns = {"np": np}
+    exec(compile(ast.Module(body=[fn], type_ignores=[]), "run_mpm_fluid_2d.py", "exec"), ns)
+    key = "fluid_2d/fluid_2d_t16385_dt0.0002_p10000_g128.npy"
+    out["driver_solver"] = []
+    for rate in (0.3, 0.5, 0.7):
+        g = np.array(out["grads"][key])
+        r = np.array(out["ranges"][key], dtype=np.float64)
+        r[:2] = 1.0
+        r[2:] *= 2.0
+        g = g / g.min()
+        bits, fun = ns["LagrangianCR"](g * r ** 2, r=rate)
+        out["driver_solver"].append({"driver": "fluid_2d", "key": key, "mode": "CR", "eps": rate,
+                                     "ranges": r.tolist(), "bits": bits.tolist(), "fun": float(fun)})
     with open(os.path.join(HERE, "reference_data.json"), "w") as f:
         json.dump(out, f, indent=1)
     print("wrote", os.path.join(HERE, "reference_data.json"))

@@ -1,0 +1,80 @@
+"""The experiment pipeline (-r, -a, -f) on the GPU.
+
+Range detection is pinned to the ranges the reference shipped for its
+deterministic 2D experiments (mpm_exps/ranges/elastic_2d/*.npy,
+mpm_exps/ranges/fluid_2d/*.npy; values in tests/golden/reference_data.json).
+The error-bound forward runs of the 2D elastic experiment, on the schemes
+solved from the reference's shipped sensitivities and ranges, must meet the
+success criterion of run_mpm_elastic_2d.py:190-205 (|loss - f64 loss| <
+3 * eps * f64 loss).
+"""
+import json
+import os
+
+import numpy as np
+import pytest
+
+from autoquantizer_b200 import drivers as D
+
+pytestmark = pytest.mark.gpu
+GOLD = json.load(open(os.path.join(os.path.dirname(__file__), "golden", "reference_data.json")))
+
+
+def test_elastic_2d_ranges_match_reference(tmp_path):
+    exp = D.Elastic2D()
+    out = D.detect_range(exp, exp.config(), str(tmp_path))
+    ours = np.array(out["ranges"])
+    a = np.array(GOLD["ranges"]["elastic_2d/elastic_2d.npy"])
+    b = np.array(GOLD["ranges"]["elastic_2d/elastic_2d_t8193_dt0.0002_p80000_g128.npy"])
+    print("elastic_2d ranges ours/reference:", np.array2string(ours / a, precision=6))
+    assert np.array_equal(np.load(out["file"]), ours)
+    # the two shipped files differ only in C_01 (549.96 vs 593.46); ours must
+    # match one of them there and both elsewhere
+    close = lambda x, y: np.abs(x - y) <= 1e-3 * np.abs(y)  # noqa: E731
+    assert np.all(close(ours, a) | close(ours, b)), (ours, a, b)
+
+
+def test_fluid_2d_ranges_match_reference(tmp_path):
+    """The shipped fluid_2d file holds max|J - 1| for J (the offset of J's
+    fixed-point type), not max|J| as the reference's current get_limits
+    returns; the test compares J that way and the rest directly."""
+    exp = D.Fluid2D()
+    out = D.detect_range(exp, exp.config(), str(tmp_path))
+    ours = np.array(out["ranges"])
+    ref = np.array(GOLD["ranges"]["fluid_2d/fluid_2d_t16385_dt0.0002_p10000_g128.npy"])
+    j_dev = max(abs(out["max"][-1] - 1.0), abs(out["min"][-1] - 1.0))
+    cmp = np.concatenate([ours[:-1], [j_dev]])
+    print("fluid_2d ranges ours/reference:", np.array2string(cmp / ref, precision=4))
+    assert ours[-1] == pytest.approx(max(abs(out["max"][-1]), abs(out["min"][-1])))
+    assert cmp == pytest.approx(ref, rel=0.05)
+
+
+def test_elastic_2d_error_bound_runs_meet_the_drivers_criterion(tmp_path):
+    exp = D.Elastic2D()
+    cfg = exp.config()
+    gfn, rfn = D._paths(exp, str(tmp_path))
+    os.makedirs(os.path.dirname(gfn))
+    os.makedirs(os.path.dirname(rfn))
+    np.save(gfn, np.array(GOLD["grads"]["elastic_2d/elastic_2d.npy"]))
+    np.save(rfn, np.array(GOLD["ranges"]["elastic_2d/elastic_2d.npy"]))
+    eps = 0.1
+    sol = D.solve(exp, cfg, str(tmp_path), D.EB, eps)
+    loss = D.run(exp, cfg, 3)
+    print("elastic_2d EB eps %g bits %s losses %s (f64 %.3f)" % (eps, sol["bits"], loss, exp.f64_data))
+    assert sol["compression_rate"] < 0.5
+    assert np.all(np.abs(loss - exp.f64_data) < 3 * eps * exp.f64_data)
+    assert len(set(loss.tolist())) > 1  # dithering seeds differ between runs
+
+
+def test_short_pipeline_end_to_end(tmp_path):
+    """-r, -a and -f chained through the CLI on a 256-substep horizon."""
+    root = str(tmp_path)
+    common = ["elastic_2d", "--root", root, "--timesteps", "257", "--json"]
+    r = D.main(common + ["-r"])
+    a = D.main(common + ["-a"])
+    f = D.main(common + ["-f", "-m", "0", "-e", "0.5", "-N", "2"])
+    assert os.path.exists(r["file"]) and os.path.exists(a["file"])
+    assert np.all(np.isfinite(a["grads"])) and min(a["grads"]) > 0
+    assert len(f["bits"]) == 12 and min(f["bits"]) >= 1
+    assert f["compression_rate"] == pytest.approx(0.5, abs=0.1)
+    assert np.allclose(f["losses"], a["loss"], rtol=0.05), (f["losses"], a["loss"])
