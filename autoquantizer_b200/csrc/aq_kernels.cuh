@@ -8,12 +8,12 @@
 // (codegen_llvm_quant.cpp).
 //
 // Data layout in HBM
-//   records  : n x W u64 bit_pack records, ordered by 4^3 (3D) or 8^2 (2D)
-//              cell block and cells inside a block; each block is cut into
-//              chunks of <= 256 records (the work items) and inside a chunk
-//              records are slot-major: the first record of every cell, then
-//              the second of every cell, ...  The 32 lanes of a warp then
-//              hold particles of 32 different cells.
+//   records  : n x W u64 bit_pack records, grouped by 4^3 (3D) or 8^2 (2D)
+//              cell block; inside a block slot-major (the first record of
+//              every cell in cell order, then the second of every cell, ...),
+//              so that the 32 lanes of a warp hold particles of 32 different
+//              cells except where a slot has fewer than 32 cells; each
+//              block's sequence is cut into chunks of <= 256 (work items).
 //              A particle-id array moves with the records.
 //   grids    : two dense grids of R4 nodes, row-major; one receives P2G
 //              sums (m, m v), the other holds grid_op output (m, v).
@@ -288,6 +288,7 @@ __global__ void __launch_bounds__(CH, AQ_STEP_MIN_BLOCKS) k_step(const __grid_co
   R4* ptile = gtile + TNP;                                           // NWARP x TNP (m, m v): P2G, per warp
   int32_t* spid = reinterpret_cast<int32_t*>(ptile + NWARP * TNP);  // CH
   uint64_t* srec = reinterpret_cast<uint64_t*>(spid + CH);          // CH x WS
+  __shared__ int sbox[6];  // tile-coordinate box of the item's P2G base cells (min[3], max[3])
 
   const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
   const int nitems = *A.n_items;
@@ -305,6 +306,7 @@ __global__ void __launch_bounds__(CH, AQ_STEP_MIN_BLOCKS) k_step(const __grid_co
     const int cnt = item.z;
     const int64_t first = item.y;
     const bool active = tid < cnt;
+    if (tid < 6) sbox[tid] = tid < 3 ? T : -1;
     int o[3] = {0, 0, 0};  // tile origin (node coordinates)
     {
       int blk = item.x;
@@ -502,6 +504,22 @@ __global__ void __launch_bounds__(CH, AQ_STEP_MIN_BLOCKS) k_step(const __grid_co
           ++nfall;
         }
       }
+      {  // grow the item's box by this warp's in-tile base cells
+        int mn[3], mx[3];
+#pragma unroll
+        for (int d = 0; d < D; ++d) {
+          const int l = base[d] - o[d];
+          mn[d] = __reduce_min_sync(0xffffffffu, (active && in_tile) ? l : T);
+          mx[d] = __reduce_max_sync(0xffffffffu, (active && in_tile) ? l : -1);
+        }
+        if (lane == 0 && mx[0] >= 0) {
+#pragma unroll
+          for (int d = 0; d < D; ++d) {
+            atomicMin(&sbox[d], mn[d]);
+            atomicMax(&sbox[3 + d], mx[d]);
+          }
+        }
+      }
       // Lanes of a warp with the same base cell add into the same nodes and
       // take turns (rank among peers); lanes of different base cells never
       // share a node for the same stencil offset.  Binning orders records so
@@ -559,29 +577,28 @@ __global__ void __launch_bounds__(CH, AQ_STEP_MIN_BLOCKS) k_step(const __grid_co
       }
       __syncthreads();
       // sum the warp tiles, re-zero them, flush: one vector reduction per
-      // touched node
-      for (int j = tid; j < TNP; j += CH) {
+      // node of the box the item's particles touched (base box + 2); the
+      // tiles are zero outside it
+      const int e0 = sbox[3] - sbox[0] + 3, e1 = sbox[4] - sbox[1] + 3, e2 = D == 3 ? sbox[5] - sbox[2] + 3 : 1;
+      const int nbox = sbox[3] >= 0 ? e0 * e1 * e2 : 0;
+      const float ie1 = 1.0f / (float)e1, ie2 = 1.0f / (float)e2;  // exact floors: j < 2^10, e <= 12
+      for (int j = tid; j < nbox; j += CH) {
+        const int q = D == 3 ? (int)(((float)j + 0.5f) * ie2) : j;
+        const int l2 = D == 3 ? sbox[2] + (j - q * e2) : 0;
+        const int i0 = (int)(((float)q + 0.5f) * ie1);
+        const int l0 = sbox[0] + i0, l1 = sbox[1] + (q - i0 * e1);
+        const int t = D == 3 ? l0 * G::XS + l1 * T + l2 : l0 * T + l1;
         R4 sum = zero4;
 #pragma unroll
         for (int k = 0; k < NWARP; ++k) {
-          const R4 v = ptile[k * TNP + j];
+          const R4 v = ptile[k * TNP + t];
           sum.x += v.x;
           sum.y += v.y;
           sum.z += v.z;
           sum.w += v.w;
-          ptile[k * TNP + j] = zero4;
+          ptile[k * TNP + t] = zero4;
         }
         if (sum.x == (R)0) continue;
-        int l0, l1, l2 = 0;
-        if (D == 3) {
-          l0 = j / G::XS;
-          const int rr = j - l0 * G::XS;
-          l1 = rr / T;
-          l2 = rr - l1 * T;
-        } else {
-          l0 = j / T;
-          l1 = j - l0 * T;
-        }
         const int g0 = o[0] + l0, g1 = o[1] + l1, g2 = o[2] + l2;
         if (g0 < 0 || g0 >= K.res[0] || g1 < 0 || g1 >= K.res[1] || (D == 3 && (g2 < 0 || g2 >= K.res[2])))
           continue;

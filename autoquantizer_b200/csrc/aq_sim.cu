@@ -62,12 +62,12 @@ __device__ __forceinline__ void chunk_of(int cnt, int local, int& c0, int& c1) {
   c1 = c0 + base + (j < rem ? 1 : 0);
 }
 
-// Move record i to its sorted position.  A block's records (in cell
-// order) are cut into chunks of at most 256 (chunk_of), the work items.  Inside a chunk
-// the order is slot-major: first the chunk's first record of every cell (in
-// cell order), then the second of every cell, and so on.  Consecutive
-// records, i.e. the lanes of a warp in k_step, are then in different cells
-// whenever the chunk spans at least 32 cells.
+// Move record i to its sorted position.  A block's records are ordered
+// slot-major over the whole block: first the first record of every cell of
+// the block (in cell order), then the second record of every cell, and so
+// on; this sequence is then cut into chunks of at most 256 (chunk_of), the
+// work items.  Consecutive records, i.e. the lanes of a warp in k_step, are
+// then in different cells except where a slot holds fewer than 32 cells.
 __global__ void __launch_bounds__(256) k_scatter(const uint64_t* __restrict__ win, const int32_t* __restrict__ pin,
                                                  uint64_t* __restrict__ wout, int32_t* __restrict__ pout,
                                                  const int32_t* __restrict__ keys, const int32_t* __restrict__ ranks,
@@ -75,24 +75,21 @@ __global__ void __launch_bounds__(256) k_scatter(const uint64_t* __restrict__ wi
   const int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
   if (i >= n) return;
   const int key = keys[i];
-  const int64_t g = (int64_t)start[key] + ranks[i];
+  const int r = ranks[i];  // rank of the record in its cell
   const int64_t c0 = (int64_t)(key >> 6) * 64;
-  const int64_t b0 = start[c0];
-  const int64_t be = start[c0 + 64];
-  int a, z;
-  chunk_of((int)(be - b0), (int)(g - b0), a, z);
-  const int64_t cs = b0 + a, ce = b0 + z;  // chunk [cs, ce)
-  const int r = (int)(g - max((int64_t)start[key], cs));  // rank in its cell within the chunk
   const int myc = key & 63;
+  // records before this one: min(count, r) of every cell, plus one more for
+  // every earlier cell that has an r-th record
   int t = 0;
   int64_t s0 = start[c0];
+  const int64_t b0 = s0;
   for (int k = 0; k < 64; ++k) {
     const int64_t s1 = start[c0 + k + 1];
-    const int nk = (int)max((int64_t)0, min(s1, ce) - max(s0, cs));
+    const int nk = (int)(s1 - s0);
     t += min(nk, r) + ((k < myc && nk > r) ? 1 : 0);
     s0 = s1;
   }
-  const int64_t dst = cs + t;
+  const int64_t dst = b0 + t;
   for (int j = 0; j < W; ++j) wout[dst * W + j] = win[i * W + j];
   pout[dst] = pin[i];
 }

@@ -253,6 +253,9 @@ def solve(exp, cfg, root, mode, eps):
     gfn, rfn = _paths(exp, root)
     grads, ranges = np.load(gfn), np.load(rfn)
     bits, ranges = exp.scheme(grads, ranges, mode, eps)
+    if np.any(np.asarray(bits) < 1) or np.any(np.asarray(bits) > 32):
+        # the reference passes these to ti.quant.fixed, which rejects them
+        raise ValueError("solved bit widths %s fall outside [1, 32]; choose another epsilon" % list(bits))
     cfg.quant_bits = np.asarray(bits)
     cfg.quant_ranges = np.asarray(ranges)
     return {"bits": [int(b) for b in bits], "ranges": ranges.tolist(),

@@ -116,3 +116,25 @@ def test_cli_needs_one_action():
         D.main(["elastic_2d"])
     with pytest.raises(SystemExit):
         D.main(["fluid_2d", "-f", "-m", "1", "--root", "/nonexistent"])
+
+
+def test_solve_rejects_unusable_widths(tmp_path):
+    exp = D.Elastic2D()
+    cfg = exp.config()
+    gfn, rfn = D._paths(exp, str(tmp_path))
+    os.makedirs(os.path.dirname(gfn))
+    os.makedirs(os.path.dirname(rfn))
+    np.save(gfn, np.array(GOLD["grads"]["elastic_2d/elastic_2d.npy"]))
+    np.save(rfn, np.array(GOLD["ranges"]["elastic_2d/elastic_2d.npy"]))
+    with pytest.raises(ValueError):
+        D.solve(exp, cfg, str(tmp_path), D.CR, 0.05)
+
+
+def test_adjoint_report_groups_partition_the_3d_record():
+    from autoquantizer_b200 import adjoint_report as AR
+    from autoquantizer_b200.adjoint import group_fields_3d
+
+    g = AR.group_slots()
+    assert sorted(sum(g, [])) == list(range(24)) and len(g) == len(AR.GROUP_NAMES) == 12
+    v = np.arange(24, dtype=np.float64)
+    assert np.array_equal([v[s].sum() for s in g], group_fields_3d(v))

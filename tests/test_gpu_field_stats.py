@@ -53,4 +53,6 @@ def test_device_initial_values_match_host(dtype):
     assert np.array_equal(a.words(), b.words())
     a.substeps(3)
     b.substeps(3)
-    assert np.array_equal(a.words(), b.words())
+    # P2G sums with float atomics in no fixed order: equal up to rounding
+    # (a dithered code may flip: C steps are 64 / 2^15)
+    assert np.allclose(a.state_values(), b.state_values(), rtol=0, atol=5e-3)
