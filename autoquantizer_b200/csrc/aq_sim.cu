@@ -368,7 +368,8 @@ struct aq_sim {
   unsigned long long* fallbacks = nullptr;
   double *rmax = nullptr, *rmin = nullptr;
   double* dloss = nullptr;
-  double* dstats = nullptr;  // aq_sim_field_stats accumulators, allocated on first use
+  double* dstats = nullptr;  // aq_sim_field_stats accumulators
+  void* slab = nullptr;      // the one device allocation all buffers above live in
   int ranges_on = 0;
   int64_t step = 0;
   int since_sort = 0;
@@ -578,11 +579,7 @@ static void free_sim(aq_sim* s) {
       delete[] s->prof_ev[k];
     }
   }
-  void* ptrs[] = {s->words[0], s->words[1], s->pid[0], s->pid[1], s->grid[0], s->grid[1], s->keys, s->ranks,
-                  s->cell_count, s->cell_start, s->scan_sums, s->items, s->n_items, s->status, s->fallbacks,
-                  s->rmax, s->rmin, s->dloss, s->dstats};
-  for (void* p : ptrs)
-    if (p) cudaFree(p);
+  if (s->slab) cudaFree(s->slab);
   delete s;
 }
 
@@ -634,8 +631,18 @@ int aq_sim_create(const aq_params* P, const aq_layout* L, aq_sim** out) {
   const int64_t n = s->n;
   const int nt = (int)((s->nkeys + SCAN_TILE - 1) / SCAN_TILE);
   cudaError_t e = cudaSuccess;
+  // every buffer is carved from one device allocation (one cudaMalloc per
+  // simulator, one cudaFree at destroy), each on a 256-byte boundary
+  struct Part {
+    void** p;
+    size_t off;
+  };
+  Part parts[24];
+  int nparts = 0;
+  size_t total = 0;
   auto alloc = [&](void** p, size_t bytes) {
-    if (e == cudaSuccess) e = cudaMalloc(p, bytes < 16 ? 16 : bytes);
+    parts[nparts++] = Part{p, total};
+    total += (bytes + 255) & ~(size_t)255;
   };
   alloc((void**)&s->words[0], sizeof(uint64_t) * (n * s->W + 2));
   alloc((void**)&s->words[1], sizeof(uint64_t) * (n * s->W + 2));
@@ -655,7 +662,12 @@ int aq_sim_create(const aq_params* P, const aq_layout* L, aq_sim** out) {
   alloc((void**)&s->rmax, sizeof(double) * AQ_MAX_SLOTS);
   alloc((void**)&s->rmin, sizeof(double) * AQ_MAX_SLOTS);
   alloc((void**)&s->dloss, sizeof(double));
+  alloc((void**)&s->dstats, sizeof(double) * 5 * AQ_MAX_SLOTS);
+  e = cudaMalloc(&s->slab, total);
+  if (e == cudaSuccess)
+    for (int k = 0; k < nparts; ++k) *parts[k].p = static_cast<char*>(s->slab) + parts[k].off;
   if (e != cudaSuccess) {
+    s->slab = nullptr;
     set_last_cuda_error(e, "cudaMalloc");
     free_sim(s);
     return AQ_E_NOMEM;
@@ -726,9 +738,7 @@ int aq_sim_get_state(aq_sim* s, void* values, int32_t values_f64, void* stream) 
 int aq_sim_field_stats(aq_sim* s, const void* ref, int32_t ref_f64, double* h_out, void* stream) {
   if (!s || !h_out) return AQ_E_ARG;
   cudaStream_t st = as_stream(stream);
-  const size_t bytes = sizeof(double) * 5 * AQ_MAX_SLOTS;
-  if (!s->dstats) AQ_CUDA_TRY(cudaMalloc((void**)&s->dstats, bytes));
-  AQ_CUDA_TRY(cudaMemsetAsync(s->dstats, 0, bytes, st));
+  AQ_CUDA_TRY(cudaMemsetAsync(s->dstats, 0, sizeof(double) * 5 * AQ_MAX_SLOTS, st));
   const unsigned nb = (unsigned)std::min<int64_t>(grid_for(s->n, 256), (int64_t)num_sms() * 4);
   const dim3 grid(nb > 0 ? nb : 1, s->NS);
   if (ref_f64)

