@@ -530,7 +530,15 @@ __global__ void __launch_bounds__(CH, AQ_STEP_MIN_BLOCKS) k_step(const __grid_co
       const int rounds = __reduce_max_sync(0xffffffffu, (unsigned)__popc(peers));
       R4* mytile = ptile + warp * TNP;
       for (int r = 0; r < rounds; ++r) {
-        if (active && rank == r) {
+        const bool mine = active && rank == r;
+        const unsigned tm = __ballot_sync(0xffffffffu, mine && in_tile);  // lanes writing the tile this round
+        if (mine && in_tile) {
+          // Lanes add into their nodes offset by offset.  Lanes whose base
+          // cells are neighbours reach the same node at different offsets,
+          // so every offset's read-modify-write must be visible to the warp
+          // before the next one reads: __syncwarp orders them (without it
+          // the compiler and the shared-memory pipeline may overlap them
+          // and lose updates).
 #pragma unroll
           for (int a = 0; a < 3; ++a)
 #pragma unroll
@@ -557,21 +565,39 @@ __global__ void __launch_bounds__(CH, AQ_STEP_MIN_BLOCKS) k_step(const __grid_co
                   if (D == 3 && c == 2) s += (R)2 * Aff[d * D + 2];
                   mv[d] = weight * s;
                 }
-                const R m = weight * K.p_mass;
-                if (in_tile) {
-                  R4& t = mytile[lb + (D == 3 ? a * G::XS + b * T + c : a * T + b)];
-                  R4 v = t;
-                  v.x += m;
-                  v.y += mv[0];
-                  v.z += mv[1];
-                  v.w += mv[2];
-                  t = v;
-                } else {
-                  R4* g = gout + cell_index<D>(K.res, base[0] + a, base[1] + b, D == 3 ? base[2] + c : 0);
-                  red_add_node(g, m, mv[0], mv[1], mv[2]);
-                }
+                R4& t = mytile[lb + (D == 3 ? a * G::XS + b * T + c : a * T + b)];
+                R4 v = t;
+                v.x += weight * K.p_mass;
+                v.y += mv[0];
+                v.z += mv[1];
+                v.w += mv[2];
+                t = v;
+                __syncwarp(tm);
               }
             }
+        } else if (mine) {  // outside the tile: straight to the global grid
+#pragma unroll
+          for (int a = 0; a < 3; ++a)
+#pragma unroll
+            for (int b = 0; b < 3; ++b)
+#pragma unroll
+              for (int c = 0; c < (D == 3 ? 3 : 1); ++c) {
+                const R weight = D == 3 ? w[a][0] * w[b][1] * w[c][2] : w[a][0] * w[b][1];
+                R mv[3] = {0, 0, 0};
+#pragma unroll
+                for (int d = 0; d < D; ++d) {
+                  R s = q[d];
+                  if (a == 1) s += Aff[d * D + 0];
+                  if (a == 2) s += (R)2 * Aff[d * D + 0];
+                  if (b == 1) s += Aff[d * D + 1];
+                  if (b == 2) s += (R)2 * Aff[d * D + 1];
+                  if (D == 3 && c == 1) s += Aff[d * D + 2];
+                  if (D == 3 && c == 2) s += (R)2 * Aff[d * D + 2];
+                  mv[d] = weight * s;
+                }
+                R4* g = gout + cell_index<D>(K.res, base[0] + a, base[1] + b, D == 3 ? base[2] + c : 0);
+                red_add_node(g, weight * K.p_mass, mv[0], mv[1], mv[2]);
+              }
         }
         __syncwarp();
       }
