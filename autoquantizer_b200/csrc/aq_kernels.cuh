@@ -13,14 +13,14 @@
 //              every cell in cell order, then the second of every cell, ...),
 //              so that the 32 lanes of a warp hold particles of 32 different
 //              cells except where a slot has fewer than 32 cells; each
-//              block's sequence is cut into chunks of <= 256 (work items).
+//              block's sequence is cut into chunks of <= CH (work items).
 //              A particle-id array moves with the records.
 //   grids    : two dense grids of R4 nodes, row-major; one receives P2G
 //              sums (m, m v), the other holds grid_op output (m, v).
 //   binning  : per-cell counts/offsets, per-particle key and rank, and work
-//              items (block, first record, count <= 256).
+//              items (block, first record, count <= CH).
 //
-// k_step, one CTA of 256 threads per work item (persistent loop):
+// k_step, one CTA of CH = 128 threads per work item (persistent loop):
 //   1. thread t loads record t of the item into shared memory (odd word
 //      stride: conflict-free) and stages the block's grid tile (G2P source);
 //   2. G2P of substep k: gather 3^d nodes, new v, C, x, F|J;
@@ -45,10 +45,13 @@
 
 namespace aq {
 
-constexpr int CH = 256;  // particles per work item = threads per CTA
+#ifndef AQ_CH
+#define AQ_CH 128
+#endif
+constexpr int CH = AQ_CH;  // particles per work item = threads per CTA
 constexpr int NWARP = CH / 32;
 #ifndef AQ_STEP_MIN_BLOCKS
-#define AQ_STEP_MIN_BLOCKS 2  // CTAs per SM the register allocation must allow
+#define AQ_STEP_MIN_BLOCKS (512 / AQ_CH)  // CTAs per SM the register allocation must allow (128 registers)
 #endif
 
 template <int D>

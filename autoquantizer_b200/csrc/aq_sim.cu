@@ -52,7 +52,7 @@ __global__ void __launch_bounds__(256) k_bin(const __grid_constant__ aq_layout L
   if (fl) atomicOr(status, fl);
 }
 
-// A block of cnt records is cut into k = ceil(cnt/256) chunks of nearly
+// A block of cnt records is cut into k = ceil(cnt/CH) chunks of nearly
 // equal size (the first cnt % k chunks one record larger).
 __device__ __forceinline__ void chunk_of(int cnt, int local, int& c0, int& c1) {
   const int k = (cnt + CH - 1) / CH, base = cnt / k, rem = cnt - base * k;
@@ -65,7 +65,7 @@ __device__ __forceinline__ void chunk_of(int cnt, int local, int& c0, int& c1) {
 // Move record i to its sorted position.  A block's records are ordered
 // slot-major over the whole block: first the first record of every cell of
 // the block (in cell order), then the second record of every cell, and so
-// on; this sequence is then cut into chunks of at most 256 (chunk_of), the
+// on; this sequence is then cut into chunks of at most CH (chunk_of), the
 // work items.  Consecutive records, i.e. the lanes of a warp in k_step, are
 // then in different cells except where a slot holds fewer than 32 cells.
 __global__ void __launch_bounds__(256) k_scatter(const uint64_t* __restrict__ win, const int32_t* __restrict__ pin,
