@@ -52,14 +52,12 @@ __global__ void __launch_bounds__(256) k_bin(const __grid_constant__ aq_layout L
   if (fl) atomicOr(status, fl);
 }
 
-// A block of cnt records is cut into k = ceil(cnt/CH) chunks of nearly
-// equal size (the first cnt % k chunks one record larger).
+// A block of cnt records is cut into chunks of CH records and one last
+// chunk of the remainder: every warp but the last one of a block then has
+// all 32 lanes busy.
 __device__ __forceinline__ void chunk_of(int cnt, int local, int& c0, int& c1) {
-  const int k = (cnt + CH - 1) / CH, base = cnt / k, rem = cnt - base * k;
-  const int big = rem * (base + 1);
-  const int j = local < big ? local / (base + 1) : rem + (local - big) / base;
-  c0 = j * base + min(j, rem);
-  c1 = c0 + base + (j < rem ? 1 : 0);
+  c0 = (local / CH) * CH;
+  c1 = min(c0 + CH, cnt);
 }
 
 // Move record i to its sorted position.  A block's records are ordered
