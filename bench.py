@@ -126,7 +126,9 @@ class Clocks:
                 "reasons": sorted(reasons), "samples": len(sm)}
 
 
-def dist_init():
+def dist_init(backend="nccl"):
+    """One process per GPU (torchrun env); each rank is an independent replica
+    of the whole workload.  backend "gloo" runs the same host logic on CPU."""
     ws = int(os.environ.get("WORLD_SIZE", "1"))
     rank = int(os.environ.get("RANK", "0"))
     local = int(os.environ.get("LOCAL_RANK", "0"))
@@ -136,9 +138,12 @@ def dist_init():
         import torch
         import torch.distributed as dist
 
-        torch.cuda.set_device(local)
-        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=300),
-                                device_id=torch.device("cuda", local))
+        if backend == "nccl":
+            torch.cuda.set_device(local)
+            dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=300),
+                                    device_id=torch.device("cuda", local))
+        else:
+            dist.init_process_group(backend, timeout=datetime.timedelta(seconds=60))
     return ws, rank, local
 
 
@@ -155,9 +160,17 @@ def max_over_ranks(x, ws):
     import torch
     import torch.distributed as dist
 
-    t = torch.tensor([x], dtype=torch.float64, device="cuda")
+    dev = "cuda" if dist.get_backend() == "nccl" else "cpu"
+    t = torch.tensor([x], dtype=torch.float64, device=dev)
     dist.all_reduce(t, op=dist.ReduceOp.MAX)
     return float(t.item())
+
+
+def job_rate(units_per_rank, ms_per_rank, ws):
+    """Whole-job throughput of ws replicas: every rank processes
+    units_per_rank; the job takes as long as the slowest rank."""
+    ms = max_over_ranks(ms_per_rank, ws)
+    return ws * units_per_rank / (ms * 1e-3), ms
 
 
 def cpu_oracle_rate(cfg, vals, seconds=15.0, stride=16, threads=None):
@@ -263,8 +276,7 @@ def run_ours(args, ws, rank, local):
     clocks.start()
     ms, launches = timed(q, K, prof=True)
     ck = clocks.stop()
-    ms = max_over_ranks(ms, ws)
-    value = ws * n * K / (ms * 1e-3)
+    value, ms = job_rate(n * K, ms, ws)
     tot = C.c_double()
     cnt = C.c_int64()
     _lib.check(L.aq_sim_profile_get(q._sim, 0, C.byref(tot), C.byref(cnt)))
@@ -284,8 +296,7 @@ def run_ours(args, ws, rank, local):
     f.set_particles(vals)
     f.substeps(W)
     ms32, _ = timed(f, K)
-    ms32 = max_over_ranks(ms32, ws)
-    value32 = ws * n * K / (ms32 * 1e-3)
+    value32, ms32 = job_rate(n * K, ms32, ws)
 
     # ---- FP64 oracle run on the GPU and position errors after W+K substeps
     cfg64, _ = scenes.mixed_boxes_3d(seed=rank, quantized=False, precision="f64")
@@ -326,8 +337,7 @@ def run_ours(args, ws, rank, local):
         e2e_step()
     e1.record()
     torch.cuda.synchronize()
-    e2e_ms = max_over_ranks(e0.elapsed_time(e1), ws)
-    e2e_val = ws * n * frame * e2e_steps / (e2e_ms * 1e-3)
+    e2e_val, e2e_ms = job_rate(n * frame * e2e_steps, e0.elapsed_time(e1), ws)
 
     # ---- CPU baseline (rank 0, N=1 only)
     cpu = None
