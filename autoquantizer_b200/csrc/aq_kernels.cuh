@@ -97,6 +97,8 @@ struct StepArgs {
   const int32_t* pid;
   const int4* items;
   const int32_t* n_items;
+  int32_t* item_ctr;       // next unclaimed item of this launch (starts at zero)
+  int32_t* item_ctr_next;  // the next launch's counter, zeroed by this launch
   const void* grid_in;  // G2P source (after grid_op)
   void* grid_out;       // P2G target (zeroed)
   unsigned* status;
@@ -288,10 +290,10 @@ __global__ void __launch_bounds__(CH, AQ_STEP_MIN_BLOCKS) k_step(const __grid_co
 
   extern __shared__ __align__(16) unsigned char smem_raw[];
   R4* gtile = reinterpret_cast<R4*>(smem_raw);                      // TNP nodes (m, v): G2P source
-  R4* ptile = gtile + TNP;                                           // NWARP x TNP (m, m v): P2G, per warp
-  int32_t* spid = reinterpret_cast<int32_t*>(ptile + NWARP * TNP);  // CH
-  uint64_t* srec = reinterpret_cast<uint64_t*>(spid + CH);          // CH x WS
+  R4* ptile = gtile + TNP;                                     // NWARP x TNP (m, m v): P2G, per warp
+  uint64_t* srec = reinterpret_cast<uint64_t*>(ptile + NWARP * TNP);  // CH x WS: each thread's record
   __shared__ int sbox[6];  // tile-coordinate box of the item's P2G base cells (min[3], max[3])
+  __shared__ int s_next;   // the CTA's next work item, claimed from A.item_ctr
 
   const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
   const int nitems = *A.n_items;
@@ -304,11 +306,21 @@ __global__ void __launch_bounds__(CH, AQ_STEP_MIN_BLOCKS) k_step(const __grid_co
   if (A.do_p2g)  // private tiles start at zero; the flush of every item re-zeroes them
     for (int j = tid; j < NWARP * TNP; j += CH) ptile[j] = zero4;
 
-  for (int it = blockIdx.x; it < nitems; it += gridDim.x) {
+  // Work items are whole cell blocks, claimed one at a time from a counter
+  // (largest imbalance: one item).  Inside an item the warps take the
+  // block's records 32 at a time (units u = warp, warp + NWARP, ...), with
+  // no CTA barrier between units: the grid tile is staged once per item and
+  // the warp tiles are flushed once per item.
+  if (tid == 0) {
+    if (blockIdx.x == 0) *A.item_ctr_next = 0;
+    s_next = atomicAdd(A.item_ctr, 1);
+  }
+  __syncthreads();
+  for (int it = s_next; it < nitems; it = s_next) {
     const int4 item = A.items[it];
     const int cnt = item.z;
     const int64_t first = item.y;
-    const bool active = tid < cnt;
+    const int nunits = (cnt + 31) >> 5;
     if (tid < 6) sbox[tid] = tid < 3 ? T : -1;
     int o[3] = {0, 0, 0};  // tile origin (node coordinates)
     {
@@ -319,11 +331,6 @@ __global__ void __launch_bounds__(CH, AQ_STEP_MIN_BLOCKS) k_step(const __grid_co
       }
       o[1] = (blk % K.nb[1]) * G::BS - 1;
       o[0] = (blk / K.nb[1]) * G::BS - 1;
-    }
-    if (active) {
-      const uint64_t* src = A.words + (first + tid) * W;
-      for (int k = 0; k < W; ++k) myrec[k] = __ldg(src + k);
-      spid[tid] = A.pid[first + tid];
     }
     if (A.do_g2p) {  // stage the grid tile (m, v after grid_op)
       for (int j = tid; j < TNP; j += CH) {
@@ -345,248 +352,219 @@ __global__ void __launch_bounds__(CH, AQ_STEP_MIN_BLOCKS) k_step(const __grid_co
     }
     __syncthreads();
 
-    R vals[NS];
-    if (active) {
-      if (A.do_g2p) {  // G2P reads x, F|J and the material id; v and C are rewritten
-        constexpr unsigned XFM = ((1u << D) - 1u) | (((1u << S::NFJ) - 1u) << S::FJ) | (HM ? 1u << S::MAT : 0u);
-        decode_record<NS, R, XFM>(L, myrec, vals);
-#pragma unroll
-        for (int k = S::V; k < S::FJ; ++k) vals[k] = 0;
-      } else {
-        decode_record<NS, R>(L, myrec, vals);
-      }
-    }
-
-    // ---------------------------------------------------------------- G2P
-    if (A.do_g2p && active) {
-      int base[3] = {0, 0, 0};
-      R fx[3] = {0, 0, 0}, w[3][3];
-      bspline<D, R>(vals + S::X, K, base, fx, w, fl);
-      bool in_tile = true;
-#pragma unroll
-      for (int d = 0; d < D; ++d) {
-        const int l = base[d] - o[d];
-        in_tile = in_tile && l >= 0 && l <= T - 3;
-      }
-      R nv[D], Sm[D][D];
-#pragma unroll
-      for (int d = 0; d < D; ++d) {
-        nv[d] = 0;
-#pragma unroll
-        for (int e = 0; e < D; ++e) Sm[d][e] = 0;
-      }
-      const int lb = in_tile ? (D == 3 ? (base[0] - o[0]) * G::XS + (base[1] - o[1]) * T + (base[2] - o[2])
-                                       : (base[0] - o[0]) * T + (base[1] - o[1]))
-                             : 0;
-      if (!in_tile) ++nfall;
-#pragma unroll
-      for (int a = 0; a < 3; ++a)
-#pragma unroll
-        for (int b = 0; b < 3; ++b) {
-          const R wab = w[a][0] * w[b][1];
-#pragma unroll
-          for (int c = 0; c < (D == 3 ? 3 : 1); ++c) {
-            const R weight = D == 3 ? wab * w[c][2] : wab;
-            const R4 g = in_tile ? gtile[lb + (D == 3 ? a * G::XS + b * T + c : a * T + b)]
-                                 : gin[cell_index<D>(K.res, base[0] + a, base[1] + b, D == 3 ? base[2] + c : 0)];
-            const R gv[3] = {g.y, g.z, g.w};
-            const int off[3] = {a, b, c};
-#pragma unroll
-            for (int d = 0; d < D; ++d) {
-              const R wg = weight * gv[d];
-              nv[d] += wg;
-#pragma unroll
-              for (int e = 0; e < D; ++e) {
-                if (off[e] == 1) Sm[d][e] += wg;
-                if (off[e] == 2) Sm[d][e] += (R)2 * wg;
-              }
-            }
-          }
-        }
-      // new_C = 4 inv_dx sum w g_v (off - fx)^T;  new_x = x + dt new_v
-      R nC[D * D];
-#pragma unroll
-      for (int d = 0; d < D; ++d)
-#pragma unroll
-        for (int e = 0; e < D; ++e) nC[d * D + e] = K.four_inv_dx * (Sm[d][e] - nv[d] * fx[e]);
-#pragma unroll
-      for (int d = 0; d < D; ++d) {
-        R nx = vals[S::X + d] + K.dt * nv[d];
-        if (K.bound_clip) nx = fmax(fmin(nx, K.clip_hi[d]), K.clip_lo[d]);
-        vals[S::X + d] = nx;
-        vals[S::V + d] = nv[d];
-      }
-      const int mat = HM ? min(max((int)vals[S::MAT], 0), K.n_mat - 1) : 0;
-      if (HF) {
-        R nF[D * D];
-#pragma unroll
-        for (int i = 0; i < D; ++i)
-#pragma unroll
-          for (int j = 0; j < D; ++j) {
-            R acc = 0;
-#pragma unroll
-            for (int k = 0; k < D; ++k)
-              acc += ((i == k ? (R)1 : (R)0) + K.dt * nC[i * D + k]) * vals[S::FJ + k * D + j];
-            nF[i * D + j] = acc;
-          }
-        if (HM && K.mat_kind[mat] == AQ_MAT_FLUID) {  // fluid in an F record keeps only J
-          const R Jn = det<D, R>(nF);
-          const R sj = D == 3 ? cbrt(Jn) : sqrt(Jn);
-#pragma unroll
-          for (int i = 0; i < D; ++i)
-#pragma unroll
-            for (int j = 0; j < D; ++j) nF[i * D + j] = i == j ? sj : (R)0;
-        }
-#pragma unroll
-        for (int k = 0; k < D * D; ++k) vals[S::FJ + k] = nF[k];
-      } else {
-        R tr = 0;
-#pragma unroll
-        for (int d = 0; d < D; ++d) tr += nC[d * D + d];
-        vals[S::FJ] = ((R)1 + K.dt * tr) * vals[S::FJ];
-      }
-#pragma unroll
-      for (int k = 0; k < D * D; ++k) vals[S::C + k] = nC[k];
-      // bit_pack_assign of the new state; vals become the values a later
-      // read of the record returns (input of the next P2G)
-      encode_record<NS, R>(L, vals, myrec, particle_key(A.sk, spid[tid]), (const float*)0, (const double*)0);
-      uint64_t* dst = A.words + (first + tid) * W;
-      for (int k = 0; k < W; ++k) dst[k] = myrec[k];
-    }
-
-    // -------------------------------------------- range detection (opt)
-    if (A.ranges && A.do_g2p) {
-#pragma unroll
-      for (int s = 0; s < NS; ++s) {
-        double mx = active ? (double)vals[s] : -(double)AQ_POS_INF, mn = active ? (double)vals[s] : (double)AQ_POS_INF;
-#pragma unroll
-        for (int k = 16; k; k >>= 1) {
-          mx = fmax(mx, __shfl_xor_sync(0xffffffffu, mx, k));
-          mn = fmin(mn, __shfl_xor_sync(0xffffffffu, mn, k));
-        }
-        if (lane == 0) {
-          atomic_max_d(A.rmax + s, mx);
-          atomic_min_d(A.rmin + s, mn);
-        }
-      }
-    }
-
-    // ---------------------------------------------------------------- P2G
-    if (A.do_p2g) {
-      int base[3] = {0, 0, 0};
-      R fx[3] = {0, 0, 0}, w[3][3];
-      R Aff[D * D], q[D];
-      bool in_tile = false;
-      int lb = 0;
+    for (int u = warp; u < nunits; u += NWARP) {
+      const int64_t rec = first + 32 * u + lane;
+      const bool active = 32 * u + lane < cnt;
+      int32_t pid = 0;
       if (active) {
-        const int mat = HM ? min(max((int)vals[S::MAT], 0), K.n_mat - 1) : 0;
+        const uint64_t* src = A.words + rec * W;
+        for (int k = 0; k < W; ++k) myrec[k] = __ldg(src + k);
+        pid = __ldg(A.pid + rec);
+      }
+      R vals[NS];
+      if (active) {
+        if (A.do_g2p) {  // G2P reads x, F|J and the material id; v and C are rewritten
+          constexpr unsigned XFM = ((1u << D) - 1u) | (((1u << S::NFJ) - 1u) << S::FJ) | (HM ? 1u << S::MAT : 0u);
+          decode_record<NS, R, XFM>(L, myrec, vals);
+#pragma unroll
+          for (int k = S::V; k < S::FJ; ++k) vals[k] = 0;
+        } else {
+          decode_record<NS, R>(L, myrec, vals);
+        }
+      }
+
+      // ---------------------------------------------------------------- G2P
+      if (A.do_g2p && active) {
+        int base[3] = {0, 0, 0};
+        R fx[3] = {0, 0, 0}, w[3][3];
         bspline<D, R>(vals + S::X, K, base, fx, w, fl);
-        in_tile = true;
+        bool in_tile = true;
 #pragma unroll
         for (int d = 0; d < D; ++d) {
           const int l = base[d] - o[d];
           in_tile = in_tile && l >= 0 && l <= T - 3;
         }
-        R cau[D * D];
-        cauchy<D, HF, R>(K, mat, vals + S::FJ, vals[S::FJ], cau);
-        // node value = m v + affine (off - fx) dx = q + Aff off,
-        // q = m v - affine fx dx, Aff = (stress + m C) dx
-#pragma unroll
-        for (int k = 0; k < D * D; ++k) Aff[k] = (K.stress_coef * cau[k] + K.p_mass * vals[S::C + k]) * K.dx;
+        R nv[D], Sm[D][D];
 #pragma unroll
         for (int d = 0; d < D; ++d) {
-          R s = K.p_mass * vals[S::V + d];
+          nv[d] = 0;
 #pragma unroll
-          for (int e = 0; e < D; ++e) s -= Aff[d * D + e] * fx[e];
-          q[d] = s;
+          for (int e = 0; e < D; ++e) Sm[d][e] = 0;
         }
-        if (in_tile) {
-          lb = D == 3 ? (base[0] - o[0]) * G::XS + (base[1] - o[1]) * T + (base[2] - o[2])
-                      : (base[0] - o[0]) * T + (base[1] - o[1]);
+        const int lb = in_tile ? (D == 3 ? (base[0] - o[0]) * G::XS + (base[1] - o[1]) * T + (base[2] - o[2])
+                                         : (base[0] - o[0]) * T + (base[1] - o[1]))
+                               : 0;
+        if (!in_tile) ++nfall;
+#pragma unroll
+        for (int a = 0; a < 3; ++a)
+#pragma unroll
+          for (int b = 0; b < 3; ++b) {
+            const R wab = w[a][0] * w[b][1];
+#pragma unroll
+            for (int c = 0; c < (D == 3 ? 3 : 1); ++c) {
+              const R weight = D == 3 ? wab * w[c][2] : wab;
+              const R4 g = in_tile ? gtile[lb + (D == 3 ? a * G::XS + b * T + c : a * T + b)]
+                                   : gin[cell_index<D>(K.res, base[0] + a, base[1] + b, D == 3 ? base[2] + c : 0)];
+              const R gv[3] = {g.y, g.z, g.w};
+              const int off[3] = {a, b, c};
+#pragma unroll
+              for (int d = 0; d < D; ++d) {
+                const R wg = weight * gv[d];
+                nv[d] += wg;
+#pragma unroll
+                for (int e = 0; e < D; ++e) {
+                  if (off[e] == 1) Sm[d][e] += wg;
+                  if (off[e] == 2) Sm[d][e] += (R)2 * wg;
+                }
+              }
+            }
+          }
+        // new_C = 4 inv_dx sum w g_v (off - fx)^T;  new_x = x + dt new_v
+        R nC[D * D];
+#pragma unroll
+        for (int d = 0; d < D; ++d)
+#pragma unroll
+          for (int e = 0; e < D; ++e) nC[d * D + e] = K.four_inv_dx * (Sm[d][e] - nv[d] * fx[e]);
+#pragma unroll
+        for (int d = 0; d < D; ++d) {
+          R nx = vals[S::X + d] + K.dt * nv[d];
+          if (K.bound_clip) nx = fmax(fmin(nx, K.clip_hi[d]), K.clip_lo[d]);
+          vals[S::X + d] = nx;
+          vals[S::V + d] = nv[d];
+        }
+        const int mat = HM ? min(max((int)vals[S::MAT], 0), K.n_mat - 1) : 0;
+        if (HF) {
+          R nF[D * D];
+#pragma unroll
+          for (int i = 0; i < D; ++i)
+#pragma unroll
+            for (int j = 0; j < D; ++j) {
+              R acc = 0;
+#pragma unroll
+              for (int k = 0; k < D; ++k)
+                acc += ((i == k ? (R)1 : (R)0) + K.dt * nC[i * D + k]) * vals[S::FJ + k * D + j];
+              nF[i * D + j] = acc;
+            }
+          if (HM && K.mat_kind[mat] == AQ_MAT_FLUID) {  // fluid in an F record keeps only J
+            const R Jn = det<D, R>(nF);
+            const R sj = D == 3 ? cbrt(Jn) : sqrt(Jn);
+#pragma unroll
+            for (int i = 0; i < D; ++i)
+#pragma unroll
+              for (int j = 0; j < D; ++j) nF[i * D + j] = i == j ? sj : (R)0;
+          }
+#pragma unroll
+          for (int k = 0; k < D * D; ++k) vals[S::FJ + k] = nF[k];
         } else {
-          ++nfall;
+          R tr = 0;
+#pragma unroll
+          for (int d = 0; d < D; ++d) tr += nC[d * D + d];
+          vals[S::FJ] = ((R)1 + K.dt * tr) * vals[S::FJ];
         }
+#pragma unroll
+        for (int k = 0; k < D * D; ++k) vals[S::C + k] = nC[k];
+        // bit_pack_assign of the new state; vals become the values a later
+        // read of the record returns (input of the next P2G)
+        encode_record<NS, R>(L, vals, myrec, particle_key(A.sk, pid), (const float*)0, (const double*)0);
+        uint64_t* dst = A.words + rec * W;
+        for (int k = 0; k < W; ++k) dst[k] = myrec[k];
       }
-      {  // grow the item's box by this warp's in-tile base cells
-        int mn[3], mx[3];
+
+      // -------------------------------------------- range detection (opt)
+      if (A.ranges && A.do_g2p) {
 #pragma unroll
-        for (int d = 0; d < D; ++d) {
-          const int l = base[d] - o[d];
-          mn[d] = __reduce_min_sync(0xffffffffu, (active && in_tile) ? l : T);
-          mx[d] = __reduce_max_sync(0xffffffffu, (active && in_tile) ? l : -1);
-        }
-        if (lane == 0 && mx[0] >= 0) {
+        for (int s = 0; s < NS; ++s) {
+          double mx = active ? (double)vals[s] : -(double)AQ_POS_INF;
+          double mn = active ? (double)vals[s] : (double)AQ_POS_INF;
 #pragma unroll
-          for (int d = 0; d < D; ++d) {
-            atomicMin(&sbox[d], mn[d]);
-            atomicMax(&sbox[3 + d], mx[d]);
+          for (int k = 16; k; k >>= 1) {
+            mx = fmax(mx, __shfl_xor_sync(0xffffffffu, mx, k));
+            mn = fmin(mn, __shfl_xor_sync(0xffffffffu, mn, k));
+          }
+          if (lane == 0) {
+            atomic_max_d(A.rmax + s, mx);
+            atomic_min_d(A.rmin + s, mn);
           }
         }
       }
-      // Lanes of a warp with the same base cell add into the same nodes and
-      // take turns (rank among peers); lanes of different base cells never
-      // share a node for the same stencil offset.  Binning orders records so
-      // that a warp's lanes are in different cells: one turn is the norm.
-      const int key = (active && in_tile) ? lb : -1 - lane;
-      const unsigned peers = __match_any_sync(0xffffffffu, key);
-      const int rank = __popc(peers & ((1u << lane) - 1u));
-      const int rounds = __reduce_max_sync(0xffffffffu, (unsigned)__popc(peers));
-      R4* mytile = ptile + warp * TNP;
-      for (int r = 0; r < rounds; ++r) {
-        const bool mine = active && rank == r;
-        const unsigned tm = __ballot_sync(0xffffffffu, mine && in_tile);  // lanes writing the tile this round
-        if (mine && in_tile) {
-          // Lanes add into their nodes offset by offset.  Lanes whose base
-          // cells are neighbours reach the same node at different offsets,
-          // so every offset's read-modify-write must be visible to the warp
-          // before the next one reads: __syncwarp orders them (without it
-          // the compiler and the shared-memory pipeline may overlap them
-          // and lose updates).
+
+      // ---------------------------------------------------------------- P2G
+      if (A.do_p2g) {
+        int base[3] = {0, 0, 0};
+        R fx[3] = {0, 0, 0}, w[3][3];
+        R Aff[D * D], q[D];
+        bool in_tile = false;
+        int lb = 0;
+        if (active) {
+          const int mat = HM ? min(max((int)vals[S::MAT], 0), K.n_mat - 1) : 0;
+          bspline<D, R>(vals + S::X, K, base, fx, w, fl);
+          in_tile = true;
 #pragma unroll
-          for (int a = 0; a < 3; ++a)
+          for (int d = 0; d < D; ++d) {
+            const int l = base[d] - o[d];
+            in_tile = in_tile && l >= 0 && l <= T - 3;
+          }
+          R cau[D * D];
+          cauchy<D, HF, R>(K, mat, vals + S::FJ, vals[S::FJ], cau);
+          // node value = m v + affine (off - fx) dx = q + Aff off,
+          // q = m v - affine fx dx, Aff = (stress + m C) dx
 #pragma unroll
-            for (int b = 0; b < 3; ++b) {
-              const R wab = w[a][0] * w[b][1];
-              R qab[3];
+          for (int k = 0; k < D * D; ++k) Aff[k] = (K.stress_coef * cau[k] + K.p_mass * vals[S::C + k]) * K.dx;
 #pragma unroll
-              for (int d = 0; d < D; ++d) {
-                R s = q[d];
-                if (a == 1) s += Aff[d * D + 0];
-                if (a == 2) s += (R)2 * Aff[d * D + 0];
-                if (b == 1) s += Aff[d * D + 1];
-                if (b == 2) s += (R)2 * Aff[d * D + 1];
-                qab[d] = s;
-              }
+          for (int d = 0; d < D; ++d) {
+            R s = K.p_mass * vals[S::V + d];
 #pragma unroll
-              for (int c = 0; c < (D == 3 ? 3 : 1); ++c) {
-                const R weight = D == 3 ? wab * w[c][2] : wab;
-                R mv[3] = {0, 0, 0};
+            for (int e = 0; e < D; ++e) s -= Aff[d * D + e] * fx[e];
+            q[d] = s;
+          }
+          if (in_tile) {
+            lb = D == 3 ? (base[0] - o[0]) * G::XS + (base[1] - o[1]) * T + (base[2] - o[2])
+                        : (base[0] - o[0]) * T + (base[1] - o[1]);
+          } else {
+            ++nfall;
+          }
+        }
+        {  // grow the item's box by this warp's in-tile base cells
+          int mn[3], mx[3];
 #pragma unroll
-                for (int d = 0; d < D; ++d) {
-                  R s = qab[d];
-                  if (D == 3 && c == 1) s += Aff[d * D + 2];
-                  if (D == 3 && c == 2) s += (R)2 * Aff[d * D + 2];
-                  mv[d] = weight * s;
-                }
-                R4& t = mytile[lb + (D == 3 ? a * G::XS + b * T + c : a * T + b)];
-                R4 v = t;
-                v.x += weight * K.p_mass;
-                v.y += mv[0];
-                v.z += mv[1];
-                v.w += mv[2];
-                t = v;
-                __syncwarp(tm);
-              }
+          for (int d = 0; d < D; ++d) {
+            const int l = base[d] - o[d];
+            mn[d] = __reduce_min_sync(0xffffffffu, (active && in_tile) ? l : T);
+            mx[d] = __reduce_max_sync(0xffffffffu, (active && in_tile) ? l : -1);
+          }
+          if (lane == 0 && mx[0] >= 0) {
+#pragma unroll
+            for (int d = 0; d < D; ++d) {
+              atomicMin(&sbox[d], mn[d]);
+              atomicMax(&sbox[3 + d], mx[d]);
             }
-        } else if (mine) {  // outside the tile: straight to the global grid
+          }
+        }
+        // Lanes of a warp with the same base cell add into the same nodes and
+        // take turns (rank among peers); lanes of different base cells never
+        // share a node for the same stencil offset.  Binning orders records so
+        // that a warp's lanes are in different cells: one turn is the norm.
+        const int key = (active && in_tile) ? lb : -1 - lane;
+        const unsigned peers = __match_any_sync(0xffffffffu, key);
+        const int rank = __popc(peers & ((1u << lane) - 1u));
+        const int rounds = __reduce_max_sync(0xffffffffu, (unsigned)__popc(peers));
+        R4* mytile = ptile + warp * TNP;
+        for (int r = 0; r < rounds; ++r) {
+          const bool mine = active && rank == r;
+          const unsigned tm = __ballot_sync(0xffffffffu, mine && in_tile);  // lanes writing the tile this round
+          if (mine && in_tile) {
+            // Lanes add into their nodes offset by offset.  Lanes whose base
+            // cells are neighbours reach the same node at different offsets,
+            // so every offset's read-modify-write must be visible to the warp
+            // before the next one reads: __syncwarp orders them (without it
+            // the compiler and the shared-memory pipeline may overlap them
+            // and lose updates).
 #pragma unroll
-          for (int a = 0; a < 3; ++a)
+            for (int a = 0; a < 3; ++a)
 #pragma unroll
-            for (int b = 0; b < 3; ++b)
-#pragma unroll
-              for (int c = 0; c < (D == 3 ? 3 : 1); ++c) {
-                const R weight = D == 3 ? w[a][0] * w[b][1] * w[c][2] : w[a][0] * w[b][1];
-                R mv[3] = {0, 0, 0};
+              for (int b = 0; b < 3; ++b) {
+                const R wab = w[a][0] * w[b][1];
+                R qab[3];
 #pragma unroll
                 for (int d = 0; d < D; ++d) {
                   R s = q[d];
@@ -594,17 +572,59 @@ __global__ void __launch_bounds__(CH, AQ_STEP_MIN_BLOCKS) k_step(const __grid_co
                   if (a == 2) s += (R)2 * Aff[d * D + 0];
                   if (b == 1) s += Aff[d * D + 1];
                   if (b == 2) s += (R)2 * Aff[d * D + 1];
-                  if (D == 3 && c == 1) s += Aff[d * D + 2];
-                  if (D == 3 && c == 2) s += (R)2 * Aff[d * D + 2];
-                  mv[d] = weight * s;
+                  qab[d] = s;
                 }
-                R4* g = gout + cell_index<D>(K.res, base[0] + a, base[1] + b, D == 3 ? base[2] + c : 0);
-                red_add_node(g, weight * K.p_mass, mv[0], mv[1], mv[2]);
+#pragma unroll
+                for (int c = 0; c < (D == 3 ? 3 : 1); ++c) {
+                  const R weight = D == 3 ? wab * w[c][2] : wab;
+                  R mv[3] = {0, 0, 0};
+#pragma unroll
+                  for (int d = 0; d < D; ++d) {
+                    R s = qab[d];
+                    if (D == 3 && c == 1) s += Aff[d * D + 2];
+                    if (D == 3 && c == 2) s += (R)2 * Aff[d * D + 2];
+                    mv[d] = weight * s;
+                  }
+                  R4& t = mytile[lb + (D == 3 ? a * G::XS + b * T + c : a * T + b)];
+                  R4 v = t;
+                  v.x += weight * K.p_mass;
+                  v.y += mv[0];
+                  v.z += mv[1];
+                  v.w += mv[2];
+                  t = v;
+                  __syncwarp(tm);
+                }
               }
+          } else if (mine) {  // outside the tile: straight to the global grid
+#pragma unroll
+            for (int a = 0; a < 3; ++a)
+#pragma unroll
+              for (int b = 0; b < 3; ++b)
+#pragma unroll
+                for (int c = 0; c < (D == 3 ? 3 : 1); ++c) {
+                  const R weight = D == 3 ? w[a][0] * w[b][1] * w[c][2] : w[a][0] * w[b][1];
+                  R mv[3] = {0, 0, 0};
+#pragma unroll
+                  for (int d = 0; d < D; ++d) {
+                    R s = q[d];
+                    if (a == 1) s += Aff[d * D + 0];
+                    if (a == 2) s += (R)2 * Aff[d * D + 0];
+                    if (b == 1) s += Aff[d * D + 1];
+                    if (b == 2) s += (R)2 * Aff[d * D + 1];
+                    if (D == 3 && c == 1) s += Aff[d * D + 2];
+                    if (D == 3 && c == 2) s += (R)2 * Aff[d * D + 2];
+                    mv[d] = weight * s;
+                  }
+                  R4* g = gout + cell_index<D>(K.res, base[0] + a, base[1] + b, D == 3 ? base[2] + c : 0);
+                  red_add_node(g, weight * K.p_mass, mv[0], mv[1], mv[2]);
+                }
+          }
+          __syncwarp();
         }
-        __syncwarp();
       }
-      __syncthreads();
+    }  // units
+    __syncthreads();
+    if (A.do_p2g) {
       // sum the warp tiles, re-zero them, flush: one vector reduction per
       // node of the box the item's particles touched (base box + 2); the
       // tiles are zero outside it
@@ -634,6 +654,7 @@ __global__ void __launch_bounds__(CH, AQ_STEP_MIN_BLOCKS) k_step(const __grid_co
         red_add_node(gout + cell_index<D>(K.res, g0, g1, g2), sum.x, sum.y, sum.z, sum.w);
       }
     }
+    if (tid == 0) s_next = atomicAdd(A.item_ctr, 1);
     __syncthreads();
   }
   if (fl) atomicOr(A.status, fl);

@@ -52,20 +52,12 @@ __global__ void __launch_bounds__(256) k_bin(const __grid_constant__ aq_layout L
   if (fl) atomicOr(status, fl);
 }
 
-// A block of cnt records is cut into chunks of CH records and one last
-// chunk of the remainder: every warp but the last one of a block then has
-// all 32 lanes busy.
-__device__ __forceinline__ void chunk_of(int cnt, int local, int& c0, int& c1) {
-  c0 = (local / CH) * CH;
-  c1 = min(c0 + CH, cnt);
-}
-
 // Move record i to its sorted position.  A block's records are ordered
 // slot-major over the whole block: first the first record of every cell of
 // the block (in cell order), then the second record of every cell, and so
-// on; this sequence is then cut into chunks of at most CH (chunk_of), the
-// work items.  Consecutive records, i.e. the lanes of a warp in k_step, are
-// then in different cells except where a slot holds fewer than 32 cells.
+// on.  k_step's warps take this sequence 32 records at a time, so the lanes
+// of a warp are in different cells except where a slot holds fewer than 32
+// cells.
 __global__ void __launch_bounds__(256) k_scatter(const uint64_t* __restrict__ win, const int32_t* __restrict__ pin,
                                                  uint64_t* __restrict__ wout, int32_t* __restrict__ pout,
                                                  const int32_t* __restrict__ keys, const int32_t* __restrict__ ranks,
@@ -92,21 +84,14 @@ __global__ void __launch_bounds__(256) k_scatter(const uint64_t* __restrict__ wi
   pout[dst] = pin[i];
 }
 
+// One work item per occupied cell block: (block, first record, count).
 __global__ void k_items(const int32_t* __restrict__ start, int nblk, int4* __restrict__ items,
                         int32_t* __restrict__ n_items) {
   const int b = blockIdx.x * blockDim.x + threadIdx.x;
   if (b >= nblk) return;
   const int s = start[(int64_t)b * 64], e = start[(int64_t)(b + 1) * 64];
-  const int cnt = e - s;
-  if (cnt <= 0) return;
-  const int k = (cnt + CH - 1) / CH;
-  const int at = atomicAdd(n_items, k);
-  for (int j = 0, c0 = 0; j < k; ++j) {
-    int a, z;
-    chunk_of(cnt, c0, a, z);
-    items[at + j] = make_int4(b, s + a, z - a, 0);
-    c0 = z;
-  }
+  if (e <= s) return;
+  items[atomicAdd(n_items, 1)] = make_int4(b, s, e - s, 0);
 }
 
 // Exclusive scan of n int32 counts into out[0..n] (out[n] = total), in
@@ -361,6 +346,8 @@ struct aq_sim {
   int32_t *keys = nullptr, *ranks = nullptr, *cell_count = nullptr, *cell_start = nullptr, *scan_sums = nullptr;
   int4* items = nullptr;
   int32_t* n_items = nullptr;
+  int32_t* item_ctr = nullptr;  // [2] k_step's item claim counters
+  int64_t step_launches = 0;
   int64_t max_items = 0;
   unsigned* status = nullptr;
   unsigned long long* fallbacks = nullptr;
@@ -421,7 +408,7 @@ struct SimImpl final : SimBase {
   }
 
   size_t smem_bytes() const override {
-    size_t b = sizeof(typename R4T<R>::type) * (NWARP + 1) * Geo<D>::TNP + sizeof(int32_t) * CH;
+    const size_t b = sizeof(typename R4T<R>::type) * (NWARP + 1) * Geo<D>::TNP;
     return b + sizeof(uint64_t) * (size_t)CH * s->WS;
   }
 
@@ -456,6 +443,11 @@ struct SimImpl final : SimBase {
     a.pid = S_->pid[S_->cur];
     a.items = S_->items;
     a.n_items = S_->n_items;
+    // two claim counters alternate between launches; each launch zeroes the
+    // one the next launch uses (both start at zero)
+    a.item_ctr = S_->item_ctr + (S_->step_launches & 1);
+    a.item_ctr_next = S_->item_ctr + ((S_->step_launches + 1) & 1);
+    ++S_->step_launches;
     a.grid_in = gin;
     a.grid_out = gout;
     a.status = S_->status;
@@ -624,7 +616,7 @@ int aq_sim_create(const aq_params* P, const aq_layout* L, aq_sim** out) {
   }
   s->nblk = nb[0] * nb[1] * nb[2];
   s->nkeys = (int64_t)s->nblk * 64;
-  s->max_items = s->n / CH + s->nblk + 1;
+  s->max_items = s->nblk + 1;
   const size_t rsz = P->precision ? sizeof(double) : sizeof(float);
   const int64_t n = s->n;
   const int nt = (int)((s->nkeys + SCAN_TILE - 1) / SCAN_TILE);
@@ -655,6 +647,7 @@ int aq_sim_create(const aq_params* P, const aq_layout* L, aq_sim** out) {
   alloc((void**)&s->scan_sums, sizeof(int32_t) * (nt + 1));
   alloc((void**)&s->items, sizeof(int4) * s->max_items);
   alloc((void**)&s->n_items, sizeof(int32_t));
+  alloc((void**)&s->item_ctr, 2 * sizeof(int32_t));
   alloc((void**)&s->status, sizeof(unsigned));
   alloc((void**)&s->fallbacks, sizeof(unsigned long long));
   alloc((void**)&s->rmax, sizeof(double) * AQ_MAX_SLOTS);
@@ -675,6 +668,7 @@ int aq_sim_create(const aq_params* P, const aq_layout* L, aq_sim** out) {
   if (e == cudaSuccess) e = cudaMemset(s->words[0], 0, sizeof(uint64_t) * (n * s->W + 2));
   if (e == cudaSuccess) e = cudaMemset(s->status, 0, sizeof(unsigned));
   if (e == cudaSuccess) e = cudaMemset(s->fallbacks, 0, sizeof(unsigned long long));
+  if (e == cudaSuccess) e = cudaMemset(s->item_ctr, 0, 2 * sizeof(int32_t));
   if (e != cudaSuccess) {
     set_last_cuda_error(e, "cudaMemset");
     free_sim(s);
