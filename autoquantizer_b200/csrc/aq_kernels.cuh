@@ -394,31 +394,59 @@ __global__ void __launch_bounds__(CH, AQ_STEP_MIN_BLOCKS) k_step(const __grid_co
         const int lb = in_tile ? (D == 3 ? (base[0] - o[0]) * G::XS + (base[1] - o[1]) * T + (base[2] - o[2])
                                          : (base[0] - o[0]) * T + (base[1] - o[1]))
                                : 0;
-        if (!in_tile) ++nfall;
+        if (D == 3 && in_tile) {
+          // separable in z: per (a, b) the three z-neighbours are summed
+          // with weights w_c and c w_c first (P, Q), then spread with w_a w_b
+          const R tw2 = (R)2 * w[2][2];
 #pragma unroll
-        for (int a = 0; a < 3; ++a)
+          for (int a = 0; a < 3; ++a)
 #pragma unroll
-          for (int b = 0; b < 3; ++b) {
-            const R wab = w[a][0] * w[b][1];
+            for (int b = 0; b < 3; ++b) {
+              const R4* gp = gtile + lb + a * G::XS + b * T;
+              const R4 g0 = gp[0], g1 = gp[1], g2 = gp[2];
+              const R P[3] = {w[0][2] * g0.y + w[1][2] * g1.y + w[2][2] * g2.y,
+                              w[0][2] * g0.z + w[1][2] * g1.z + w[2][2] * g2.z,
+                              w[0][2] * g0.w + w[1][2] * g1.w + w[2][2] * g2.w};
+              const R Q[3] = {w[1][2] * g1.y + tw2 * g2.y, w[1][2] * g1.z + tw2 * g2.z, w[1][2] * g1.w + tw2 * g2.w};
+              const R wab = w[a][0] * w[b][1];
 #pragma unroll
-            for (int c = 0; c < (D == 3 ? 3 : 1); ++c) {
-              const R weight = D == 3 ? wab * w[c][2] : wab;
-              const R4 g = in_tile ? gtile[lb + (D == 3 ? a * G::XS + b * T + c : a * T + b)]
-                                   : gin[cell_index<D>(K.res, base[0] + a, base[1] + b, D == 3 ? base[2] + c : 0)];
-              const R gv[3] = {g.y, g.z, g.w};
-              const int off[3] = {a, b, c};
+              for (int d = 0; d < 3; ++d) {
+                const R wp = wab * P[d];
+                nv[d] += wp;
+                if (a == 1) Sm[d][0] += wp;
+                if (a == 2) Sm[d][0] += (R)2 * wp;
+                if (b == 1) Sm[d][1] += wp;
+                if (b == 2) Sm[d][1] += (R)2 * wp;
+                Sm[d][2] += wab * Q[d];
+              }
+            }
+        } else {
+          if (!in_tile) ++nfall;
 #pragma unroll
-              for (int d = 0; d < D; ++d) {
-                const R wg = weight * gv[d];
-                nv[d] += wg;
+          for (int a = 0; a < 3; ++a)
 #pragma unroll
-                for (int e = 0; e < D; ++e) {
-                  if (off[e] == 1) Sm[d][e] += wg;
-                  if (off[e] == 2) Sm[d][e] += (R)2 * wg;
+            for (int b = 0; b < 3; ++b) {
+              const R wab = w[a][0] * w[b][1];
+#pragma unroll
+              for (int c = 0; c < (D == 3 ? 3 : 1); ++c) {
+                const R weight = D == 3 ? wab * w[c][2] : wab;
+                const R4 g = in_tile ? gtile[lb + (D == 3 ? a * G::XS + b * T + c : a * T + b)]
+                                     : gin[cell_index<D>(K.res, base[0] + a, base[1] + b, D == 3 ? base[2] + c : 0)];
+                const R gv[3] = {g.y, g.z, g.w};
+                const int off[3] = {a, b, c};
+#pragma unroll
+                for (int d = 0; d < D; ++d) {
+                  const R wg = weight * gv[d];
+                  nv[d] += wg;
+#pragma unroll
+                  for (int e = 0; e < D; ++e) {
+                    if (off[e] == 1) Sm[d][e] += wg;
+                    if (off[e] == 2) Sm[d][e] += (R)2 * wg;
+                  }
                 }
               }
             }
-          }
+        }
         // new_C = 4 inv_dx sum w g_v (off - fx)^T;  new_x = x + dt new_v
         R nC[D * D];
 #pragma unroll
