@@ -106,7 +106,8 @@ struct StepArgs {
   double* rmax;
   double* rmin;
   uint64_t sk;          // dithering key of the G2P substep
-  int do_g2p, do_p2g, ranges, _pad;
+  int do_g2p, do_p2g, ranges;
+  int raw_in;           // grid_in holds P2G sums: apply grid_op while reading
 };
 
 // Layout from the kernel parameter (nvcc build).
@@ -170,6 +171,30 @@ __device__ __forceinline__ void atomic_min_d(double* a, double v) {
     if (prev == old) break;
     old = prev;
   }
+}
+
+// grid_op (mpm_solver.py:633-665) of one node (m, m v) at grid index I:
+// velocity, gravity, optional friction on the floor, sticky walls.
+template <int D, class R, class R4>
+__device__ __forceinline__ R4 grid_op_node(const SimK<R>& K, R4 g, int I0, int I1, int I2) {
+  const int I[3] = {I0, I1, I2};
+  const R inv_m = (R)1 / (g.x + (R)1e-10);
+  R v[3] = {inv_m * g.y, inv_m * g.z, D == 3 ? inv_m * g.w : (R)0};
+  v[1] -= K.dt * K.grav;
+  if (K.friction && I[1] < K.lb[1] && v[1] < (R)0) {  // n = (0,1,0), v = (v - n (n.v)) * 0.02
+    v[1] = 0;
+#pragma unroll
+    for (int d = 0; d < D; ++d) v[d] *= (R)0.02;
+  }
+#pragma unroll
+  for (int k = 0; k < D; ++k) {
+    if (I[k] < K.lb[k] && v[k] < (R)0) v[k] = 0;
+    if (I[k] > K.ub[k] && v[k] > (R)0) v[k] = 0;
+  }
+  g.y = v[0];
+  g.z = v[1];
+  g.w = v[2];
+  return g;
 }
 
 // ------------------------------------------------------------- materials
@@ -347,7 +372,12 @@ __global__ void __launch_bounds__(CH, AQ_STEP_MIN_BLOCKS) k_step(const __grid_co
         const int g0 = o[0] + l0, g1 = o[1] + l1, g2 = o[2] + l2;
         const bool ok = (D == 3 ? l1 < T : true) && g0 >= 0 && g0 < K.res[0] && g1 >= 0 && g1 < K.res[1] &&
                         (D == 2 || (g2 >= 0 && g2 < K.res[2]));
-        gtile[j] = ok ? gin[cell_index<D>(K.res, g0, g1, g2)] : zero4;
+        R4 g = zero4;
+        if (ok) {
+          g = gin[cell_index<D>(K.res, g0, g1, g2)];
+          if (A.raw_in) g = grid_op_node<D, R>(K, g, g0, g1, g2);
+        }
+        gtile[j] = g;
       }
     }
     __syncthreads();
@@ -430,8 +460,14 @@ __global__ void __launch_bounds__(CH, AQ_STEP_MIN_BLOCKS) k_step(const __grid_co
 #pragma unroll
               for (int c = 0; c < (D == 3 ? 3 : 1); ++c) {
                 const R weight = D == 3 ? wab * w[c][2] : wab;
-                const R4 g = in_tile ? gtile[lb + (D == 3 ? a * G::XS + b * T + c : a * T + b)]
-                                     : gin[cell_index<D>(K.res, base[0] + a, base[1] + b, D == 3 ? base[2] + c : 0)];
+                R4 g;
+                if (in_tile) {
+                  g = gtile[lb + (D == 3 ? a * G::XS + b * T + c : a * T + b)];
+                } else {
+                  const int n0 = base[0] + a, n1 = base[1] + b, n2 = D == 3 ? base[2] + c : 0;
+                  g = gin[cell_index<D>(K.res, n0, n1, n2)];
+                  if (A.raw_in) g = grid_op_node<D, R>(K, g, n0, n1, n2);
+                }
                 const R gv[3] = {g.y, g.z, g.w};
                 const int off[3] = {a, b, c};
 #pragma unroll

@@ -2,11 +2,12 @@
 // of the substep (include/aq.h).  The fused substep kernel k_step lives in
 // aq_kernels.cuh (see there for the data layout and the algorithm).
 //
-// Per substep: k_step (G2P of substep k + P2G of substep k+1) and k_grid
-// (grid_op of the accumulated grid, clear of the other).  Every
-// sort_interval substeps the records are re-binned: k_bin (cell key and
-// rank), an exclusive scan of the per-cell counts, k_scatter (move records
-// and ids into slot-major chunks), k_items (work items).
+// Per substep: one k_step launch (grid_op of the accumulated grid as each
+// tile is staged, G2P of substep k, P2G of substep k+1 into the other grid,
+// which a memset clears first).  Every sort_interval substeps the records
+// are re-binned: k_bin (cell key and rank), an exclusive scan of the
+// per-cell counts, k_scatter (records and ids into block-wide slot-major
+// order), k_items (one work item per occupied block).
 #include <math.h>
 #include <stdio.h>
 #include <string.h>
@@ -174,50 +175,6 @@ __global__ void __launch_bounds__(SCAN_T) k_scan_apply(const int32_t* __restrict
   }
 }
 
-// grid_op (mpm_solver.py:633-665) on `acc`; zero `clr`.
-template <int D, class R>
-__global__ void __launch_bounds__(256) k_grid(const SimK<R> K, void* acc_, void* clr_, int64_t ncell) {
-  typedef typename R4T<R>::type R4;
-  const int64_t c = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
-  if (c >= ncell) return;
-  R4* acc = reinterpret_cast<R4*>(acc_);
-  R4* clr = reinterpret_cast<R4*>(clr_);
-  if (clr) {
-    R4 z;
-    z.x = z.y = z.z = z.w = 0;
-    clr[c] = z;
-  }
-  if (!acc) return;
-  int I[3];
-  if (D == 3) {
-    I[2] = (int)(c % K.res[2]);
-    I[1] = (int)((c / K.res[2]) % K.res[1]);
-    I[0] = (int)(c / ((int64_t)K.res[2] * K.res[1]));
-  } else {
-    I[1] = (int)(c % K.res[1]);
-    I[0] = (int)(c / K.res[1]);
-    I[2] = 0;
-  }
-  R4 g = acc[c];
-  const R inv_m = (R)1 / (g.x + (R)1e-10);
-  R v[3] = {inv_m * g.y, inv_m * g.z, D == 3 ? inv_m * g.w : (R)0};
-  v[1] -= K.dt * K.grav;
-  if (K.friction && I[1] < K.lb[1] && v[1] < (R)0) {  // n = (0,1,0), v = (v - n (n.v)) * 0.02
-    v[1] = 0;
-#pragma unroll
-    for (int d = 0; d < D; ++d) v[d] *= (R)0.02;
-  }
-#pragma unroll
-  for (int k = 0; k < D; ++k) {
-    if (I[k] < K.lb[k] && v[k] < (R)0) v[k] = 0;
-    if (I[k] > K.ub[k] && v[k] > (R)0) v[k] = 0;
-  }
-  g.y = v[0];
-  g.z = v[1];
-  g.w = v[2];
-  acc[c] = g;
-}
-
 // decode records into particle order
 template <class T>
 __global__ void __launch_bounds__(128) k_get_state(const __grid_constant__ aq_layout L,
@@ -340,7 +297,6 @@ struct aq_sim {
   int32_t* pid[2] = {nullptr, nullptr};
   int cur = 0;
   void* grid[2] = {nullptr, nullptr};
-  int zero_grid = 0;
   int64_t ncell = 0, nkeys = 0;
   int nblk = 0;
   int32_t *keys = nullptr, *ranks = nullptr, *cell_count = nullptr, *cell_start = nullptr, *scan_sums = nullptr;
@@ -436,6 +392,8 @@ struct SimImpl final : SimBase {
   }
 
   int launch_step(int do_g2p, int do_p2g, void* gin, void* gout, cudaStream_t st) {
+    // the P2G target starts at zero (profiled as the grid pass)
+    if (do_p2g && (rc_ = clear_grid(gout, st))) return rc_;
     aq_sim* S_ = s;
     StepArgs a;
     memset(&a, 0, sizeof(a));
@@ -458,6 +416,7 @@ struct SimImpl final : SimBase {
     a.do_g2p = do_g2p;
     a.do_p2g = do_p2g;
     a.ranges = S_->ranges_on;
+    a.raw_in = do_g2p;  // grid_in holds the previous P2G sums; grid_op runs as the tile is staged
     const bool prof = S_->prof_on && S_->prof_n[0] < aq_sim::PROF_CAP;
     if (prof) AQ_CUDA_TRY(cudaEventRecord(S_->prof_ev[0][2 * S_->prof_n[0]], st));
     if (S_->jit_fn) {
@@ -475,13 +434,12 @@ struct SimImpl final : SimBase {
     return AQ_OK;
   }
 
-  int launch_grid(void* acc, void* clr, cudaStream_t st) {
+  int rc_ = 0;
+  int clear_grid(void* g, cudaStream_t st) {
     const bool prof = s->prof_on && s->prof_n[1] < aq_sim::PROF_CAP;
     if (prof) AQ_CUDA_TRY(cudaEventRecord(s->prof_ev[1][2 * s->prof_n[1]], st));
-    k_grid<D, R><<<grid_for(s->ncell, 256), 256, 0, st>>>(K, acc, clr, s->ncell);
-    AQ_CUDA_TRY(cudaGetLastError());
+    AQ_CUDA_TRY(cudaMemsetAsync(g, 0, sizeof(typename R4T<R>::type) * s->ncell, st));
     if (prof) AQ_CUDA_TRY(cudaEventRecord(s->prof_ev[1][2 * s->prof_n[1]++ + 1], st));
-    s->launches += 1;
     return AQ_OK;
   }
 
@@ -495,20 +453,20 @@ struct SimImpl final : SimBase {
       }
       int m = interval - S_->since_sort;
       if (m > n) m = n;
-      int a = S_->zero_grid;
+      // P2G of the first substep, then per substep one fused launch: grid_op
+      // applied while staging the tile, G2P, P2G of the next substep into
+      // the other (cleared) grid
+      int a = 0;
       if ((rc = launch_step(0, 1, nullptr, S_->grid[a], st))) return rc;
       for (int k = 0; k < m; ++k) {
         const int b = 1 - a;
-        if ((rc = launch_grid(S_->grid[a], S_->grid[b], st))) return rc;
         if (k + 1 < m) {
           if ((rc = launch_step(1, 1, S_->grid[a], S_->grid[b], st))) return rc;
-          ++S_->step;
           a = b;
         } else {
           if ((rc = launch_step(1, 0, S_->grid[a], nullptr, st))) return rc;
-          ++S_->step;
-          S_->zero_grid = b;
         }
+        ++S_->step;
       }
       S_->since_sort += m;
       n -= m;

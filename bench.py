@@ -361,7 +361,7 @@ def run_ours(args, ws, rank, local):
             "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
                          "frac": achieved / peak, "traffic": ncu_traffic(), "peak_kind": peak_kind,
                          "kernel": "k_step (fused G2P+P2G)", "avg_launch_ms": step_ms,
-                         "alg_bytes_per_launch": alg_bytes, "k_grid_avg_ms": grid_ms},
+                         "alg_bytes_per_launch": alg_bytes, "grid_clear_avg_ms": grid_ms},
             "cpu_baseline": cpu,
             "e2e": {"value": e2e_val, "unit": UNIT, "h2d_bytes_per_step": int(h_in.numel() * 8),
                     "d2h_bytes_per_step": int(h_out.numel() * 8 + 8), "substeps_per_step": frame,

@@ -228,7 +228,8 @@ int aq_sim_launches(const aq_sim* sim, int64_t* h_out);
  * substep kernel (k_step) and of the grid kernel (k_grid) on the stream they
  * run on.  No reference counterpart (the reference profiles through CUPTI,
  * taichi_submission/taichi/program/kernel_profiler.h:46).  which: 0 = k_step,
- * 1 = k_grid.  profile_get synchronizes and resets the accumulators. */
+ * 1 = the grid clear before each P2G.  profile_get synchronizes and resets
+ * the accumulators. */
 int aq_sim_profile_enable(aq_sim* sim, int32_t on);
 int aq_sim_profile_get(aq_sim* sim, int32_t which, double* h_total_ms, int64_t* h_launches);
 
