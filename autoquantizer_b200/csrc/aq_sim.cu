@@ -70,15 +70,22 @@ __global__ void __launch_bounds__(256) k_scatter(const uint64_t* __restrict__ wi
   const int64_t c0 = (int64_t)(key >> 6) * 64;
   const int myc = key & 63;
   // records before this one: min(count, r) of every cell, plus one more for
-  // every earlier cell that has an r-th record
+  // every earlier cell that has an r-th record.  The block's 65 offsets are
+  // read as int4 vectors (start is 256-byte aligned, c0 a multiple of 64).
+  const int4* st4 = reinterpret_cast<const int4*>(start + c0);
+  int4 v = __ldg(st4);
+  const int64_t b0 = v.x;
   int t = 0;
-  int64_t s0 = start[c0];
-  const int64_t b0 = s0;
-  for (int k = 0; k < 64; ++k) {
-    const int64_t s1 = start[c0 + k + 1];
-    const int nk = (int)(s1 - s0);
-    t += min(nk, r) + ((k < myc && nk > r) ? 1 : 0);
-    s0 = s1;
+#pragma unroll 4
+  for (int q = 0; q < 16; ++q) {
+    const int4 nv = q < 15 ? __ldg(st4 + q + 1) : make_int4(__ldg(start + c0 + 64), 0, 0, 0);
+    const int ss[5] = {v.x, v.y, v.z, v.w, nv.x};
+#pragma unroll
+    for (int j = 0; j < 4; ++j) {
+      const int k = 4 * q + j, nk = ss[j + 1] - ss[j];
+      t += min(nk, r) + ((k < myc && nk > r) ? 1 : 0);
+    }
+    v = nv;
   }
   const int64_t dst = b0 + t;
   for (int j = 0; j < W; ++j) wout[dst * W + j] = win[i * W + j];
