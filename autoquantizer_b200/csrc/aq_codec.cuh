@@ -112,17 +112,21 @@ struct BitWriter {
 
 template <class R>
 __device__ __forceinline__ R dequant_fixed(const aq_slot& S, bool f64, uint32_t code) {
+  // adding a zero offset is skipped: q * scale is never -0, so it is exact
   if (f64) {
     double q = S.is_signed ? (double)sext32(code, S.bits) : (double)code;
-    return (R)__dadd_rn(__dmul_rn(q, S.scale_f64), S.offset_f64);
+    const double y = __dmul_rn(q, S.scale_f64);
+    return (R)(S.offset_f64 != 0.0 ? __dadd_rn(y, S.offset_f64) : y);
   }
   float q = S.is_signed ? __int2float_rn(sext32(code, S.bits)) : __uint2float_rn(code);
-  return (R)__fadd_rn(__fmul_rn(q, S.scale_f32), S.offset_f32);
+  const float y = __fmul_rn(q, S.scale_f32);
+  return (R)(S.offset_f32 != 0.0f ? __fadd_rn(y, S.offset_f32) : y);
 }
 
 // u is the dithering uniform in the compute type (ignored unless dith).
 __device__ __forceinline__ uint32_t quant_fixed_f32(const aq_slot& S, bool dith, float v, float u) {
-  float c = __fmul_rn(__fsub_rn(v, S.offset_f32), S.inv_scale_f32);
+  // v - 0 == v exactly (also for -0 and NaN): a zero offset is skipped
+  float c = __fmul_rn(S.offset_f32 != 0.0f ? __fsub_rn(v, S.offset_f32) : v, S.inv_scale_f32);
   if (dith) c = __fsub_rn(__fadd_rn(c, u), 0.5f);
   c = __fadd_rn(c, copysignf(0.5f, c));
   uint32_t q = S.is_signed ? (uint32_t)__float2int_rz(c) : __float2uint_rz(c);
@@ -130,7 +134,7 @@ __device__ __forceinline__ uint32_t quant_fixed_f32(const aq_slot& S, bool dith,
 }
 
 __device__ __forceinline__ uint32_t quant_fixed_f64(const aq_slot& S, bool dith, double v, double u) {
-  double c = __dmul_rn(__dsub_rn(v, S.offset_f64), S.inv_scale_f64);
+  double c = __dmul_rn(S.offset_f64 != 0.0 ? __dsub_rn(v, S.offset_f64) : v, S.inv_scale_f64);
   if (dith) c = __dsub_rn(__dadd_rn(c, u), 0.5);
   c = __dadd_rn(c, copysign(0.5, c));
   uint32_t q = S.is_signed ? (uint32_t)__double2int_rz(c) : __double2uint_rz(c);
