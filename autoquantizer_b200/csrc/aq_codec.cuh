@@ -26,9 +26,13 @@ namespace aq {
 // ------------------------------------------------------------------ RNG
 // Counter-based uniform per (seed, step, particle id, slot): SplitMix64
 // finalizer (Steele, Lea & Flood 2014) for the per-step and per-particle
-// keys, Wellons' lowbias32 hash per draw.  The reference's generator is a
-// per-thread xorshift128 (runtime.cpp:522-536,1560-1589) whose stream depends
-// on the thread schedule; this one is reproducible.
+// keys; draw j of a particle is element j + 1 of the 32-bit LCG
+// x' = 747796405 x + 2891336453 (the PCG multiplier; full period) started at
+// the key's low half, reached in one multiply-add with jump constants known
+// at compile time, then x ^ (x >> 16) ^ (high half of the key).  The
+// reference's generator is a per-thread xorshift128 (runtime.cpp:522-536,
+// 1560-1589) whose stream depends on the thread schedule; this one is
+// reproducible.
 
 __host__ __device__ __forceinline__ uint64_t mix64(uint64_t z) {
   z += 0x9E3779B97F4A7C15ull;
@@ -37,14 +41,23 @@ __host__ __device__ __forceinline__ uint64_t mix64(uint64_t z) {
   return z ^ (z >> 31);
 }
 
-__host__ __device__ __forceinline__ uint32_t lowbias32(uint32_t x) {
-  x ^= x >> 16;
-  x *= 0x7feb352du;
-  x ^= x >> 15;
-  x *= 0x846ca68bu;
-  x ^= x >> 16;
-  return x;
+// LCG jump constants: element n of the sequence from x0 is A[n] x0 + C[n]
+constexpr int AQ_LCG_JUMPS = 2 * AQ_MAX_SLOTS + 1;
+struct LcgJumps {
+  uint32_t a[AQ_LCG_JUMPS], c[AQ_LCG_JUMPS];
+};
+__host__ __device__ constexpr LcgJumps make_lcg_jumps() {
+  LcgJumps t{};
+  uint32_t a = 1u, c = 0u;
+  for (int n = 0; n < AQ_LCG_JUMPS; ++n) {
+    t.a[n] = a;
+    t.c[n] = c;
+    a *= 747796405u;
+    c = c * 747796405u + 2891336453u;
+  }
+  return t;
 }
+__device__ constexpr LcgJumps kLcgJumps = make_lcg_jumps();
 
 __host__ __device__ __forceinline__ uint64_t step_key(uint64_t seed, int64_t step) {
   return mix64(seed + (uint64_t)(step + 1) * 0xD1B54A32D192ED03ull);
@@ -55,7 +68,8 @@ __device__ __forceinline__ uint64_t particle_key(uint64_t sk, int32_t pid) {
 }
 
 __device__ __forceinline__ uint32_t draw32(uint64_t pk, uint32_t j) {
-  return lowbias32((uint32_t)pk + 0x9E3779B9u * (j + 1u)) ^ (uint32_t)(pk >> 32);
+  const uint32_t x = kLcgJumps.a[j + 1u] * (uint32_t)pk + kLcgJumps.c[j + 1u];
+  return x ^ (x >> 16) ^ (uint32_t)(pk >> 32);
 }
 
 // rand_f32 / rand_f64 of runtime.cpp:1579-1585: u32 * 2^-32, u64 * 2^-64

@@ -110,20 +110,14 @@ static int64_t sext(uint64_t code, int nb) {
 /* Counter-based generator (the reference's per-thread xorshift128 of
  * runtime.cpp:522-536,1560-1589 depends on the thread schedule; this one
  * depends only on (seed, step, particle id, slot)).  SplitMix64 finalizer
- * (Steele, Lea & Flood 2014) and Wellons' lowbias32 integer hash. */
+ * (Steele, Lea & Flood 2014) for the keys; draw j is element j + 1 of the
+ * 32-bit LCG x' = 747796405 x + 2891336453 started at the key's low half,
+ * output x ^ (x >> 16) ^ (key's high half). */
 static uint64_t mix64(uint64_t z) {
   z += 0x9E3779B97F4A7C15ull;
   z = (z ^ (z >> 30)) * 0xBF58476D1CE4E5B9ull;
   z = (z ^ (z >> 27)) * 0x94D049BB133111EBull;
   return z ^ (z >> 31);
-}
-static uint32_t lowbias32(uint32_t x) {
-  x ^= x >> 16;
-  x *= 0x7feb352du;
-  x ^= x >> 15;
-  x *= 0x846ca68bu;
-  x ^= x >> 16;
-  return x;
 }
 uint64_t or_step_key(uint64_t seed, int64_t step) {
   return mix64(seed + (uint64_t)(step + 1) * 0xD1B54A32D192ED03ull);
@@ -132,7 +126,9 @@ uint64_t or_particle_key(uint64_t step_key, int32_t pid) {
   return mix64(step_key ^ ((uint64_t)(uint32_t)pid * 0x9E3779B97F4A7C15ull));
 }
 uint32_t or_draw32(uint64_t pk, uint32_t j) {
-  return lowbias32((uint32_t)pk + 0x9E3779B9u * (j + 1u)) ^ (uint32_t)(pk >> 32);
+  uint32_t x = (uint32_t)pk;
+  for (uint32_t n = 0; n <= j; ++n) x = x * 747796405u + 2891336453u; /* element j + 1 */
+  return x ^ (x >> 16) ^ (uint32_t)(pk >> 32);
 }
 /* runtime.cpp:1579-1585: rand_f32 = rand_u32 * 2^-32, rand_f64 = rand_u64 * 2^-64 */
 float or_uniform_f32(uint64_t pk, int slot) {

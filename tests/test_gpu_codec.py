@@ -120,7 +120,7 @@ def test_dithering_ratio_on_gpu():
     L = rec.build()
     out = gpu_decode(L, gpu_encode(L, np.full((400000, 1), 1.1), seed=1234, step=7))[:, 0]
     up, down = (out == 1.125).sum(), (out == 1.0).sum()
-    assert up + down == 400000 and abs(up / down - 4) < 0.03
+    assert up + down == 400000 and abs(up / down - 4) < 0.05  # three binomial standard deviations
 
 
 def test_c2_record_words_match_oracle_at_full_size():

@@ -50,6 +50,12 @@ def test_fluid_2d_ranges_match_reference(tmp_path):
 
 
 def test_elastic_2d_error_bound_runs_meet_the_drivers_criterion(tmp_path):
+    """The reference driver reports the fraction of its N runs with
+    |loss - f64 loss| < 3 eps f64 loss (run_mpm_elastic_2d.py:190-207).  The
+    scene is chaotic over 8192 substeps (and P2G sums in no fixed order), so
+    single runs can miss; 20 runs measured on a B200 succeeded 18 times.
+    Here 10 runs must succeed at least 6 times (a 90 % rate fails that with
+    probability 0.2 %)."""
     exp = D.Elastic2D()
     cfg = exp.config()
     gfn, rfn = D._paths(exp, str(tmp_path))
@@ -59,10 +65,12 @@ def test_elastic_2d_error_bound_runs_meet_the_drivers_criterion(tmp_path):
     np.save(rfn, np.array(GOLD["ranges"]["elastic_2d/elastic_2d.npy"]))
     eps = 0.1
     sol = D.solve(exp, cfg, str(tmp_path), D.EB, eps)
-    loss = D.run(exp, cfg, 3)
-    print("elastic_2d EB eps %g bits %s losses %s (f64 %.3f)" % (eps, sol["bits"], loss, exp.f64_data))
+    loss = D.run(exp, cfg, 10)
+    ok = np.abs(loss - exp.f64_data) < 3 * eps * exp.f64_data
+    print("elastic_2d EB eps %g bits %s losses %s (f64 %.3f) succeed %.2f" % (eps, sol["bits"], loss, exp.f64_data,
+                                                                              ok.mean()))
     assert sol["compression_rate"] < 0.5
-    assert np.all(np.abs(loss - exp.f64_data) < 3 * eps * exp.f64_data)
+    assert ok.mean() >= 0.6
     assert len(set(loss.tolist())) > 1  # dithering seeds differ between runs
 
 
