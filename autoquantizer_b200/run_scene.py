@@ -1,6 +1,7 @@
 """Run one of the seeded scenes for a number of substeps and print timing.
 
     python -m autoquantizer_b200.run_scene --scene mixed_boxes_3d --substeps 8 [--fp32] [--n N] [--grid G]
+    python -m autoquantizer_b200.run_scene --device-gen --n 300000000 --grid 640 --substeps 50
 
 Used as the target of ncu captures (profiles/ lists the exact commands).
 """
@@ -19,6 +20,8 @@ def main():
     ap.add_argument("--grid", type=int, default=None)
     ap.add_argument("--fp32", action="store_true", help="FP32 particle state instead of the quantized record")
     ap.add_argument("--sort-interval", type=int, default=None)
+    ap.add_argument("--device-gen", action="store_true",
+                    help="mixed_boxes_3d generated on the GPU (large particle counts)")
     args = ap.parse_args()
 
     import torch
@@ -33,7 +36,12 @@ def main():
         kw["n_grid"] = args.grid
     if args.fp32 and args.scene in ("mixed_boxes_3d", "dam_break_2d"):
         kw["quantized"] = False
-    cfg, vals = getattr(scenes, args.scene)(**kw)
+    if args.device_gen:
+        if args.scene != "mixed_boxes_3d" or args.fp32:
+            ap.error("--device-gen builds the quantized mixed_boxes_3d scene only")
+        cfg, vals = scenes.mixed_boxes_3d_device(n=kw.get("n", 2097152), n_grid=kw.get("n_grid", 128))
+    else:
+        cfg, vals = getattr(scenes, args.scene)(**kw)
     if args.sort_interval:
         cfg.sort_interval = args.sort_interval
     s = MPMSolver(cfg)
@@ -45,8 +53,10 @@ def main():
     torch.cuda.synchronize()
     dt = time.perf_counter() - t0
     fl, fb = s.status()
-    print(json.dumps({"scene": args.scene, "particles": vals.shape[0], "substeps": args.substeps,
-                      "ms_per_substep": 1e3 * dt / args.substeps, "bytes_per_particle": s.bytes_per_particle(),
+    print(json.dumps({"scene": args.scene, "particles": int(cfg.n_particles), "substeps": args.substeps,
+                      "ms_per_substep": 1e3 * dt / args.substeps,
+                      "particle_substeps_per_s": cfg.n_particles * args.substeps / dt,
+                      "bytes_per_particle": s.bytes_per_particle(),
                       "status": fl, "tile_fallbacks": fb}))
 
 

@@ -125,6 +125,41 @@ def mixed_boxes_3d(seed=0, n=2097152, n_grid=128, quantized=True, precision="f32
     return c, _values(c, x, np.concatenate(ms))
 
 
+def mixed_boxes_3d_device(seed=0, n=2097152, n_grid=128):
+    """The 3D throughput scene generated on the GPU (for sizes whose
+    n x n_slots values would not fit host memory): the same configuration,
+    box layout and materials as mixed_boxes_3d (numpy default_rng(seed)),
+    particle positions drawn with torch's CUDA generator (seeded with seed),
+    dt scaled with the cell size (2e-5 at 128 cells).  Returns the config and
+    a CUDA float32 tensor (n x n_slots) for MPMSolver.set_particles."""
+    import torch
+
+    c, _ = mixed_boxes_3d(seed=seed, n=4, n_grid=n_grid)
+    c.n_particles = n
+    c.dt = 2e-5 * 128.0 / n_grid
+    rng = np.random.default_rng(seed)
+    rng.uniform(3, 5, 2), rng.uniform(0.2, 0.4, 2)  # the draws mixed_boxes_3d spends on the materials
+    sizes = rng.uniform(0.25, 0.4, (4, 3))
+    lows = np.array([rng.uniform(0.08, 0.92 - s) for s in sizes.ravel()]).reshape(4, 3)
+    vol = sizes.prod(1)
+    counts = np.floor(n * vol / vol.sum()).astype(np.int64)
+    counts[-1] = n - counts[:-1].sum()
+    ns = 2 * 3 + 9 + 9 + 1
+    gen = torch.Generator(device="cuda")
+    gen.manual_seed(int(seed))
+    vals = torch.zeros((n, ns), dtype=torch.float32, device="cuda")
+    vals[:, 15] = vals[:, 19] = vals[:, 23] = 1.0  # F = I
+    at = 0
+    for b in range(4):
+        k = int(counts[b])
+        lo = torch.tensor(lows[b], dtype=torch.float32, device="cuda")
+        sz = torch.tensor(sizes[b], dtype=torch.float32, device="cuda")
+        vals[at:at + k, :3] = lo + torch.rand((k, 3), generator=gen, device="cuda") * sz
+        vals[at:at + k, 24] = float(b)
+        at += k
+    return c, vals
+
+
 def falling_block_3d(seed=0, n=262144, n_grid=64):
     c = _base(3, n_grid, n, 5e-5)
     c.use_fluid = False
