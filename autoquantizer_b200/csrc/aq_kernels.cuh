@@ -11,27 +11,33 @@
 //   records  : n x W u64 bit_pack records, grouped by 4^3 (3D) or 8^2 (2D)
 //              cell block; inside a block slot-major (the first record of
 //              every cell in cell order, then the second of every cell, ...),
-//              so that the 32 lanes of a warp hold particles of 32 different
-//              cells except where a slot has fewer than 32 cells; each
-//              block's sequence is cut into chunks of <= CH (work items).
-//              A particle-id array moves with the records.
-//   grids    : two dense grids of R4 nodes, row-major; one receives P2G
-//              sums (m, m v), the other holds grid_op output (m, v).
-//   binning  : per-cell counts/offsets, per-particle key and rank, and work
-//              items (block, first record, count <= CH).
+//              so that 32 consecutive records lie in 32 different cells
+//              except where a slot has fewer than 32 cells.  A particle-id
+//              array moves with the records.
+//   grids    : two dense grids of R4 nodes (m, m v), row-major: one holds
+//              the P2G sums of substep k (grid_op is applied as tiles are
+//              staged from it), the other receives the P2G of substep k+1
+//              (cleared by the host before the launch).
+//   binning  : per-cell counts/offsets, per-particle key and rank, and one
+//              work item per occupied block (block, first record, count).
 //
-// k_step, one CTA of CH = 128 threads per work item (persistent loop):
-//   1. thread t loads record t of the item into shared memory (odd word
-//      stride: conflict-free) and stages the block's grid tile (G2P source);
-//   2. G2P of substep k: gather 3^d nodes, new v, C, x, F|J;
-//      bit_pack_assign into the shared record, which also yields the values
-//      a later decode returns; records written back to HBM;
-//   3. P2G of substep k+1 from those values into a per-warp private tile
-//      of float4 nodes with plain shared-memory adds (lanes that share a
-//      cell take turns, found with __match_any_sync), then the 8 warp tiles
-//      are summed (and re-zeroed) and flushed with one red.global.add.v4.f32
-//      per touched node.
-// Either phase may be off (first / last substep of a run).
+// k_step, persistent CTAs of CH = 128 threads claiming work items (whole
+// cell blocks) from a counter:
+//   1. stage the block's grid tile in shared memory, applying grid_op to
+//      every node (G2P source);
+//   2. the 4 warps take the block's records 32 at a time (units), without
+//      CTA barriers between units; per unit each lane loads its record into
+//      its shared slot and
+//      a. G2P of substep k: gather 3^d nodes (z-separable sums), new v, C,
+//         x, F|J; bit_pack_assign into the shared record, which also yields
+//         the values a later decode returns; record written back to HBM;
+//      b. P2G of substep k+1 from those values into the warp's private tile
+//         of float4 nodes with plain shared-memory read-add-writes, offset
+//         by offset with __syncwarp ordering (lanes that share a base cell
+//         take turns, found with __match_any_sync);
+//   3. the warp tiles are summed (and re-zeroed) over the box of touched
+//      nodes and flushed with one red.global.add.v4.f32 per node.
+// G2P or P2G may be off (first / last substep of a run).
 #pragma once
 
 #include "aq_codec.cuh"
