@@ -96,6 +96,15 @@ struct SimK {
   R clip_lo[3], clip_hi[3];
   int mat_kind[AQ_MAX_MATERIALS];
   R mu[AQ_MAX_MATERIALS], lam[AQ_MAX_MATERIALS];
+  // SDF collider (3D; col_on = 0: none): signed distance and normal volumes
+  // (float, col_dims, placed at grid index col_off), rotation centre at
+  // (col_n, ., col_n), rotated indices clamped to [col_lo, col_hi]
+  int col_on, col_n, col_dims[3], col_off[3], col_lo[3], col_hi[3];
+  const float* col_sdf;
+  const float* col_nrm;
+  R col_omega;
+  R col_c, col_s;  // cos and sin of the collider angle this launch
+  int col_yshift;  // collider height in cells this launch, int(height / dx + 0.5)
 };
 
 struct StepArgs {
@@ -181,7 +190,52 @@ __device__ __forceinline__ void atomic_min_d(double* a, double v) {
 
 // grid_op (mpm_solver.py:633-665) of one node (m, m v) at grid index I:
 // velocity, gravity, optional friction on the floor, sticky walls.
-template <int D, class R, class R4>
+__device__ __forceinline__ float mul_rn(float a, float b) { return __fmul_rn(a, b); }
+__device__ __forceinline__ double mul_rn(double a, double b) { return __dmul_rn(a, b); }
+__device__ __forceinline__ float add_rn(float a, float b) { return __fadd_rn(a, b); }
+__device__ __forceinline__ double add_rn(double a, double b) { return __dadd_rn(a, b); }
+__device__ __forceinline__ float sub_rn(float a, float b) { return __fsub_rn(a, b); }
+__device__ __forceinline__ double sub_rn(double a, double b) { return __dsub_rn(a, b); }
+
+// Grid post-process of the rotating SDF collider (sdf_collision and
+// rot_scene, mpm_solver.py:1459-1480,1515-1540): the node's index is rotated
+// by -theta about (n, ., n) and lowered by the collider height; where the
+// signed distance there is below -1e-5 the velocity relative to the
+// collider (omega x r, r = (rotated index - (n, I1, n)) dx) loses its
+// component into the surface along the rotated normal.
+template <class R>
+__device__ __forceinline__ void collide_node(const SimK<R>& K, int I0, int I1, int I2, R (&v)[3]) {
+  const int n = K.col_n;
+  const int i0 = I0 >= 2 * n ? I0 - 2 * n : I0, i2 = I2 >= 2 * n ? I2 - 2 * n : I2;
+  const R c = K.col_c, s = K.col_s;
+  const R o0 = (R)(i0 - n), o2 = (R)(i2 - n);
+  // each operation rounded on its own (no FMA contraction), so that the
+  // truncation to an index matches a plain CPU evaluation
+  const R x = add_rn(add_rn(sub_rn(mul_rn(c, o0), mul_rn(s, o2)), (R)n), (R)0.5);
+  const R z = add_rn(add_rn(add_rn(mul_rn(s, o0), mul_rn(c, o2)), (R)n), (R)0.5);
+  int r[3] = {(int)x, I1 - K.col_yshift, (int)z};
+#pragma unroll
+  for (int k = 0; k < 3; ++k) r[k] = max(min(r[k], K.col_hi[k]), K.col_lo[k]);
+  const int a = r[0] - K.col_off[0], b = r[1] - K.col_off[1], e = r[2] - K.col_off[2];
+  if (a < 0 || a >= K.col_dims[0] || b < 0 || b >= K.col_dims[1] || e < 0 || e >= K.col_dims[2]) return;
+  const int64_t q = ((int64_t)a * K.col_dims[1] + b) * K.col_dims[2] + e;
+  if (!(K.col_sdf[q] < -1e-5f)) return;
+  const R g0 = (R)K.col_nrm[3 * q], g1 = (R)K.col_nrm[3 * q + 1], g2 = (R)K.col_nrm[3 * q + 2];
+  const R nrm[3] = {c * g0 + s * g2, g1, -s * g0 + c * g2};
+  const R rx = (R)(r[0] - n) * K.dx, rz = (R)(r[2] - n) * K.dx;
+  const R cv[3] = {K.col_omega * rz, (R)0, -K.col_omega * rx};
+  R vr[3], dn = 0;
+#pragma unroll
+  for (int k = 0; k < 3; ++k) {
+    vr[k] = v[k] - cv[k];
+    dn += vr[k] * nrm[k];
+  }
+  dn = dn < (R)0 ? dn : (R)0;
+#pragma unroll
+  for (int k = 0; k < 3; ++k) v[k] = cv[k] + (vr[k] - dn * nrm[k]);
+}
+
+template <int D, class R, bool COL, class R4>
 __device__ __forceinline__ R4 grid_op_node(const SimK<R>& K, R4 g, int I0, int I1, int I2) {
   const int I[3] = {I0, I1, I2};
   const R inv_m = (R)1 / (g.x + (R)1e-10);
@@ -197,6 +251,7 @@ __device__ __forceinline__ R4 grid_op_node(const SimK<R>& K, R4 g, int I0, int I
     if (I[k] < K.lb[k] && v[k] < (R)0) v[k] = 0;
     if (I[k] > K.ub[k] && v[k] > (R)0) v[k] = 0;
   }
+  if (COL && D == 3 && K.col_on) collide_node<R>(K, I0, I1, I2, v);
   g.y = v[0];
   g.z = v[1];
   g.w = v[2];
@@ -306,7 +361,9 @@ __device__ __forceinline__ void bspline(const R* x, const SimK<R>& K, int* base,
 
 // ------------------------------------------------------------ the step
 
-template <int D, bool HF, bool HM, class R, class LA>
+// COL: compiled with the SDF collider (the library's own build always is;
+// the layout-specialized build only when a collider is set).
+template <int D, bool HF, bool HM, class R, class LA, bool COL = true>
 __global__ void __launch_bounds__(CH, AQ_STEP_MIN_BLOCKS) k_step(const __grid_constant__ aq_layout Lp, const SimK<R> K,
                                                 const StepArgs A) {
   typedef Sch<D, HF, HM> S;
@@ -381,7 +438,7 @@ __global__ void __launch_bounds__(CH, AQ_STEP_MIN_BLOCKS) k_step(const __grid_co
         R4 g = zero4;
         if (ok) {
           g = gin[cell_index<D>(K.res, g0, g1, g2)];
-          if (A.raw_in) g = grid_op_node<D, R>(K, g, g0, g1, g2);
+          if (A.raw_in) g = grid_op_node<D, R, COL>(K, g, g0, g1, g2);
         }
         gtile[j] = g;
       }
@@ -472,7 +529,7 @@ __global__ void __launch_bounds__(CH, AQ_STEP_MIN_BLOCKS) k_step(const __grid_co
                 } else {
                   const int n0 = base[0] + a, n1 = base[1] + b, n2 = D == 3 ? base[2] + c : 0;
                   g = gin[cell_index<D>(K.res, n0, n1, n2)];
-                  if (A.raw_in) g = grid_op_node<D, R>(K, g, n0, n1, n2);
+                  if (A.raw_in) g = grid_op_node<D, R, COL>(K, g, n0, n1, n2);
                 }
                 const R gv[3] = {g.y, g.z, g.w};
                 const int off[3] = {a, b, c};

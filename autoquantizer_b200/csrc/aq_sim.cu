@@ -291,6 +291,8 @@ struct SimBase {
   virtual int loss(double* h, cudaStream_t st) = 0;
   virtual int sort(cudaStream_t st) = 0;
   virtual size_t smem_bytes() const = 0;
+  virtual void set_collider(const aq_sim* sim) = 0;
+  virtual int setup_kernel(bool col) = 0;
 };
 
 }  // namespace aq
@@ -317,6 +319,11 @@ struct aq_sim {
   double *rmax = nullptr, *rmin = nullptr;
   double* dloss = nullptr;
   double* dstats = nullptr;  // aq_sim_field_stats accumulators
+  // SDF collider (aq_sim_set_collider): caller-owned volumes and its motion
+  int col_on = 0, col_center = 0, col_dims[3] = {0, 0, 0}, col_off[3] = {0, 0, 0};
+  const float* col_sdf = nullptr;
+  const float* col_nrm = nullptr;
+  double col_theta = 0, col_height = 0, col_omega = 0, col_rate = 0;
   void* slab = nullptr;      // the one device allocation all buffers above live in
   int ranges_on = 0;
   int64_t step = 0;
@@ -335,6 +342,9 @@ struct aq_sim {
 };
 
 namespace aq {
+
+template <int D, bool HF, bool HM, class R>
+static int setup_step_kernel(aq_sim* s, size_t smem, bool col);
 
 template <int D, bool HF, bool HM, class R>
 struct SimImpl final : SimBase {
@@ -368,6 +378,23 @@ struct SimImpl final : SimBase {
       K.mu[m] = (R)P.mat[m].mu;
       K.lam[m] = (R)P.mat[m].lam;
     }
+  }
+
+  int setup_kernel(bool col) override { return setup_step_kernel<D, HF, HM, R>(s, smem_bytes(), col); }
+
+  void set_collider(const aq_sim* c) override {
+    const aq_params& P = c->P;
+    K.col_on = c->col_on && D == 3;
+    K.col_n = c->col_center;
+    for (int k = 0; k < 3; ++k) {
+      K.col_dims[k] = c->col_dims[k];
+      K.col_off[k] = c->col_off[k];
+      K.col_lo[k] = (int)P.lb[k];
+      K.col_hi[k] = (int)P.ub[k];
+    }
+    K.col_sdf = c->col_sdf;
+    K.col_nrm = c->col_nrm;
+    K.col_omega = (R)c->col_omega;
   }
 
   size_t smem_bytes() const override {
@@ -424,6 +451,9 @@ struct SimImpl final : SimBase {
     a.do_p2g = do_p2g;
     a.ranges = S_->ranges_on;
     a.raw_in = do_g2p;  // grid_in holds the previous P2G sums; grid_op runs as the tile is staged
+    K.col_c = (R)cos(S_->col_theta);
+    K.col_s = (R)sin(S_->col_theta);
+    K.col_yshift = (int)(S_->col_height / S_->P.dx + 0.5);
     const bool prof = S_->prof_on && S_->prof_n[0] < aq_sim::PROF_CAP;
     if (prof) AQ_CUDA_TRY(cudaEventRecord(S_->prof_ev[0][2 * S_->prof_n[0]], st));
     if (S_->jit_fn) {
@@ -474,6 +504,9 @@ struct SimImpl final : SimBase {
           if ((rc = launch_step(1, 0, S_->grid[a], nullptr, st))) return rc;
         }
         ++S_->step;
+        // step_collider (mpm_solver.py:1542-1547) after every substep
+        S_->col_theta += S_->col_omega * S_->P.dt;
+        S_->col_height += S_->col_rate * S_->P.dt;
       }
       S_->since_sort += m;
       n -= m;
@@ -491,16 +524,14 @@ struct SimImpl final : SimBase {
   }
 };
 
+// Compile (NVRTC, layout as a constant; with or without the collider) or
+// select the library's own k_step, and size its persistent grid.
 template <int D, bool HF, bool HM, class R>
-static int make_impl(aq_sim* s) {
-  auto* im = new (std::nothrow) SimImpl<D, HF, HM, R>(s);
-  if (!im) return AQ_E_NOMEM;
-  s->impl = im;
-  const size_t smem = im->smem_bytes();
-  if (smem > 227 * 1024) return AQ_E_LIMIT;
+static int setup_step_kernel(aq_sim* s, size_t smem, bool col) {
   int occ = 0;
+  s->jit_fn = nullptr;
   if (s->P.jit) {
-    s->jit_fn = jit_k_step(D, HF, HM, sizeof(R) == 8, s->L, &s->jit_error);
+    s->jit_fn = jit_k_step(D, HF, HM, sizeof(R) == 8, col, s->L, &s->jit_error);
     if (s->jit_fn && (jit_set_smem(s->jit_fn, (int)smem) != AQ_OK || jit_occupancy(s->jit_fn, CH, smem, &occ) != AQ_OK)) {
       s->jit_fn = nullptr;
       s->jit_error = "cuFuncSetAttribute/occupancy failed";
@@ -514,6 +545,16 @@ static int make_impl(aq_sim* s) {
   if (occ < 1) occ = 1;
   s->step_grid = occ * num_sms();
   return AQ_OK;
+}
+
+template <int D, bool HF, bool HM, class R>
+static int make_impl(aq_sim* s) {
+  auto* im = new (std::nothrow) SimImpl<D, HF, HM, R>(s);
+  if (!im) return AQ_E_NOMEM;
+  s->impl = im;
+  const size_t smem = im->smem_bytes();
+  if (smem > 227 * 1024) return AQ_E_LIMIT;
+  return setup_step_kernel<D, HF, HM, R>(s, smem, false);
 }
 
 template <int D, class R>
@@ -689,6 +730,42 @@ int aq_sim_get_state(aq_sim* s, void* values, int32_t values_f64, void* stream) 
                                                             s->n);
   AQ_CUDA_TRY(cudaGetLastError());
   s->launches += 1;
+  return AQ_OK;
+}
+
+int aq_sim_set_collider(aq_sim* s, const float* d_sdf, const float* d_normal, const int32_t* dims,
+                        const int32_t* offset, int32_t center, double theta, double height, double omega,
+                        double height_rate) {
+  if (!s) return AQ_E_ARG;
+  if (!d_sdf) {
+    s->col_on = 0;
+  } else {
+    if (s->D != 3 || !d_normal || !dims || !offset) return AQ_E_ARG;
+    for (int k = 0; k < 3; ++k)
+      if (dims[k] < 1) return AQ_E_ARG;
+    s->col_on = 1;
+    s->col_center = center;
+    s->col_sdf = d_sdf;
+    s->col_nrm = d_normal;
+    for (int k = 0; k < 3; ++k) {
+      s->col_dims[k] = dims[k];
+      s->col_off[k] = offset[k];
+    }
+  }
+  s->col_theta = theta;
+  s->col_height = height;
+  s->col_omega = omega;
+  s->col_rate = height_rate;
+  s->impl->set_collider(s);
+  // the layout-specialized kernel is built with the collider only when one is set
+  if (s->P.jit) return s->impl->setup_kernel(s->col_on != 0);
+  return AQ_OK;
+}
+
+int aq_sim_collider_get(aq_sim* s, double* h_theta, double* h_height) {
+  if (!s || !h_theta || !h_height) return AQ_E_ARG;
+  *h_theta = s->col_theta;
+  *h_height = s->col_height;
   return AQ_OK;
 }
 

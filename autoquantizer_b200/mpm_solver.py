@@ -80,6 +80,7 @@ class MPMSolver:
         self._dirty = True
         self._layout = None
         self.materials = p.materials
+        self._col = None  # SDF collider: (sdf, normal) CUDA tensors, offset, motion state
         self.initialize()
 
     # ------------------------------------------------------------ layout
@@ -209,6 +210,10 @@ class MPMSolver:
 
     def _drop_sim(self):
         if self._sim is not None:
+            if self._col is not None:  # carry the collider's angle and height over
+                th, hh = C.c_double(), C.c_double()
+                _lib.lib().aq_sim_collider_get(self._sim, C.byref(th), C.byref(hh))
+                self._col["theta"], self._col["height"] = th.value, hh.value
             _lib.lib().aq_sim_destroy(self._sim)
             self._sim = None
         self._dirty = True
@@ -280,6 +285,8 @@ class MPMSolver:
             _lib.check(_lib.lib().aq_sim_create(C.byref(self._params()), C.byref(self.layout()), C.byref(sim)),
                        "aq_sim_create")
             self._sim = sim
+            if self._col is not None:
+                self._apply_collider()
         if self._dev is not None and self._host is None:
             vals = self._dev
             if vals.dtype not in (torch.float32, torch.float64):
@@ -411,6 +418,52 @@ class MPMSolver:
         _lib.check(_lib.lib().aq_sim_launches(self._sim, C.byref(n)), "aq_sim_launches")
         return n.value
 
+    # ------------------------------------------------------ SDF collider
+
+    def init_sdf_value(self, sdf, normal, offset=None, theta=0.0, height=0.0, omega=5.0, height_rate=0.1):
+        """The rotating SDF collider (init_sdf_collider / init_sdf_value,
+        mpm_solver.py:284-318): sdf [a, b, c] signed distances and normal
+        [a, b, c, 3] (e.g. the reference's inputs/propeller_*.npz, array
+        'sdf'), placed at grid index offset (default the solver's
+        sdf_offset, zero).  After every substep the angle advances by
+        omega dt and the height by height_rate dt (step_collider,
+        :1542-1547).  3D only."""
+        import torch
+
+        if self.dim != 3:
+            raise ValueError("the SDF collider is 3D")
+        sdf = np.asarray(sdf)
+        normal = np.asarray(normal)
+        if sdf.ndim != 3 or normal.shape != sdf.shape + (3,):
+            raise ValueError("sdf must be [a, b, c] and normal [a, b, c, 3]")
+        self._col = {
+            "sdf": torch.from_numpy(np.ascontiguousarray(sdf, dtype=np.float32)).cuda(),
+            "normal": torch.from_numpy(np.ascontiguousarray(normal, dtype=np.float32)).cuda(),
+            "offset": [int(o) for o in (offset if offset is not None else [0, 0, 0])],
+            "theta": float(theta), "height": float(height), "omega": float(omega), "rate": float(height_rate),
+        }
+        if self._sim is not None:
+            self._apply_collider()
+
+    def _apply_collider(self):
+        c = self._col
+        dims = (C.c_int32 * 3)(*c["sdf"].shape)
+        off = (C.c_int32 * 3)(*c["offset"])
+        _lib.check(_lib.lib().aq_sim_set_collider(self._sim, C.c_void_p(c["sdf"].data_ptr()),
+                                                  C.c_void_p(c["normal"].data_ptr()), dims, off, int(self.n_grid),
+                                                  c["theta"], c["height"], c["omega"], c["rate"]),
+                   "aq_sim_set_collider")
+
+    def collider_state(self):
+        """(angle, height) of the collider now."""
+        if self._col is None:
+            return None
+        if self._sim is None:
+            return self._col["theta"], self._col["height"]
+        th, hh = C.c_double(), C.c_double()
+        _lib.check(_lib.lib().aq_sim_collider_get(self._sim, C.byref(th), C.byref(hh)), "aq_sim_collider_get")
+        return th.value, hh.value
+
     # ------------------------------------------------- scheme parameters
 
     def reshape_params(self, ranges):
@@ -452,6 +505,8 @@ class MPMSolver:
 
         from .adjoint import Adjoint, ek_loss, ek_seed
 
+        if self._col is not None:
+            raise NotImplementedError("the adjoint has no SDF collider (sdf_collision_no_arg.grad)")
         if self.has_mat:
             raise ValueError("the adjoint runs single-material scenes")
         self._pull()

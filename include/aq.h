@@ -206,6 +206,23 @@ int aq_sim_loss(aq_sim* sim, int32_t kind, double* h_out, void* stream);
  * Synchronizes the stream. */
 int aq_sim_field_stats(aq_sim* sim, const void* d_ref, int32_t ref_f64, double* h_out, void* stream);
 
+/* Rotating SDF collider of the 3D experiments (init_sdf_collider,
+ * init_sdf_value, sdf_collision, rot_scene, step_collider:
+ * mpm_solver.py:284-318,1444-1547), applied to the grid velocities after
+ * grid_op.  d_sdf: signed distances (float, dims[0] x dims[1] x dims[2],
+ * row-major), d_normal: their normals (float x 3), both placed at grid index
+ * offset[] and owned by the caller, who keeps them alive while the
+ * simulator runs.  The grid index is rotated by -theta about (center, .,
+ * center) and lowered by height/dx before the lookup; after every substep
+ * theta += omega dt and height += height_rate dt (the reference's
+ * step_collider: omega 5, rate 0.1).  d_sdf null switches the collider off.
+ * 3D simulators only. */
+int aq_sim_set_collider(aq_sim* sim, const float* d_sdf, const float* d_normal, const int32_t* dims,
+                        const int32_t* offset, int32_t center, double theta, double height, double omega,
+                        double height_rate);
+/* Current collider angle and height. */
+int aq_sim_collider_get(aq_sim* sim, double* h_theta, double* h_height);
+
 /* Per-slot running max/min of the state (range detection), accumulated on
  * the device after every substep once enabled.
  * Replaces update_limits_* / get_limits (mpm_solver.py:944-997). */

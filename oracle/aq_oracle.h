@@ -43,6 +43,13 @@ typedef struct or_params {
   double mat_mu[4], mat_lam[4];
   uint64_t seed;
   int threads; /* OpenMP threads for the timed baseline; <=1 = serial, deterministic */
+  /* rotating SDF collider (mpm_solver.py:1459-1547), 3D; col_on = 0: none.
+   * col_c, col_s: cos and sin of this substep's angle (float in the f32
+   * simulator), col_yshift = int(height / dx + 0.5) */
+  int col_on, col_n, col_dims[3], col_off[3], col_yshift;
+  double col_c, col_s, col_omega;
+  const float* col_sdf;
+  const float* col_nrm;
 } or_params;
 
 #endif

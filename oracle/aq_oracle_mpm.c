@@ -145,6 +145,39 @@ static int SUF(base_of)(R xv, R inv_dx, int res, int* flags) {
 /* One substep over n records.  grid: ncells*4 REAL scratch.  ranges_max/min
  * (optional, n_slots each) accumulate the decoded new state.  Returns the
  * status flags (1 = out of domain, 2 = NaN). */
+/* grid post-process of the rotating SDF collider: rot_scene
+ * (mpm_solver.py:1515-1540) then sdf_collision (:1459-1480) */
+static void SUF(collide)(const or_params* P, const int* I, R* v) {
+  const int n = P->col_n;
+  const int i0 = I[0] >= 2 * n ? I[0] - 2 * n : I[0], i2 = I[2] >= 2 * n ? I[2] - 2 * n : I[2];
+  const R c = (R)P->col_c, s = (R)P->col_s;
+  const R o0 = (R)(i0 - n), o2 = (R)(i2 - n);
+  const R x = c * o0 - s * o2 + (R)n + (R)0.5;
+  const R z = s * o0 + c * o2 + (R)n + (R)0.5;
+  int r[3] = {(int)x, I[1] - P->col_yshift, (int)z};
+  for (int k = 0; k < 3; ++k) {
+    const int lo = (int)P->lb[k], hi = (int)P->ub[k];
+    r[k] = r[k] > hi ? hi : r[k];
+    r[k] = r[k] < lo ? lo : r[k];
+  }
+  const int a = r[0] - P->col_off[0], b = r[1] - P->col_off[1], e = r[2] - P->col_off[2];
+  if (a < 0 || a >= P->col_dims[0] || b < 0 || b >= P->col_dims[1] || e < 0 || e >= P->col_dims[2]) return;
+  const int64_t q = ((int64_t)a * P->col_dims[1] + b) * P->col_dims[2] + e;
+  if (!(P->col_sdf[q] < -1e-5f)) return; /* sdf(): the value where below -1e-5, else 1 */
+  const R g0 = (R)P->col_nrm[3 * q], g1 = (R)P->col_nrm[3 * q + 1], g2 = (R)P->col_nrm[3 * q + 2];
+  const R nrm[3] = {c * g0 + s * g2, g1, -s * g0 + c * g2};
+  const R dx = (R)P->dx, om = (R)P->col_omega;
+  const R rx = (R)(r[0] - n) * dx, rz = (R)(r[2] - n) * dx;
+  const R cv[3] = {om * rz, (R)0, -om * rx}; /* (0, omega, 0) x r */
+  R vr[3], dn = 0;
+  for (int k = 0; k < 3; ++k) {
+    vr[k] = v[k] - cv[k];
+    dn += vr[k] * nrm[k];
+  }
+  dn = dn < (R)0 ? dn : (R)0;
+  for (int k = 0; k < 3; ++k) v[k] = cv[k] + (vr[k] - dn * nrm[k]);
+}
+
 int SUF(or_substep)(const or_params* P, const or_layout* L, uint64_t* words, const int32_t* pid,
                     int64_t n, int64_t step, R* grid, double* vals_scratch, double* rmax,
                     double* rmin) {
@@ -225,6 +258,7 @@ int SUF(or_substep)(const or_params* P, const or_layout* L, uint64_t* words, con
       if (I[k] < P->lb[k] && vo[k] < 0) vo[k] = 0;
       if (I[k] > P->ub[k] && vo[k] > 0) vo[k] = 0;
     }
+    if (D == 3 && P->col_on) SUF(collide)(P, I, vo);
     for (int d = 0; d < D; ++d) gc[1 + d] = vo[d];
   }
 

@@ -10,6 +10,7 @@ offset) with kind codes FIXED=0, INT=1, FLOAT_EXP=2, SHARED_EXP=3,
 RAW_F32=4, RAW_F64=5, so this module does not depend on the product package.
 """
 import ctypes as C
+import math
 import os
 import sys
 
@@ -42,6 +43,9 @@ class OrParams(C.Structure):
         ("g", C.c_double), ("lb", C.c_double * 3), ("ub", C.c_double * 3),
         ("mat_kind", C.c_int * 4), ("mat_mu", C.c_double * 4), ("mat_lam", C.c_double * 4),
         ("seed", C.c_uint64), ("threads", C.c_int),
+        ("col_on", C.c_int), ("col_n", C.c_int), ("col_dims", C.c_int * 3), ("col_off", C.c_int * 3),
+        ("col_yshift", C.c_int), ("col_c", C.c_double), ("col_s", C.c_double), ("col_omega", C.c_double),
+        ("col_sdf", C.c_void_p), ("col_nrm", C.c_void_p),
     ]
 
 
@@ -168,17 +172,46 @@ class Sim:
     def get_state(self):
         return decode(self.L, self.words)
 
+    def set_collider(self, sdf, normal, offset, center, theta=0.0, height=0.0, omega=5.0, height_rate=0.1):
+        """The rotating SDF collider (float32 volumes sdf [a,b,c], normal
+        [a,b,c,3] placed at grid index offset); angle and height advance by
+        omega dt and height_rate dt after every substep."""
+        self._col = (np.ascontiguousarray(sdf, dtype=np.float32), np.ascontiguousarray(normal, dtype=np.float32))
+        self.P.col_on = 1
+        self.P.col_n = int(center)
+        for k in range(3):
+            self.P.col_dims[k] = self._col[0].shape[k]
+            self.P.col_off[k] = int(offset[k])
+        self.P.col_sdf = self._col[0].ctypes.data
+        self.P.col_nrm = self._col[1].ctypes.data
+        self.P.col_omega = float(omega)
+        self.col_theta, self.col_height, self.col_rate = float(theta), float(height), float(height_rate)
+
+    def _collider_step_values(self):
+        if not getattr(self.P, "col_on", 0):
+            return
+        self.P.col_c = math.cos(self.col_theta)
+        self.P.col_s = math.sin(self.col_theta)
+        if not self.P.precision:  # the f32 simulator carries them as float
+            self.P.col_c = float(np.float32(self.P.col_c))
+            self.P.col_s = float(np.float32(self.P.col_s))
+        self.P.col_yshift = int(self.col_height / self.P.dx + 0.5)
+
     def substeps(self, k, ranges=False):
         f = lib().or_substep_f64 if self.P.precision else lib().or_substep_f32
         n = self.words.shape[0]
         scratch = np.zeros(n * self.L.n, dtype=np.float64)
         for _ in range(k):
+            self._collider_step_values()
             self.flags |= f(C.byref(self.P), C.byref(self.L), _ptr(self.words, C.c_uint64),
                             self.pid.ctypes.data, n, self.step, self.grid.ctypes.data,
                             _ptr(scratch, C.c_double),
                             self.rmax.ctypes.data if ranges else None,
                             self.rmin.ctypes.data if ranges else None)
             self.step += 1
+            if self.P.col_on:
+                self.col_theta += self.P.col_omega * self.P.dt
+                self.col_height += self.col_rate * self.P.dt
 
     def loss(self):
         f = lib().or_loss_ek_f64 if self.P.precision else lib().or_loss_ek_f32

@@ -375,3 +375,37 @@ def test_raw_fields_roundtrip():
     vals = np.array([[np.float32(1.1), 1.1, 0.25]])
     out = O.decode(L, O.encode(L, vals))
     assert out[0, 0] == np.float32(1.1) and out[0, 1] == 1.1 and out[0, 2] == 0.25
+
+
+# ------------------------------------------------------ SDF collider (oracle)
+
+def test_oracle_collider_holds_a_block_on_a_static_slab():
+    """sdf_collision with omega 0: grid velocities into a slab (normal up)
+    are removed, so a block resting on it stops falling, while the same
+    block without the collider keeps falling."""
+    import oracle as Orc
+
+    n = 2000
+    rng = np.random.default_rng(0)
+    x = np.column_stack([0.45 + 0.1 * rng.random(n), 0.40 + 0.1 * rng.random(n), 0.45 + 0.1 * rng.random(n)])
+    vals = np.zeros((n, 24))
+    vals[:, :3] = x
+    vals[:, 15] = vals[:, 19] = vals[:, 23] = 1.0
+    P = {"dim": 3, "precision": 0, "res": [32, 32, 32], "lb": [3, 3, 3], "ub": [29, 29, 29], "has_F": 1,
+         "has_mat": 0, "materials": [(1, 50.0, 50.0)], "use_friction": 0, "use_bound_clip": 0,
+         "dx": 1 / 32, "dt": 1e-4, "p_vol": (0.5 / 32) ** 3, "p_mass": (0.5 / 32) ** 3, "gravity": 9.8, "seed": 0}
+    L = Orc.build_layout([(4, 32, 1, 0, 0, 0.0, 0.0)] * 24, False, False)  # raw f32 slots
+    sdf = np.full((32, 32, 32), 0.02, dtype=np.float32)
+    sdf[:, 10:13, :] = -0.01  # slab under the block (block bottom at y = 0.40 -> node 12.8)
+    nrm = np.zeros((32, 32, 32, 3), dtype=np.float32)
+    nrm[..., 1] = 1.0
+    ys = []
+    for col in (False, True):
+        o = Orc.Sim(P, L)
+        o.set_state(vals)
+        if col:
+            o.set_collider(sdf, nrm, offset=(0, 0, 0), center=16, omega=0.0, height_rate=0.0)
+        o.substeps(1000)
+        ys.append(o.get_state()[:, 1].min())
+    assert ys[0] < 0.40 - 0.04  # free fall over 0.1 s: 0.5 g t^2 = 0.049
+    assert ys[1] > 0.375 - 0.01  # held at the slab's top (node 13 = 0.406, stencil reach one cell)
