@@ -209,6 +209,13 @@ __global__ void k_iota(int32_t* p, int64_t n) {
   if (i < n) p[i] = (int32_t)i;
 }
 
+// Node masses (component 0 of the row-major m, m v grid) as float.
+template <class R4>
+__global__ void k_grid_mass(const R4* __restrict__ g, float* __restrict__ out, int64_t n) {
+  for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x)
+    out[i] = (float)g[i].x;
+}
+
 template <int D, class R>
 __global__ void __launch_bounds__(256) k_loss(const __grid_constant__ aq_layout L, const SimK<R> K,
                                               const uint64_t* __restrict__ words, int64_t n, double* out) {
@@ -327,6 +334,7 @@ struct aq_sim {
   void* slab = nullptr;      // the one device allocation all buffers above live in
   int ranges_on = 0;
   int64_t step = 0;
+  int last_grid = 0;  // grid[] holding the P2G sums of the latest substep
   int since_sort = 0;
   bool sorted = false;
   int64_t launches = 0;
@@ -502,6 +510,7 @@ struct SimImpl final : SimBase {
           a = b;
         } else {
           if ((rc = launch_step(1, 0, S_->grid[a], nullptr, st))) return rc;
+          S_->last_grid = a;
         }
         ++S_->step;
         // step_collider (mpm_solver.py:1542-1547) after every substep
@@ -811,6 +820,19 @@ int aq_sim_substeps(aq_sim* s, int32_t n, void* stream) {
   if (!s || n < 0) return AQ_E_ARG;
   if (n == 0) return AQ_OK;
   return s->impl->substeps(n, as_stream(stream));
+}
+
+int aq_sim_grid_mass(aq_sim* s, float* d_out, void* stream) {
+  if (!s || !d_out) return AQ_E_ARG;
+  cudaStream_t st = as_stream(stream);
+  const unsigned nb = (unsigned)std::min<int64_t>(grid_for(s->ncell, 256), (int64_t)num_sms() * 8);
+  if (s->P.precision)
+    k_grid_mass<<<nb, 256, 0, st>>>((const double4*)s->grid[s->last_grid], d_out, s->ncell);
+  else
+    k_grid_mass<<<nb, 256, 0, st>>>((const float4*)s->grid[s->last_grid], d_out, s->ncell);
+  AQ_CUDA_TRY(cudaGetLastError());
+  s->launches += 1;
+  return AQ_OK;
 }
 
 int aq_sim_loss(aq_sim* s, int32_t kind, double* h_out, void* stream) {

@@ -9,6 +9,7 @@ this module only builds the record layout and moves buffers.  PyTorch is used
 for device buffers and the current stream.
 """
 import ctypes as C
+import os
 
 import numpy as np
 
@@ -81,6 +82,7 @@ class MPMSolver:
         self._layout = None
         self.materials = p.materials
         self._col = None  # SDF collider: (sdf, normal) CUDA tensors, offset, motion state
+        self._vox = None  # mesh voxelizer of add_mesh, made on first use
         self.initialize()
 
     # ------------------------------------------------------------ layout
@@ -224,34 +226,163 @@ class MPMSolver:
             self._staging()[: self.current_idx] = self.state_values()
             self._dev = None
 
-    def add_cube(self, low_corner, box_size, num, material=0):
-        """3D: uniform random positions (fill_in_box, :1573-1590); 2D: the
-        deterministic lattice of fill_in_box_2duniform (:1561-1571)."""
+    def _rng(self, tag):
+        return np.random.default_rng((int(self.param.seed), self.current_idx, tag))
+
+    def _append(self, x, v=None, material=0, what="add"):
+        """New particles at current_idx: positions x (cnt x dim), velocity v
+        (a dim vector or cnt x dim, default 0), F = I or J = 1, C = 0."""
+        x = np.asarray(x, dtype=np.float64).reshape(-1, self.dim)
+        st, cnt = self.current_idx, len(x)
+        if st + cnt > self.n_particles:
+            raise ValueError("%s: %d particles exceed n_particles=%d" % (what, st + cnt, self.n_particles))
         self._pull()
-        self._staging()
+        h = self._staging()
         self._dev = None
+        a, b = self.slot_range("x")
+        h[st:st + cnt, a:b] = x
+        va, vb = self.slot_range("v")
+        h[st:st + cnt, va:vb] = 0.0 if v is None else np.broadcast_to(np.asarray(v, dtype=np.float64), (cnt, self.dim))
+        ca, cb = self.slot_range("C")
+        h[st:st + cnt, ca:cb] = 0.0
+        fa, fb = self.slot_range("F" if self.has_F else "J")
+        h[st:st + cnt, fa:fb] = np.eye(self.dim).ravel() if self.has_F else 1.0
+        if self.has_mat:
+            h[st:st + cnt, self.slot_range("mat")[0]] = material
+        self.current_idx = st + cnt
+        self._drop_sim()
+        return cnt
+
+    def add_cube(self, low_corner, box_size, num, material=0):
+        """3D: uniform random positions (fill_in_box, :1573-1590), pushed out
+        of the SDF collider when one is set; 2D: the deterministic lattice of
+        fill_in_box_2duniform (:1561-1571)."""
         d = self.dim
-        st = self.current_idx
         if d == 3 or len(low_corner) == 3:
-            rng = np.random.default_rng((int(self.param.seed), st))
+            rng = self._rng(0)
             x = np.asarray(low_corner)[None, :] + rng.random((num, d)) * np.asarray(box_size)[None, :]
-            cnt = num
+            if self._col is not None:
+                x = self._push_out_of_collider(x, rng)
         else:
             n = int(np.sqrt(num))
             i, j = np.meshgrid(np.arange(n), np.arange(n), indexing="ij")
             x = np.stack([low_corner[0] + 1.0 / n * j.ravel() * box_size[0],
                           low_corner[1] + 1.0 / n * i.ravel() * box_size[1]], axis=1)
-            cnt = n * n
-        if st + cnt > self.n_particles:
-            raise ValueError("add_cube: %d particles exceed n_particles=%d" % (st + cnt, self.n_particles))
-        a, b = self.slot_range("x")
-        self._host[st:st + cnt, a:b] = x
-        va, vb = self.slot_range("v")
-        self._host[st:st + cnt, va:vb] = 0.0
-        if self.has_mat:
-            self._host[st:st + cnt, self.slot_range("mat")[0]] = material
-        self.current_idx = st + cnt
-        self._drop_sim()
+        self._append(x, None, material, "add_cube")
+
+    def _push_out_of_collider(self, x, rng):
+        """fill_in_box with the collider (mpm_solver.py:1582-1588): a particle
+        whose cell int(x / dx + 0.5), rotated into the collider's frame
+        (rot_scene, :1518-1540), lies inside (sdf < -1e-5) moves along the
+        stored normal by (2 + 3 u) dx."""
+        c = self._col
+        theta, height = self.collider_state()
+        sdf, nrm = c["sdf"].cpu().numpy(), c["normal"].cpu().numpy()
+        n = int(self.n_grid)
+        base = (x / self.dx + 0.5).astype(np.int64)
+        i0 = np.where(base[:, 0] >= 2 * n, base[:, 0] - 2 * n, base[:, 0])
+        i2 = np.where(base[:, 2] >= 2 * n, base[:, 2] - 2 * n, base[:, 2])
+        cs, sn = np.cos(-theta), np.sin(-theta)
+        o0, o2 = (i0 - n).astype(np.float64), (i2 - n).astype(np.float64)
+        r = np.stack([(cs * o0 + sn * o2 + n + 0.5).astype(np.int64), base[:, 1] - int(height / self.dx + 0.5),
+                      (-sn * o0 + cs * o2 + n + 0.5).astype(np.int64)], axis=1)
+        r = np.clip(r, np.asarray(self.lb, dtype=np.int64), np.asarray(self.ub, dtype=np.int64))
+        q = r - np.asarray(c["offset"])
+        ok = np.all((q >= 0) & (q < np.asarray(sdf.shape)), axis=1)
+        inside = np.zeros(len(x), dtype=bool)
+        inside[ok] = sdf[q[ok, 0], q[ok, 1], q[ok, 2]] < -1e-5
+        u = rng.random(len(x))
+        x = x.copy()
+        g = nrm[q[inside, 0], q[inside, 1], q[inside, 2]]
+        x[inside] += g * ((u[inside] * 3 + 2) * self.dx)[:, None]
+        return x
+
+    def add_ball(self, center, radius, num, material=0):
+        """fill_in_ball (mpm_solver.py:1592-1598, 1620-1627): uniform points
+        in the ball by rejection, at rest.  As in the reference, nothing is
+        added unless current_idx + num < n_particles."""
+        if self.current_idx + num >= self.n_particles:
+            return 0
+        rng = self._rng(1)
+        pts = np.empty((0, self.dim))
+        while len(pts) < num:
+            p = rng.random((2 * num + 16, self.dim)) * 2 - 1
+            pts = np.concatenate([pts, p[(p * p).sum(1) <= 1]])
+        return self._append(np.asarray(center)[None, :] + pts[:num] * radius, None, material, "add_ball")
+
+    def emit_water(self, center, radius, velocity, num, material=0):
+        """fill_in_ball_with_vel (mpm_solver.py:1600-1618, 1629-1632): points
+        at angle 2 pi u1 and distance radius u2 from the centre in the xy
+        plane, all moving with velocity; nothing is added unless
+        current_idx + num < n_particles."""
+        if self.current_idx + num >= self.n_particles:
+            return 0
+        rng = self._rng(2)
+        th, r = rng.random(num) * np.pi * 2.0, rng.random(num)
+        off = np.zeros((num, self.dim))
+        off[:, 0], off[:, 1] = np.cos(th) * r, np.sin(th) * r
+        x = np.asarray(center[:self.dim], dtype=np.float64)[None, :] + off * radius
+        return self._append(x, velocity[:self.dim], material, "emit_water")
+
+    # mesh emitters (3D)
+
+    def _voxelizer(self):
+        if self.dim != 3:
+            raise ValueError("mesh emitters are 3D")
+        if self._vox is None:
+            from .voxelizer import Voxelizer
+
+            self.voxelizer_super_sample = 2
+            self._vox = Voxelizer(res=(self.n_grid,) * 3, dx=self.dx, super_sample=self.voxelizer_super_sample)
+        return self._vox
+
+    @property
+    def voxelizer(self):
+        return self._voxelizer()
+
+    def add_mesh(self, triangles, material=None, color=0xFFFFFF, sample_density=None, velocity=None,
+                 translation=None, s=0):
+        """add_mesh (mpm_solver.py:1356-1376): voxelize the triangles, then
+        seed sample_density + 1 particles per inside voxel."""
+        if sample_density is None:
+            sample_density = 2 ** self.dim
+        self._voxelizer().voxelize(triangles)
+        return self.add_particles_from_voxels(sample_density, translation, velocity, s,
+                                              material if isinstance(material, int) else 0)
+
+    def cnt_mesh_particles_num(self, triangles, material=None, color=0xFFFFFF, sample_density=None, velocity=None,
+                               translation=None):
+        """Particles add_mesh would emit (mpm_solver.py:1382-1400)."""
+        if sample_density is None:
+            sample_density = 2 ** self.dim
+        vox = self._voxelizer().voxelize(triangles)
+        return int((vox > 0).sum()) * (sample_density + 1)
+
+    def add_particles_from_voxels(self, sample_density, translation=None, velocity=None, s=0, material=0):
+        """seed_from_voxels (mpm_solver.py:1415-1440): for every voxel (i, j,
+        k) with a positive count, sample_density + 1 particles at
+        (u + (i, j, k)) dx + translation with the given velocity.  dx is the
+        simulation grid's spacing, not the voxel's, as in the reference.
+        Particles are appended in voxel order (row-major), then sample."""
+        vox = self._voxelizer().voxels
+        idx = np.argwhere(vox.cpu().numpy() > 0).astype(np.float64)
+        k = int(sample_density) + 1
+        rng = self._rng(3)
+        x = (rng.random((len(idx), k, 3)) + idx[:, None, :]) * self.dx
+        x = x.reshape(-1, 3) + np.asarray([0.0, 0.0, 0.0] if translation is None else list(translation))
+        v = np.zeros(3) if velocity is None else np.asarray(list(velocity), dtype=np.float64)
+        return self._append(x, v, material, "add_mesh")
+
+    def set_emit_data(self, data):
+        """Positions the letters emitter places (mpm_solver.py:124-128)."""
+        self._emit_data = np.asarray(data, dtype=np.float64).reshape(-1, self.dim)
+
+    def emit_letters_one_frame(self, velocity=(0.0, -2.0, 0.0)):
+        """emit_letters_one_frame (mpm_solver.py:130-135): the set_emit_data
+        positions, moving with velocity (0, -2, 0)."""
+        if getattr(self, "_emit_data", None) is None:
+            raise ValueError("set_emit_data first")
+        return self._append(self._emit_data, np.asarray(velocity[:self.dim]), 0, "emit_letters_one_frame")
 
     def set_particles(self, values):
         """Set all active particles from an (n x n_slots) array: numpy (host),
@@ -308,8 +439,20 @@ class MPMSolver:
         self.substeps(1)
 
     def run_forward_only(self, save_pics=False, save_states=False):
-        """run_forward_only of the drivers: n_timestep-1 substeps, then the loss."""
-        self.substeps(self.n_timestep - 1)
+        """run_forward_only of the drivers (run_mpm_elastic_2d.py:124-162):
+        n_timestep-1 substeps, then the loss; with save_states the positions
+        are dumped after every frame of `steps` substeps (dump_states)."""
+        total = self.n_timestep - 1
+        if not save_states:
+            self.substeps(total)
+        else:
+            s, frame = 0, 0
+            while s < total:
+                k = min(int(self.param.steps), total - s)
+                self.substeps(k)
+                s += k
+                self.dump_states(frame)
+                frame += 1
         self.compute_loss()
         return self.loss[None]
 
@@ -396,6 +539,76 @@ class MPMSolver:
         if self._sim is not None:
             self._ensure_sim()
         return data
+
+    fetch_mat_data_np = fetch_data_np
+    fetch_scalar_data_np = fetch_data_np
+    push_mat_data_np = push_data_np
+    push_scalar_data_np = push_data_np
+
+    # ------------------------------------------------------ on-disk formats
+
+    def _out_folder(self):
+        folder = self.param.pos_output_folder
+        if not folder:
+            raise ValueError("pos_output_folder is not set")
+        os.makedirs(folder, exist_ok=True)
+        return folder
+
+    def dump_states(self, frame):
+        """Positions as data_{frame:06d}.ply in pos_output_folder
+        (mpm_solver.py:1776-1780); 2D positions get z = 0."""
+        from .mesh_io import write_point_cloud_packed
+
+        x = self.fetch_data_np("x")
+        if self.dim == 2:
+            x = np.concatenate([x, np.zeros((len(x), 1), np.float32)], axis=1)
+        fn = os.path.join(self._out_folder(), "data_%06d.ply" % frame)
+        write_point_cloud_packed(fn, x, len(x))
+        return fn
+
+    def checkpoint_states(self, frame):
+        """v.npy, C.npy and J.npy (fluid) or F.npy in pos_output_folder, the
+        rest of the state load_states needs (mpm_solver.py:1761-1774)."""
+        folder = self._out_folder()
+        for name in ("v", "C", "F" if self.has_F else "J"):
+            np.save(os.path.join(folder, "%s.npy" % name), self.fetch_data_np(name))
+        return folder
+
+    def load_states(self, folder, frame):
+        """Particles from data_{frame:06d}.ply plus v.npy, C.npy and F.npy
+        or J.npy (mpm_solver.py:1869-1895); the particle count is the file's."""
+        from .mesh_io import load_particles_only
+
+        x = load_particles_only(os.path.join(folder, "data_%06d.ply" % frame))[:, :self.dim]
+        n = len(x)
+        if n > self.n_particles:
+            raise ValueError("load_states: %d particles exceed n_particles=%d" % (n, self.n_particles))
+        vals = np.array(self._staging()[:n], copy=True)
+        vals[:, slice(*self.slot_range("x"))] = x
+        for name in ("v", "C", "F" if self.has_F else "J"):
+            a, b = self.slot_range(name)
+            vals[:, a:b] = np.load(os.path.join(folder, "%s.npy" % name)).reshape(n, b - a)
+        self.set_particles(vals)
+
+    def grid_mass(self):
+        """Node masses of the latest substep's P2G (a res-shaped float32
+        CUDA tensor): the grid_m of dump_grid."""
+        import torch
+
+        self._ensure_sim()
+        out = torch.empty(tuple(self._params().res[:self.dim]), dtype=torch.float32, device="cuda")
+        _lib.check(_lib.lib().aq_sim_grid_mass(self._sim, C.c_void_p(out.data_ptr()), _lib.stream_ptr()),
+                   "aq_sim_grid_mass")
+        return out
+
+    def dump_grid(self, frame, grid_m=None):
+        """density_{frame:06d}.npz (m as float16) in pos_output_folder
+        (mpm_solver.py:1755-1759); grid_m defaults to grid_mass()."""
+        m = self.grid_mass() if grid_m is None else grid_m
+        m = m.cpu().numpy() if hasattr(m, "cpu") else np.asarray(m)
+        fn = os.path.join(self._out_folder(), "density_%06d.npz" % frame)
+        np.savez_compressed(fn, m=m.astype(np.float16))
+        return fn
 
     def status(self, clear=False):
         self._ensure_sim()

@@ -193,6 +193,25 @@ int aq_sim_get_words(aq_sim* sim, uint64_t* d_words, void* stream);
  * P2G of substep k+1 run in one kernel. */
 int aq_sim_substeps(aq_sim* sim, int32_t n, void* stream);
 
+/* Mesh voxelizer of the emitters (add_mesh: voxelizer.py:53-119): voxel
+ * counts of n_tris triangles (d_tris: n_tris x 9 doubles, corners a, b, c)
+ * on a res[0] x res[1] x res[2] voxel grid of spacing dx into d_voxels
+ * (int32, row-major; voxels > 0 are inside).  Every triangle whose normal
+ * has |z| >= 1e-10 adds +1 (normal z > 0) or -1 to the voxels
+ * [padding, height) of each column (p, q) in [padding, res - padding) whose
+ * centre ((p + 0.5) dx, (q + 0.5) dx) its xy projection covers, height =
+ * min(int(-n.(c - a) / n_z / dx + 0.5), res[1] - padding); vertices are
+ * first moved by the reference's fixed jitter times jitter_scale (1e-8 at
+ * double precision).  Needs 2 padding < res[k]; asynchronous on stream. */
+int aq_voxelize(const double* d_tris, int64_t n_tris, const int32_t* res, double dx, int32_t padding,
+                double jitter_scale, int32_t* d_voxels, void* stream);
+
+/* Grid masses after the latest substep (the P2G sums grid_op starts from;
+ * zeros before the first substep) into d_out, res[0] x res[1] (x res[2])
+ * floats, row-major: the grid_m that dump_grid writes
+ * (mpm_solver.py:1755-1759). */
+int aq_sim_grid_mass(aq_sim* sim, float* d_out, void* stream);
+
 /* Loss of the current state (written to *h_out, synchronizes the stream).
  * kind 0: compute_ek (mpm_solver.py:1043-1052): 3D sum 0.5 m|v|^2 + g m x_y,
  * 2D sum |v|^2. */

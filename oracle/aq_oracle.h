@@ -16,6 +16,9 @@
  *   bit_pack    codegen_llvm_quant.cpp:884-952 (BitPackAssignStmt)
  *   substep     mpm_exps/engine/mpm_solver.py:590-758, 1012-1031, 1043-1052
  *   polar 2D    taichi_submission/python/taichi/lang/linalg_impl.py:9-26
+ *   collider    mpm_exps/engine/mpm_solver.py:1459-1547 (in aq_oracle_mpm.c)
+ *   voxelizer   mpm_exps/engine/voxelizer.py:10-105 (aq_oracle_emit.c; no
+ *               reference output to pin it: known-answer meshes in tests/)
  * Parity of this restatement is pinned by the reference's own quant tests
  * (taichi_submission/tests/python/test_bit_pack*.py, test_dithering.py,
  * test_custom_float*.py, test_fxp_offset.py) ported in tests/.
@@ -51,5 +54,8 @@ typedef struct or_params {
   const float* col_sdf;
   const float* col_nrm;
 } or_params;
+
+void or_voxelize(const double* tris, int64_t n_tris, const int32_t* res, double dx, int32_t padding,
+                 double jitter_scale, int32_t* vox);
 
 #endif

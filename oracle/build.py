@@ -14,7 +14,7 @@ import sys
 HERE = os.path.dirname(os.path.abspath(__file__))
 OUT = os.path.join(HERE, "_build")
 LIB = os.path.join(OUT, "libaqoracle.so")
-SRCS = ["aq_oracle.h", "aq_oracle_codec.c", "aq_oracle_mpm.c"]
+SRCS = ["aq_oracle.h", "aq_oracle_codec.c", "aq_oracle_mpm.c", "aq_oracle_emit.c"]
 
 
 def _stale():
@@ -34,6 +34,7 @@ def build(force=False, verbose=False):
         ("aq_oracle_codec.c", "codec.o", []),
         ("aq_oracle_mpm.c", "mpm_f32.o", ["-DREAL=float", "-DSUF(x)=x##_f32"]),
         ("aq_oracle_mpm.c", "mpm_f64.o", ["-DREAL=double", "-DSUF(x)=x##_f64"]),
+        ("aq_oracle_emit.c", "emit.o", []),
     ]
     for src, obj, defs in units:
         o = os.path.join(OUT, obj)

@@ -81,6 +81,9 @@ def lib():
             g = getattr(L, "or_loss_ek_" + suf)
             g.argtypes = [C.POINTER(OrParams), C.POINTER(OrLayout), up, C.c_int64]
             g.restype = C.c_double
+        L.or_voxelize.argtypes = [dp, C.c_int64, C.POINTER(C.c_int32), C.c_double, C.c_int32, C.c_double,
+                                  C.POINTER(C.c_int32)]
+        L.or_voxelize.restype = None
         _lib = L
     return _lib
 
@@ -126,6 +129,17 @@ def decode(L, words):
 def uniform(seed, step, pid, slot, f64=False):
     pk = lib().or_particle_key(lib().or_step_key(C.c_uint64(seed), step), pid)
     return lib().or_uniform_f64(pk, slot) if f64 else lib().or_uniform_f32(pk, slot)
+
+
+def voxelize(triangles, res, dx, padding=3, jitter_scale=1e-8):
+    """Voxel counts of n x 9 triangles on a res voxel grid of spacing dx
+    (aq_oracle_emit.c, restating voxelizer.py:53-105)."""
+    t = np.ascontiguousarray(triangles, dtype=np.float64).reshape(-1, 9)
+    out = np.zeros(tuple(res), dtype=np.int32)
+    r = (C.c_int32 * 3)(*res)
+    lib().or_voxelize(_ptr(t, C.c_double), len(t), r, float(dx), int(padding), float(jitter_scale),
+                      _ptr(out, C.c_int32))
+    return out
 
 
 class Sim:

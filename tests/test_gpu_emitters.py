@@ -1,0 +1,130 @@
+"""Emitters and on-disk formats on the GPU: the CUDA voxelizer
+(aq_voxelize) bit-exact against the oracle's restatement, add_mesh
+seeding, the collider push-out of add_cube, the grid mass, and the
+dump / checkpoint / load round trip."""
+import os
+
+import numpy as np
+import pytest
+
+import oracle as O
+from autoquantizer_b200 import scenes
+from autoquantizer_b200.mpm_solver import MPMSolver
+from autoquantizer_b200.voxelizer import Voxelizer
+from helpers import box_mesh, sphere_mesh, quant_steps
+
+pytestmark = pytest.mark.gpu
+
+
+def _soup(n, seed=0):
+    """Random triangles, many of them large and overlapping."""
+    rng = np.random.default_rng(seed)
+    c = rng.random((n, 1, 3)) * 0.8 + 0.1
+    return (c + (rng.random((n, 3, 3)) - 0.5) * rng.random((n, 1, 1)) * 0.6).reshape(n, 9)
+
+
+@pytest.mark.parametrize("mesh", ["box", "sphere", "soup", "empty"])
+def test_voxelizer_matches_oracle(mesh):
+    tris = {"box": lambda: box_mesh((0.13, 0.21, 0.17), (0.61, 0.44, 0.72)),
+            "sphere": lambda: sphere_mesh((0.45, 0.5, 0.55), 0.3, 20, 28),
+            "soup": lambda: _soup(3000),
+            "empty": lambda: np.zeros((0, 9))}[mesh]()
+    vox = Voxelizer(res=(48, 48, 48), dx=1 / 48, super_sample=2)
+    assert vox.res == (128, 128, 128) and vox.dx == 1 / 96
+    got = vox.voxelize(tris).cpu().numpy()
+    want = O.voxelize(tris, vox.res, vox.dx, vox.padding, vox.jitter_scale)
+    assert np.array_equal(got, want)
+    if mesh == "box":
+        assert got.sum() > 0 and got.max() == 1
+
+
+def _solver(n=200000, n_grid=32):
+    cfg, _ = scenes.falling_block_3d(n=n, n_grid=n_grid)
+    s = MPMSolver(cfg)
+    s.initialize()
+    return s
+
+
+def test_add_mesh_seeds_every_inside_voxel():
+    s = _solver()
+    tris = box_mesh((0.1, 0.12, 0.14), (0.2, 0.25, 0.22))
+    cnt = s.cnt_mesh_particles_num(tris, sample_density=3)
+    n = s.add_mesh(tris, sample_density=3, velocity=(0.0, -4.0, 0.0), translation=(0.3, 0.2, 0.1))
+    assert n == cnt == s.current_idx > 0
+    vox = s.voxelizer.voxels.cpu().numpy()
+    h = s._staging()[:n]
+    idx = np.floor((h[:, :3] - [0.3, 0.2, 0.1]) / s.dx + 1e-9).astype(int)
+    assert np.all(vox[idx[:, 0], idx[:, 1], idx[:, 2]] > 0)
+    # every inside voxel got sample_density + 1 particles
+    _, per = np.unique(idx, axis=0, return_counts=True)
+    assert len(per) == int((vox > 0).sum()) and np.all(per == 4)
+    assert np.all(h[:, 3:6] == [0.0, -4.0, 0.0])
+    s.substeps(4)
+    assert s.status()[0] == 0
+
+
+def test_add_cube_moves_particles_out_of_the_collider():
+    from test_gpu_collider import bar_sdf
+
+    cfg, _ = scenes.falling_block_3d(n=20000, n_grid=32)
+    cfg.grid_res = [64, 32, 64]
+    cfg.ub = [61, 29, 61]
+    s = MPMSolver(cfg)
+    s.initialize()
+    sdf, normal = bar_sdf()
+    s.init_sdf_value(sdf, normal, theta=0.0)
+    s.add_cube((0.3, 0.2, 0.9), (1.4, 0.3, 0.2), 20000)
+    x = s._staging()[:20000, :3]
+    free = MPMSolver(cfg)
+    free.initialize()
+    free.add_cube((0.3, 0.2, 0.9), (1.4, 0.3, 0.2), 20000)
+    x0 = free._staging()[:20000, :3]
+    moved = np.any(x != x0, axis=1)
+    # the bar occupies y cells 8..11 over z cells 28..35: particles whose
+    # cell int(x / dx + 0.5) is there moved up by 2..5 cells
+    cell = (x0 / s.dx + 0.5).astype(int)
+    inside = (cell[:, 1] >= 8) & (cell[:, 1] < 12) & (cell[:, 2] >= 28) & (cell[:, 2] < 36)
+    assert inside.any() and np.array_equal(moved, inside)
+    dy = (x[moved, 1] - x0[moved, 1]) / s.dx
+    assert np.all((dy >= 2) & (dy <= 5)) and np.all(x[moved][:, [0, 2]] == x0[moved][:, [0, 2]])
+
+
+def test_grid_mass_conserves_particle_mass():
+    s = _solver(n=20000)
+    s.add_cube((0.3, 0.3, 0.3), (0.3, 0.3, 0.3), 20000)
+    assert float(s.grid_mass().abs().sum()) == 0.0  # before the first substep
+    s.substeps(3)
+    m = s.grid_mass()
+    assert tuple(m.shape) == (32, 32, 32)
+    assert float(m.double().sum()) == pytest.approx(20000 * s.p_mass, rel=1e-5)
+
+
+def test_dump_checkpoint_load_round_trip(tmp_path):
+    s = _solver(n=20000)
+    s.param.pos_output_folder = str(tmp_path)
+    s.add_cube((0.3, 0.3, 0.3), (0.3, 0.3, 0.3), 20000)
+    s.substeps(10)
+    fn = s.dump_states(7)
+    assert os.path.basename(fn) == "data_000007.ply"
+    s.checkpoint_states(7)
+    assert sorted(os.listdir(tmp_path)) == ["C.npy", "F.npy", "data_000007.ply", "v.npy"]
+    g = s.dump_grid(7)
+    assert np.load(g)["m"].dtype == np.float16
+    before = s.state_values()
+    t = _solver(n=20000)
+    t.load_states(str(tmp_path), 7)
+    assert t.current_idx == 20000
+    after = t.state_values()
+    # float32 files, re-encoded: within one quantization step (plus f32 rounding)
+    tol = np.maximum(np.nan_to_num(quant_steps(s)), 1e-6 * np.abs(before).max(0))
+    assert np.all(np.abs(after - before) <= tol[None, :] + 1e-7)
+
+
+def test_run_forward_only_dumps_every_frame(tmp_path):
+    s = _solver(n=5000)
+    s.param.pos_output_folder = str(tmp_path)
+    s.n_timestep, s.param.steps = 11, 4
+    s.add_cube((0.3, 0.3, 0.3), (0.2, 0.2, 0.2), 5000)
+    s.run_forward_only(save_states=True)
+    assert sorted(os.listdir(tmp_path)) == ["data_000000.ply", "data_000001.ply", "data_000002.ply"]
+    assert s.launches() > 0
