@@ -7,7 +7,8 @@
 // which a memset clears first).  Every sort_interval substeps the records
 // are re-binned: k_bin (cell key and rank), an exclusive scan of the
 // per-cell counts, k_scatter (records and ids into block-wide slot-major
-// order), k_items (one work item per occupied block).
+// order), k_items_count + k_items (one work item per occupied block, the
+// fullest blocks first).
 #include <math.h>
 #include <stdio.h>
 #include <string.h>
@@ -92,14 +93,40 @@ __global__ void __launch_bounds__(256) k_scatter(const uint64_t* __restrict__ wi
   pout[dst] = pin[i];
 }
 
-// One work item per occupied cell block: (block, first record, count).
-__global__ void k_items(const int32_t* __restrict__ start, int nblk, int4* __restrict__ items,
-                        int32_t* __restrict__ n_items) {
+// One work item per occupied cell block: (block, first record, count),
+// ordered by decreasing count in buckets of 16 records (largest first, so
+// that the persistent CTAs that claim items end on small ones).
+// item_info: [0] item count, [1, 1 + IB) bucket sizes, [1 + IB, 1 + 2 IB)
+// bucket fill cursors; zeroed before k_items_count.
+constexpr int IB = 64;
+
+__device__ __forceinline__ int item_bucket(int c) { return IB - 1 - min(IB - 1, (c - 1) >> 4); }
+
+__global__ void k_items_count(const int32_t* __restrict__ start, int nblk, int32_t* __restrict__ item_info) {
   const int b = blockIdx.x * blockDim.x + threadIdx.x;
   if (b >= nblk) return;
-  const int s = start[(int64_t)b * 64], e = start[(int64_t)(b + 1) * 64];
-  if (e <= s) return;
-  items[atomicAdd(n_items, 1)] = make_int4(b, s, e - s, 0);
+  const int c = start[(int64_t)(b + 1) * 64] - start[(int64_t)b * 64];
+  if (c > 0) atomicAdd(item_info + 1 + item_bucket(c), 1);
+}
+
+__global__ void k_items(const int32_t* __restrict__ start, int nblk, int4* __restrict__ items,
+                        int32_t* __restrict__ item_info) {
+  __shared__ int off[IB];
+  if (threadIdx.x == 0) {
+    int acc = 0;
+    for (int k = 0; k < IB; ++k) {
+      off[k] = acc;
+      acc += item_info[1 + k];
+    }
+    if (blockIdx.x == 0) item_info[0] = acc;
+  }
+  __syncthreads();
+  const int b = blockIdx.x * blockDim.x + threadIdx.x;
+  if (b >= nblk) return;
+  const int s = start[(int64_t)b * 64], c = start[(int64_t)(b + 1) * 64] - s;
+  if (c <= 0) return;
+  const int k = item_bucket(c);
+  items[off[k] + atomicAdd(item_info + 1 + IB + k, 1)] = make_int4(b, s, c, 0);
 }
 
 // Exclusive scan of n int32 counts into out[0..n] (out[n] = total), in
@@ -317,7 +344,7 @@ struct aq_sim {
   int nblk = 0;
   int32_t *keys = nullptr, *ranks = nullptr, *cell_count = nullptr, *cell_start = nullptr, *scan_sums = nullptr;
   int4* items = nullptr;
-  int32_t* n_items = nullptr;
+  int32_t* n_items = nullptr;  // [0] item count, then k_items' bucket sizes and cursors
   int32_t* item_ctr = nullptr;  // [2] k_step's item claim counters
   int64_t step_launches = 0;
   int64_t max_items = 0;
@@ -414,7 +441,7 @@ struct SimImpl final : SimBase {
     aq_sim* S_ = s;
     const int64_t n = S_->n;
     AQ_CUDA_TRY(cudaMemsetAsync(S_->cell_count, 0, sizeof(int32_t) * S_->nkeys, st));
-    AQ_CUDA_TRY(cudaMemsetAsync(S_->n_items, 0, sizeof(int32_t), st));
+    AQ_CUDA_TRY(cudaMemsetAsync(S_->n_items, 0, sizeof(int32_t) * (1 + 2 * IB), st));
     k_bin<D, R><<<grid_for(n, 256), 256, 0, st>>>(S_->L, K, S_->words[S_->cur], n, S_->keys, S_->ranks, S_->cell_count,
                                                   S_->status);
     const int nt = (int)((S_->nkeys + SCAN_TILE - 1) / SCAN_TILE);
@@ -424,10 +451,11 @@ struct SimImpl final : SimBase {
     const int nxt = 1 - S_->cur;
     k_scatter<<<grid_for(n, 256), 256, 0, st>>>(S_->words[S_->cur], S_->pid[S_->cur], S_->words[nxt], S_->pid[nxt],
                                                 S_->keys, S_->ranks, S_->cell_start, n, S_->W);
+    k_items_count<<<grid_for(S_->nblk, 256), 256, 0, st>>>(S_->cell_start, S_->nblk, S_->n_items);
     k_items<<<grid_for(S_->nblk, 256), 256, 0, st>>>(S_->cell_start, S_->nblk, S_->items, S_->n_items);
     AQ_CUDA_TRY(cudaGetLastError());
     S_->cur = nxt;
-    S_->launches += 6;
+    S_->launches += 7;
     S_->since_sort = 0;
     S_->sorted = true;
     return AQ_OK;
@@ -661,7 +689,7 @@ int aq_sim_create(const aq_params* P, const aq_layout* L, aq_sim** out) {
   alloc((void**)&s->cell_start, sizeof(int32_t) * (s->nkeys + 1));
   alloc((void**)&s->scan_sums, sizeof(int32_t) * (nt + 1));
   alloc((void**)&s->items, sizeof(int4) * s->max_items);
-  alloc((void**)&s->n_items, sizeof(int32_t));
+  alloc((void**)&s->n_items, sizeof(int32_t) * (1 + 2 * IB));
   alloc((void**)&s->item_ctr, 2 * sizeof(int32_t));
   alloc((void**)&s->status, sizeof(unsigned));
   alloc((void**)&s->fallbacks, sizeof(unsigned long long));
