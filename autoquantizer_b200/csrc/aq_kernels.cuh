@@ -63,8 +63,14 @@ constexpr int NWARP = CH / 32;
 template <int D>
 struct Geo {
   static constexpr int BS = D == 3 ? 4 : 8;          // block edge (cells)
-  static constexpr int T = BS + 4;                   // tile edge: one cell of drift each side + stencil
-  static constexpr int XS = D == 3 ? T * T + 4 : T;  // stride of the slowest tile axis (padded)
+  // tile edge: base cells of a block's particles span the block and the
+  // cell below it, plus the 3-node stencil; 2D keeps one cell of slack for
+  // drift between re-binnings (3D particles that drift out take the global
+  // fallback path: a 7-node tile leaves room in L1 for the 4 CTAs per SM)
+  static constexpr int T = D == 3 ? BS + 3 : BS + 4;
+  // stride of the slowest tile axis, padded to 4 mod 8 nodes so that
+  // neighbouring x planes fall in different 16-byte bank groups
+  static constexpr int XS = D == 3 ? (T * T + 3) / 8 * 8 + 4 : T;
   static constexpr int TNP = D == 3 ? T * XS : T * T;  // nodes per tile plane incl. padding
 };
 
