@@ -180,7 +180,7 @@ void* jit_k_step(int D, bool HF, bool HM, bool f64, bool col, const aq_layout& L
   }
   g_nv.add_name(prog, name);
   // AQ_JIT_DEFINES (environment): extra -D options, e.g.
-  // "AQ_STEP_MIN_BLOCKS=1", separated by spaces (tuning experiments)
+  // "AQ_STEP_MIN_BLOCKS(R)=4", separated by spaces (tuning experiments)
   std::vector<std::string> extra;
   if (const char* e = getenv("AQ_JIT_DEFINES")) {
     std::string s(e), tok;

@@ -56,8 +56,11 @@ namespace aq {
 #endif
 constexpr int CH = AQ_CH;  // particles per work item = threads per CTA
 constexpr int NWARP = CH / 32;
+// CTAs per SM the register allocation of k_step must allow: 6 (80
+// registers) for float, where more resident warps beat the extra spills and
+// 6 CTAs' shared memory still fits; 4 (128 registers) for double
 #ifndef AQ_STEP_MIN_BLOCKS
-#define AQ_STEP_MIN_BLOCKS (512 / AQ_CH)  // CTAs per SM the register allocation must allow (128 registers)
+#define AQ_STEP_MIN_BLOCKS(R) (sizeof(R) == 8 ? 512 / AQ_CH : 768 / AQ_CH)
 #endif
 
 template <int D>
@@ -370,7 +373,7 @@ __device__ __forceinline__ void bspline(const R* x, const SimK<R>& K, int* base,
 // COL: compiled with the SDF collider (the library's own build always is;
 // the layout-specialized build only when a collider is set).
 template <int D, bool HF, bool HM, class R, class LA, bool COL = true>
-__global__ void __launch_bounds__(CH, AQ_STEP_MIN_BLOCKS) k_step(const __grid_constant__ aq_layout Lp, const SimK<R> K,
+__global__ void __launch_bounds__(CH, AQ_STEP_MIN_BLOCKS(R)) k_step(const __grid_constant__ aq_layout Lp, const SimK<R> K,
                                                 const StepArgs A) {
   typedef Sch<D, HF, HM> S;
   typedef Geo<D> G;
