@@ -115,7 +115,10 @@ void fmt_f64(std::string& s, double v) {
 std::string jit_layout_source(const aq_layout& L) {
   std::string s;
   char b[256];
-  s += "struct JitLayout {\n  static __device__ __forceinline__ aq_layout get(const aq_layout&) {\n    return aq_layout{";
+  snprintf(b, sizeof b, "struct JitLayout {\n  static constexpr bool kRegRecord = true;\n  static constexpr int kWords = %d;\n",
+           L.n_words);
+  s += b;
+  s += "  static __device__ __forceinline__ aq_layout get(const aq_layout&) {\n    return aq_layout{";
   snprintf(b, sizeof b, "%d, %d, %d, %d, %d, %d, {0, 0}, {", L.n_slots, L.n_words, L.total_bits, L.compute_f64,
            L.use_dithering, L.n_groups);
   s += b;

@@ -136,6 +136,8 @@ struct StepArgs {
 
 // Layout from the kernel parameter (nvcc build).
 struct RtLayout {
+  static constexpr bool kRegRecord = false;  // records pass through shared memory (runtime word count)
+  static constexpr int kWords = 1;
   static __device__ __forceinline__ const aq_layout& get(const aq_layout& p) { return p; }
 };
 
@@ -388,7 +390,7 @@ __global__ void __launch_bounds__(CH, AQ_STEP_MIN_BLOCKS(R)) k_step(const __grid
   extern __shared__ __align__(16) unsigned char smem_raw[];
   R4* gtile = reinterpret_cast<R4*>(smem_raw);                      // TNP nodes (m, v): G2P source
   R4* ptile = gtile + TNP;                                     // NWARP x TNP (m, m v): P2G, per warp
-  uint64_t* srec = reinterpret_cast<uint64_t*>(ptile + NWARP * TNP);  // CH x WS: each thread's record
+  uint64_t* srec = reinterpret_cast<uint64_t*>(ptile + NWARP * TNP);  // CH x WS: each thread's record (RtLayout)
   __shared__ int sbox[6];  // tile-coordinate box of the item's P2G base cells (min[3], max[3])
   __shared__ int s_next;   // the CTA's next work item, claimed from A.item_ctr
 
@@ -397,7 +399,11 @@ __global__ void __launch_bounds__(CH, AQ_STEP_MIN_BLOCKS(R)) k_step(const __grid
   const R4* gin = reinterpret_cast<const R4*>(A.grid_in);
   R4* gout = reinterpret_cast<R4*>(A.grid_out);
   unsigned fl = 0, nfall = 0;
-  uint64_t* myrec = srec + tid * WS;
+  // the thread's record words: registers when the layout (and so the word
+  // count and every bit offset) is a compile-time constant, else a slot of
+  // shared memory
+  uint64_t rrec[LA::kRegRecord ? LA::kWords : 1];
+  uint64_t* const myrec = LA::kRegRecord ? rrec : srec + tid * WS;
   R4 zero4;
   zero4.x = zero4.y = zero4.z = zero4.w = 0;
   if (A.do_p2g)  // private tiles start at zero; the flush of every item re-zeroes them
@@ -460,6 +466,7 @@ __global__ void __launch_bounds__(CH, AQ_STEP_MIN_BLOCKS(R)) k_step(const __grid
       int32_t pid = 0;
       if (active) {
         const uint64_t* src = A.words + rec * W;
+#pragma unroll
         for (int k = 0; k < W; ++k) myrec[k] = __ldg(src + k);
         pid = __ldg(A.pid + rec);
       }
@@ -603,6 +610,7 @@ __global__ void __launch_bounds__(CH, AQ_STEP_MIN_BLOCKS(R)) k_step(const __grid
         // read of the record returns (input of the next P2G)
         encode_record<NS, R>(L, vals, myrec, particle_key(A.sk, pid), (const float*)0, (const double*)0);
         uint64_t* dst = A.words + rec * W;
+#pragma unroll
         for (int k = 0; k < W; ++k) dst[k] = myrec[k];
       }
 

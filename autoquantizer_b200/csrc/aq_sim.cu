@@ -324,7 +324,7 @@ struct SimBase {
   virtual int substeps(int n, cudaStream_t st) = 0;
   virtual int loss(double* h, cudaStream_t st) = 0;
   virtual int sort(cudaStream_t st) = 0;
-  virtual size_t smem_bytes() const = 0;
+  virtual size_t smem_bytes(bool reg_record) const = 0;
   virtual void set_collider(const aq_sim* sim) = 0;
   virtual int setup_kernel(bool col) = 0;
 };
@@ -366,6 +366,7 @@ struct aq_sim {
   bool sorted = false;
   int64_t launches = 0;
   int step_grid = 0;
+  size_t step_smem = 0;  // dynamic shared memory of the k_step in use
   void* jit_fn = nullptr;  // CUfunction of the layout-specialized k_step, or null
   std::string jit_error;
   aq::SimBase* impl = nullptr;
@@ -379,7 +380,7 @@ struct aq_sim {
 namespace aq {
 
 template <int D, bool HF, bool HM, class R>
-static int setup_step_kernel(aq_sim* s, size_t smem, bool col);
+static int setup_step_kernel(aq_sim* s, size_t smem_jit, size_t smem_aot, bool col);
 
 template <int D, bool HF, bool HM, class R>
 struct SimImpl final : SimBase {
@@ -415,7 +416,9 @@ struct SimImpl final : SimBase {
     }
   }
 
-  int setup_kernel(bool col) override { return setup_step_kernel<D, HF, HM, R>(s, smem_bytes(), col); }
+  int setup_kernel(bool col) override {
+    return setup_step_kernel<D, HF, HM, R>(s, smem_bytes(true), smem_bytes(false), col);
+  }
 
   void set_collider(const aq_sim* c) override {
     const aq_params& P = c->P;
@@ -432,9 +435,11 @@ struct SimImpl final : SimBase {
     K.col_omega = (R)c->col_omega;
   }
 
-  size_t smem_bytes() const override {
+  // the grid tile and the warp tiles, plus a record slot per thread unless
+  // the kernel keeps records in registers (layout-specialized build)
+  size_t smem_bytes(bool reg_record) const override {
     const size_t b = sizeof(typename R4T<R>::type) * (NWARP + 1) * Geo<D>::TNP;
-    return b + sizeof(uint64_t) * (size_t)CH * s->WS;
+    return b + (reg_record ? 0 : sizeof(uint64_t) * (size_t)CH * s->WS);
   }
 
   int sort(cudaStream_t st) override {
@@ -494,12 +499,12 @@ struct SimImpl final : SimBase {
     if (prof) AQ_CUDA_TRY(cudaEventRecord(S_->prof_ev[0][2 * S_->prof_n[0]], st));
     if (S_->jit_fn) {
       void* args[] = {(void*)&S_->L, (void*)&K, (void*)&a};
-      if (jit_launch(S_->jit_fn, S_->step_grid, CH, smem_bytes(), st, args) != AQ_OK) {
+      if (jit_launch(S_->jit_fn, S_->step_grid, CH, S_->step_smem, st, args) != AQ_OK) {
         set_last_cuda_error(cudaErrorLaunchFailure, "cuLaunchKernel(k_step)");
         return AQ_E_CUDA;
       }
     } else {
-      k_step<D, HF, HM, R, RtLayout><<<S_->step_grid, CH, smem_bytes(), st>>>(S_->L, K, a);
+      k_step<D, HF, HM, R, RtLayout><<<S_->step_grid, CH, S_->step_smem, st>>>(S_->L, K, a);
       AQ_CUDA_TRY(cudaGetLastError());
     }
     if (prof) AQ_CUDA_TRY(cudaEventRecord(S_->prof_ev[0][2 * S_->prof_n[0]++ + 1], st));
@@ -564,17 +569,21 @@ struct SimImpl final : SimBase {
 // Compile (NVRTC, layout as a constant; with or without the collider) or
 // select the library's own k_step, and size its persistent grid.
 template <int D, bool HF, bool HM, class R>
-static int setup_step_kernel(aq_sim* s, size_t smem, bool col) {
+static int setup_step_kernel(aq_sim* s, size_t smem_jit, size_t smem_aot, bool col) {
   int occ = 0;
   s->jit_fn = nullptr;
   if (s->P.jit) {
+    const size_t smem = smem_jit;
     s->jit_fn = jit_k_step(D, HF, HM, sizeof(R) == 8, col, s->L, &s->jit_error);
     if (s->jit_fn && (jit_set_smem(s->jit_fn, (int)smem) != AQ_OK || jit_occupancy(s->jit_fn, CH, smem, &occ) != AQ_OK)) {
       s->jit_fn = nullptr;
       s->jit_error = "cuFuncSetAttribute/occupancy failed";
     }
+    s->step_smem = smem;
   }
   if (!s->jit_fn) {
+    const size_t smem = smem_aot;
+    s->step_smem = smem;
     AQ_CUDA_TRY(cudaFuncSetAttribute(k_step<D, HF, HM, R, RtLayout>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                      (int)smem));
     AQ_CUDA_TRY(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, k_step<D, HF, HM, R, RtLayout>, CH, smem));
@@ -589,9 +598,9 @@ static int make_impl(aq_sim* s) {
   auto* im = new (std::nothrow) SimImpl<D, HF, HM, R>(s);
   if (!im) return AQ_E_NOMEM;
   s->impl = im;
-  const size_t smem = im->smem_bytes();
+  const size_t smem = im->smem_bytes(false);
   if (smem > 227 * 1024) return AQ_E_LIMIT;
-  return setup_step_kernel<D, HF, HM, R>(s, smem, false);
+  return setup_step_kernel<D, HF, HM, R>(s, im->smem_bytes(true), smem, false);
 }
 
 template <int D, class R>
