@@ -66,6 +66,14 @@ __global__ void __launch_bounds__(256) k_scatter(const uint64_t* __restrict__ wi
                                                  const int32_t* __restrict__ start, int64_t n, int W) {
   const int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
   if (i >= n) return;
+  // the record's words are loaded first, all at once: they do not depend on
+  // the destination, so their latency overlaps the offset computation
+  constexpr int WB = 8;
+  uint64_t buf[WB];
+#pragma unroll
+  for (int j = 0; j < WB; ++j)
+    if (j < W) buf[j] = __ldg(win + i * W + j);
+  const int32_t p = __ldg(pin + i);
   const int key = keys[i];
   const int r = ranks[i];  // rank of the record in its cell
   const int64_t c0 = (int64_t)(key >> 6) * 64;
@@ -89,8 +97,11 @@ __global__ void __launch_bounds__(256) k_scatter(const uint64_t* __restrict__ wi
     v = nv;
   }
   const int64_t dst = b0 + t;
-  for (int j = 0; j < W; ++j) wout[dst * W + j] = win[i * W + j];
-  pout[dst] = pin[i];
+#pragma unroll
+  for (int j = 0; j < WB; ++j)
+    if (j < W) wout[dst * W + j] = buf[j];
+  for (int j = WB; j < W; ++j) wout[dst * W + j] = win[i * W + j];
+  pout[dst] = p;
 }
 
 // One work item per occupied cell block: (block, first record, count),
