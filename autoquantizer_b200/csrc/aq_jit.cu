@@ -115,8 +115,10 @@ void fmt_f64(std::string& s, double v) {
 std::string jit_layout_source(const aq_layout& L) {
   std::string s;
   char b[256];
-  snprintf(b, sizeof b, "struct JitLayout {\n  static constexpr bool kRegRecord = true;\n  static constexpr int kWords = %d;\n",
-           L.n_words);
+  snprintf(b, sizeof b,
+           "struct JitLayout {\n  static constexpr bool kRegRecord = %s;\n  static constexpr int kWords = %d;\n"
+           "  static constexpr int kMinBlocks = %d;\n",
+           jit_reg_record(L) ? "true" : "false", L.n_words, jit_reg_record(L) ? kJitRegRecordMinBlocks : kJitSlotMinBlocks);
   s += b;
   s += "  static __device__ __forceinline__ aq_layout get(const aq_layout&) {\n    return aq_layout{";
   snprintf(b, sizeof b, "%d, %d, %d, %d, %d, %d, {0, 0}, {", L.n_slots, L.n_words, L.total_bits, L.compute_f64,
@@ -183,7 +185,7 @@ void* jit_k_step(int D, bool HF, bool HM, bool f64, bool col, const aq_layout& L
   }
   g_nv.add_name(prog, name);
   // AQ_JIT_DEFINES (environment): extra -D options, e.g.
-  // "AQ_STEP_MIN_BLOCKS(R)=4", separated by spaces (tuning experiments)
+  // "AQ_STEP_MIN_BLOCKS(R,LA)=4", separated by spaces (tuning experiments)
   std::vector<std::string> extra;
   if (const char* e = getenv("AQ_JIT_DEFINES")) {
     std::string s(e), tok;

@@ -56,11 +56,12 @@ namespace aq {
 #endif
 constexpr int CH = AQ_CH;  // particles per work item = threads per CTA
 constexpr int NWARP = CH / 32;
-// CTAs per SM the register allocation of k_step must allow: 6 (80
-// registers) for float, where more resident warps beat the extra spills and
-// 6 CTAs' shared memory still fits; 4 (128 registers) for double
+// CTAs per SM the register allocation of k_step must allow: the layout's
+// choice (LA::kMinBlocks) for float, 4 (128 registers) for double.  Short
+// records kept in registers run best at 6 CTAs (80 registers: more
+// resident warps beat the extra spills); records in shared-memory slots at 4.
 #ifndef AQ_STEP_MIN_BLOCKS
-#define AQ_STEP_MIN_BLOCKS(R) (sizeof(R) == 8 ? 512 / AQ_CH : 768 / AQ_CH)
+#define AQ_STEP_MIN_BLOCKS(R, LA) (sizeof(R) == 8 ? 512 / AQ_CH : LA::kMinBlocks)
 #endif
 
 template <int D>
@@ -138,6 +139,7 @@ struct StepArgs {
 struct RtLayout {
   static constexpr bool kRegRecord = false;  // records pass through shared memory (runtime word count)
   static constexpr int kWords = 1;
+  static constexpr int kMinBlocks = 512 / AQ_CH;
   static __device__ __forceinline__ const aq_layout& get(const aq_layout& p) { return p; }
 };
 
@@ -375,7 +377,7 @@ __device__ __forceinline__ void bspline(const R* x, const SimK<R>& K, int* base,
 // COL: compiled with the SDF collider (the library's own build always is;
 // the layout-specialized build only when a collider is set).
 template <int D, bool HF, bool HM, class R, class LA, bool COL = true>
-__global__ void __launch_bounds__(CH, AQ_STEP_MIN_BLOCKS(R)) k_step(const __grid_constant__ aq_layout Lp, const SimK<R> K,
+__global__ void __launch_bounds__(CH, AQ_STEP_MIN_BLOCKS(R, LA)) k_step(const __grid_constant__ aq_layout Lp, const SimK<R> K,
                                                 const StepArgs A) {
   typedef Sch<D, HF, HM> S;
   typedef Geo<D> G;
@@ -400,8 +402,8 @@ __global__ void __launch_bounds__(CH, AQ_STEP_MIN_BLOCKS(R)) k_step(const __grid
   R4* gout = reinterpret_cast<R4*>(A.grid_out);
   unsigned fl = 0, nfall = 0;
   // the thread's record words: registers when the layout (and so the word
-  // count and every bit offset) is a compile-time constant, else a slot of
-  // shared memory
+  // count and every bit offset) is a compile-time constant and the record
+  // short, else a slot of shared memory
   uint64_t rrec[LA::kRegRecord ? LA::kWords : 1];
   uint64_t* const myrec = LA::kRegRecord ? rrec : srec + tid * WS;
   R4 zero4;

@@ -428,7 +428,7 @@ struct SimImpl final : SimBase {
   }
 
   int setup_kernel(bool col) override {
-    return setup_step_kernel<D, HF, HM, R>(s, smem_bytes(true), smem_bytes(false), col);
+    return setup_step_kernel<D, HF, HM, R>(s, smem_bytes(jit_reg_record(s->L)), smem_bytes(false), col);
   }
 
   void set_collider(const aq_sim* c) override {
@@ -611,7 +611,7 @@ static int make_impl(aq_sim* s) {
   s->impl = im;
   const size_t smem = im->smem_bytes(false);
   if (smem > 227 * 1024) return AQ_E_LIMIT;
-  return setup_step_kernel<D, HF, HM, R>(s, im->smem_bytes(true), smem, false);
+  return setup_step_kernel<D, HF, HM, R>(s, im->smem_bytes(jit_reg_record(s->L)), smem, false);
 }
 
 template <int D, class R>
