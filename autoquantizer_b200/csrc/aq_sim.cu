@@ -54,54 +54,69 @@ __global__ void __launch_bounds__(256) k_bin(const __grid_constant__ aq_layout L
   if (fl) atomicOr(status, fl);
 }
 
-// Move record i to its sorted position.  A block's records are ordered
+// Move every record to its sorted position.  A block's records are ordered
 // slot-major over the whole block: first the first record of every cell of
 // the block (in cell order), then the second record of every cell, and so
 // on.  k_step's warps take this sequence 32 records at a time, so the lanes
 // of a warp are in different cells except where a slot holds fewer than 32
-// cells.
-__global__ void __launch_bounds__(256) k_scatter(const uint64_t* __restrict__ win, const int32_t* __restrict__ pin,
-                                                 uint64_t* __restrict__ wout, int32_t* __restrict__ pout,
-                                                 const int32_t* __restrict__ keys, const int32_t* __restrict__ ranks,
-                                                 const int32_t* __restrict__ start, int64_t n, int W) {
-  const int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
-  if (i >= n) return;
-  // the record's words are loaded first, all at once: they do not depend on
-  // the destination, so their latency overlaps the offset computation
-  constexpr int WB = 8;
-  uint64_t buf[WB];
-#pragma unroll
-  for (int j = 0; j < WB; ++j)
-    if (j < W) buf[j] = __ldg(win + i * W + j);
-  const int32_t p = __ldg(pin + i);
-  const int key = keys[i];
-  const int r = ranks[i];  // rank of the record in its cell
-  const int64_t c0 = (int64_t)(key >> 6) * 64;
-  const int myc = key & 63;
-  // records before this one: min(count, r) of every cell, plus one more for
-  // every earlier cell that has an r-th record.  The block's 65 offsets are
-  // read as int4 vectors (start is 256-byte aligned, c0 a multiple of 64).
-  const int4* st4 = reinterpret_cast<const int4*>(start + c0);
-  int4 v = __ldg(st4);
-  const int64_t b0 = v.x;
-  int t = 0;
+// cells.  A warp moves 32 consecutive records: it reads their words
+// (contiguous) with coalesced loads into shared memory, computes each
+// record's destination, then writes the words record by record from
+// consecutive lanes, so both sides move whole sectors.
+constexpr int SCATTER_T = 128;
+
+__global__ void __launch_bounds__(SCATTER_T) k_scatter(const uint64_t* __restrict__ win,
+                                                       const int32_t* __restrict__ pin, uint64_t* __restrict__ wout,
+                                                       int32_t* __restrict__ pout, const int32_t* __restrict__ keys,
+                                                       const int32_t* __restrict__ ranks,
+                                                       const int32_t* __restrict__ start, int64_t n, int W) {
+  extern __shared__ uint64_t sh_rec[];  // (SCATTER_T / 32) warps x 32 records x W words
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  const int64_t i0 = (int64_t)blockIdx.x * SCATTER_T + warp * 32;
+  if (i0 >= n) return;
+  const int cnt = (int)(n - i0 < 32 ? n - i0 : 32);
+  const int nw = cnt * W;
+  uint64_t* ws = sh_rec + (size_t)warp * 32 * W;
+  const uint64_t* src = win + i0 * W;
+  for (int k = lane; k < nw; k += 32) ws[k] = __ldg(src + k);
+  int64_t dst = 0;
+  int32_t p = 0;
+  if (lane < cnt) {
+    const int64_t i = i0 + lane;
+    p = __ldg(pin + i);
+    const int key = keys[i];
+    const int rk = ranks[i];  // rank of the record in its cell
+    const int64_t c0 = (int64_t)(key >> 6) * 64;
+    const int myc = key & 63;
+    // records before this one: min(count, rk) of every cell, plus one more
+    // for every earlier cell that has an rk-th record.  The block's 65
+    // offsets are read as int4 vectors (start is 256-byte aligned, c0 a
+    // multiple of 64).
+    const int4* st4 = reinterpret_cast<const int4*>(start + c0);
+    int4 v = __ldg(st4);
+    const int64_t b0 = v.x;
+    int t = 0;
 #pragma unroll 4
-  for (int q = 0; q < 16; ++q) {
-    const int4 nv = q < 15 ? __ldg(st4 + q + 1) : make_int4(__ldg(start + c0 + 64), 0, 0, 0);
-    const int ss[5] = {v.x, v.y, v.z, v.w, nv.x};
+    for (int q = 0; q < 16; ++q) {
+      const int4 nv = q < 15 ? __ldg(st4 + q + 1) : make_int4(__ldg(start + c0 + 64), 0, 0, 0);
+      const int ss[5] = {v.x, v.y, v.z, v.w, nv.x};
 #pragma unroll
-    for (int j = 0; j < 4; ++j) {
-      const int k = 4 * q + j, nk = ss[j + 1] - ss[j];
-      t += min(nk, r) + ((k < myc && nk > r) ? 1 : 0);
+      for (int j = 0; j < 4; ++j) {
+        const int k = 4 * q + j, nk = ss[j + 1] - ss[j];
+        t += min(nk, rk) + ((k < myc && nk > rk) ? 1 : 0);
+      }
+      v = nv;
     }
-    v = nv;
+    dst = b0 + t;
   }
-  const int64_t dst = b0 + t;
-#pragma unroll
-  for (int j = 0; j < WB; ++j)
-    if (j < W) wout[dst * W + j] = buf[j];
-  for (int j = WB; j < W; ++j) wout[dst * W + j] = win[i * W + j];
-  pout[dst] = p;
+  __syncwarp();
+  for (int b = 0; b < nw; b += 32) {  // uniform trip count: the shuffle needs every lane
+    const int k = b + lane;
+    const int r = min(k / W, 31);
+    const int64_t d = __shfl_sync(0xffffffffu, dst, r);
+    if (k < nw) wout[d * W + (k - r * W)] = ws[k];
+  }
+  if (lane < cnt) pout[dst] = p;
 }
 
 // One work item per occupied cell block: (block, first record, count),
@@ -465,7 +480,7 @@ struct SimImpl final : SimBase {
     k_scan_top<<<1, SCAN_T, 0, st>>>(S_->scan_sums, nt, S_->cell_start, S_->nkeys);
     k_scan_apply<<<nt, SCAN_T, 0, st>>>(S_->cell_count, S_->nkeys, S_->scan_sums, S_->cell_start);
     const int nxt = 1 - S_->cur;
-    k_scatter<<<grid_for(n, 256), 256, 0, st>>>(S_->words[S_->cur], S_->pid[S_->cur], S_->words[nxt], S_->pid[nxt],
+    k_scatter<<<grid_for(n, SCATTER_T), SCATTER_T, sizeof(uint64_t) * SCATTER_T * S_->W, st>>>(S_->words[S_->cur], S_->pid[S_->cur], S_->words[nxt], S_->pid[nxt],
                                                 S_->keys, S_->ranks, S_->cell_start, n, S_->W);
     k_items_count<<<grid_for(S_->nblk, 256), 256, 0, st>>>(S_->cell_start, S_->nblk, S_->n_items);
     k_items<<<grid_for(S_->nblk, 256), 256, 0, st>>>(S_->cell_start, S_->nblk, S_->items, S_->n_items);
