@@ -8,7 +8,7 @@ weights, fp32 accumulation; libaq aq_mlp_* kernels for inference, backward
 and Adam) predicts the log10 sensitivities of 12 field groups from cheap
 statistics of a 16-substep forward window, so a scheme can be derived without
 a backward run; the adjoint (adjoint.py) produces the training labels and
-remains the fallback and the judge of the surrogate's error.
+remains the fallback and the yardstick for the surrogate's error.
 
 Field groups: x_0..2, v_0..2, rows 0..2 of C, rows 0..2 of F (J in row 0 for
 fluids); 2D scenes leave the third entries empty (masked).
