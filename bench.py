@@ -317,6 +317,7 @@ def run_ours(args, ws, rank, local):
     cfg32, _ = scenes.mixed_boxes_3d(seed=rank, quantized=False)
     f = MPMSolver(cfg32)
     f.set_particles(vals)
+    S32 = f.bytes_per_particle()
     f.substeps(W)
     ms32, _ = timed(f, K)
     value32, ms32 = job_rate(n * K, ms32, ws)
@@ -375,7 +376,8 @@ def run_ours(args, ws, rank, local):
             "ms_per_step": ms / K, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
             "dtype": "f32", "data": "synthetic (numpy default_rng seeded scene)",
             "config": {"workload": WORKLOAD, "record_bits": q.layout().total_bits, "bytes_per_particle": S,
-                       "fp32_bytes_per_particle": 4 * 24, "particles_per_gpu": n, "grid": [128, 128, 128],
+                       "fp32_bytes_per_particle": 4 * 24, "fp32_record_bytes": S32, "particles_per_gpu": n,
+                       "grid": [128, 128, 128],
                        "l2": "inputs larger than L2 (117 MB records + 67 MB grids), no flush",
                        "parallelism": "replicas" if ws > 1 else "single"},
             "fp32_state": {"value": value32, "unit": UNIT, "ms_per_step": ms32 / K,
