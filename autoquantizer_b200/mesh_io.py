@@ -107,6 +107,10 @@ def read_ply(fn):
             off += n * dt.itemsize
             out[name] = {p[0]: rec[p[0]].astype(p[1]) for p in props}
             continue
+        fast = _fixed_lists(data, off, n, props, end)
+        if fast is not None:  # every list of the element has the same length
+            out[name], off = fast
+            continue
         cols = {p[0]: [] for p in props}
         for _ in range(n):
             for pname, t, it in props:
@@ -122,6 +126,32 @@ def read_ply(fn):
         out[name] = {p[0]: (np.array(cols[p[0]], dtype=p[1]) if p[2] is None else _lists(cols[p[0]]))
                      for p in props}
     return out
+
+
+def _fixed_lists(data, off, n, props, end):
+    """Vectorized read of an element whose lists all have the length of the
+    first record's (triangle faces): ({name: array}, new offset), or None."""
+    if n == 0:
+        return {p[0]: np.zeros((0,), dtype=p[1]) if p[2] is None else np.zeros((0, 0), dtype=p[2])
+                for p in props}, off
+    fields, pos = [], off
+    for pname, t, it in props:  # list lengths from the first record
+        if it is None:
+            fields.append((pname, end + t))
+            pos += np.dtype(t).itemsize
+        else:
+            k = int(np.frombuffer(data, dtype=end + t, count=1, offset=pos)[0])
+            fields.append(("_n_" + pname, end + t))
+            fields.append((pname, end + it, (k,)))
+            pos += np.dtype(t).itemsize + k * np.dtype(it).itemsize
+    dt = np.dtype(fields)
+    if off + n * dt.itemsize > len(data):
+        return None
+    rec = np.frombuffer(data, dtype=dt, count=n, offset=off)
+    for pname, t, it in props:
+        if it is not None and not np.all(rec["_n_" + pname] == dt[pname].shape[0]):
+            return None
+    return {p[0]: rec[p[0]].astype(p[1] if p[2] is None else p[2]) for p in props}, off + n * dt.itemsize
 
 
 def _lists(v):

@@ -364,8 +364,12 @@ class MPMSolver:
         (u + (i, j, k)) dx + translation with the given velocity.  dx is the
         simulation grid's spacing, not the voxel's, as in the reference.
         Particles are appended in voxel order (row-major), then sample."""
+        import torch
+
         vox = self._voxelizer().voxels
-        idx = np.argwhere(vox.cpu().numpy() > 0).astype(np.float64)
+        # inside voxels in row-major order, found on the device (the voxel
+        # grid is up to 2 x 2^k per axis; only the indices come back)
+        idx = torch.nonzero(vox > 0).cpu().numpy().astype(np.float64)
         k = int(sample_density) + 1
         rng = self._rng(3)
         x = (rng.random((len(idx), k, 3)) + idx[:, None, :]) * self.dx

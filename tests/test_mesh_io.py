@@ -76,3 +76,27 @@ def test_not_a_ply(tmp_path):
     open(fn, "wb").write(b"solid cube\n")
     with pytest.raises(ValueError):
         M.read_ply(fn)
+
+
+def test_ragged_faces_and_large_meshes(tmp_path):
+    fn = str(tmp_path / "mixed.ply")
+    v = np.arange(15, dtype="<f4").reshape(5, 3)
+    head = ("ply\nformat binary_little_endian 1.0\nelement vertex 5\nproperty float x\nproperty float y\n"
+            "property float z\nelement face 2\nproperty list uchar int vertex_indices\nend_header\n").encode()
+    body = v.tobytes() + np.uint8(3).tobytes() + np.array([0, 1, 2], "<i4").tobytes() + \
+        np.uint8(4).tobytes() + np.array([1, 2, 3, 4], "<i4").tobytes()
+    open(fn, "wb").write(head + body)
+    faces = M.read_ply(fn)["face"]["vertex_indices"]
+    assert [f.tolist() for f in faces] == [[0, 1, 2], [1, 2, 3, 4]]
+    with pytest.raises(ValueError):
+        M.load_mesh(fn)
+    # 200k triangles read through the vectorized path
+    n = 200000
+    rng = np.random.default_rng(1)
+    f = rng.integers(0, 5, (n, 3)).astype("<i4")
+    rec = np.zeros(n, dtype=[("n", "u1"), ("i", "<i4", (3,))])
+    rec["n"], rec["i"] = 3, f
+    head = head.replace(b"element face 2", b"element face %d" % n)
+    open(fn, "wb").write(head + v.tobytes() + rec.tobytes())
+    tri = M.load_mesh(fn)
+    assert tri.shape == (n, 9) and np.array_equal(tri.reshape(n, 3, 3), v[f])
