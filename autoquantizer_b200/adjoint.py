@@ -67,6 +67,17 @@ class Adjoint:
         self.sens = np.array(sens[:])
         return g0, self.sens
 
+    def set_collider(self, sdf, normal, offset, center, theta=0.0, height=0.0, omega=5.0, height_rate=0.1):
+        """The rotating SDF collider in every substep (aq_adjoint_set_collider):
+        sdf and normal are float32 CUDA tensors ([a, b, c] and [a, b, c, 3])
+        kept alive here; theta and height are the values at substep 0."""
+        self._col = (sdf, normal)
+        dims = (C.c_int32 * 3)(*sdf.shape)
+        off = (C.c_int32 * 3)(*offset)
+        _lib.check(_lib.lib().aq_adjoint_set_collider(self._h, C.c_void_p(sdf.data_ptr()), C.c_void_p(normal.data_ptr()),
+                                                      dims, off, int(center), float(theta), float(height),
+                                                      float(omega), float(height_rate)), "aq_adjoint_set_collider")
+
     def close(self):
         if self._h:
             _lib.lib().aq_adjoint_destroy(self._h)

@@ -52,6 +52,13 @@ struct AdK {
   double lb[3], ub[3];
   int bound_clip, friction;
   R clip_lo[3], clip_hi[3];
+  // rotating SDF collider (3D; col_on = 0: none), the fields collider_at
+  // reads; col_c, col_s, col_yshift are this substep's angle and height
+  int col_on, col_n, col_dims[3], col_off[3], col_lo[3], col_hi[3];
+  const float* col_sdf;
+  const float* col_nrm;
+  R col_omega, col_c, col_s;
+  int col_yshift;
 };
 
 template <int D>
@@ -290,6 +297,7 @@ __global__ void __launch_bounds__(256) k_ad_grid(const AdK<R> K, const R* __rest
 #pragma unroll
   for (int k = 0; k < D; ++k)
     if (ad_wall<R>(K, I, k, v[k])) v[k] = 0;
+  if (D == 3 && K.col_on) collide_node<R, true>(K, I[0], I[1], I[2], v);  // sdf_collision_no_arg
 #pragma unroll
   for (int d = 0; d < 3; ++d) gv[4 * c + d] = d < D ? v[d] : (R)0;
   gv[4 * c + 3] = 0;
@@ -492,13 +500,34 @@ __global__ void __launch_bounds__(256) k_ad_grid_bwd(const AdK<R> K, const R* __
 #pragma unroll
   for (int d = 0; d < D; ++d) v[d] = inv_m * g[1 + d];
   v[1] -= K.dt * K.grav;
+  R vb[3] = {0, 0, 0};
+#pragma unroll
+  for (int d = 0; d < D; ++d) vb[d] = gvb[4 * c + d];
+  if (D == 3 && K.col_on) {
+    // collider^T: where the node is inside and moving into the surface
+    // (relative to the collider), the forward removed the normal part of
+    // the velocity, v' = v - ((v - cv).n) n, so vbar' = vbar - (vbar.n) n
+    R nrm[3], cv[3];
+    if (collider_at<R, true>(K, I[0], I[1], I[2], nrm, cv)) {
+      R dn = 0, bn = 0;
+#pragma unroll
+      for (int k = 0; k < 3; ++k) {
+        const R vw = ad_wall<R>(K, I, k, v[k]) ? (R)0 : v[k];  // the collider's input
+        dn += (vw - cv[k]) * nrm[k];
+        bn += vb[k] * nrm[k];
+      }
+      if (dn < (R)0)
+#pragma unroll
+        for (int k = 0; k < 3; ++k) vb[k] -= bn * nrm[k];
+    }
+  }
   R mb = 0, Pb[3] = {0, 0, 0};
 #pragma unroll
   for (int d = 0; d < D; ++d) {
-    R vb = gvb[4 * c + d];
-    if (ad_wall<R>(K, I, d, v[d])) vb = 0;
-    Pb[d] = vb * inv_m;
-    mb -= vb * g[1 + d] * inv_m * inv_m;
+    R b = vb[d];
+    if (ad_wall<R>(K, I, d, v[d])) b = 0;
+    Pb[d] = b * inv_m;
+    mb -= b * g[1 + d] * inv_m * inv_m;
   }
   gvb[4 * c + 0] = mb;
 #pragma unroll
@@ -589,8 +618,9 @@ __global__ void k_ad_accum(const R* __restrict__ ab, int64_t n, int ns, double* 
 
 struct AdBase {
   virtual ~AdBase() {}
-  virtual int step(const void* in, void* out, cudaStream_t st) = 0;
-  virtual int step_bwd(const void* s_in, const void* ab_out, void* ab_in, cudaStream_t st) = 0;
+  // t: index of the substep (the collider's angle and height depend on it)
+  virtual int step(const void* in, void* out, int t, cudaStream_t st) = 0;
+  virtual int step_bwd(const void* s_in, const void* ab_out, void* ab_in, int t, cudaStream_t st) = 0;
   virtual int accum(const void* ab, double* sens, cudaStream_t st) = 0;
 };
 
@@ -609,6 +639,13 @@ struct aq_adjoint {
   int T = 0, every = 0;
   double* dsens = nullptr;
   aq::AdBase* impl = nullptr;
+  // SDF collider (aq_adjoint_set_collider): caller-owned volumes; at
+  // substep t the angle is theta + omega dt t and the height
+  // height + rate dt t (step_collider_difftaichi, mpm_solver.py:1554-1559)
+  int col_on = 0, col_center = 0, col_dims[3] = {0, 0, 0}, col_off[3] = {0, 0, 0};
+  const float* col_sdf = nullptr;
+  const float* col_nrm = nullptr;
+  double col_theta = 0, col_height = 0, col_omega = 0, col_rate = 0;
 };
 
 namespace aq {
@@ -639,7 +676,27 @@ struct AdImpl final : AdBase {
     K.mu = (R)P.mat[0].mu;
     K.lam = (R)P.mat[0].lam;
   }
-  int step(const void* in, void* out, cudaStream_t st) override {
+  void set_substep(int t) {
+    K.col_on = a->col_on;
+    if (!K.col_on) return;
+    K.col_n = a->col_center;
+    for (int d = 0; d < 3; ++d) {
+      K.col_dims[d] = a->col_dims[d];
+      K.col_off[d] = a->col_off[d];
+      K.col_lo[d] = (int)a->P.lb[d];
+      K.col_hi[d] = (int)a->P.ub[d];
+    }
+    K.col_sdf = a->col_sdf;
+    K.col_nrm = a->col_nrm;
+    K.col_omega = (R)a->col_omega;
+    const double th = a->col_theta + a->col_omega * a->P.dt * t;
+    const double h = a->col_height + a->col_rate * a->P.dt * t;
+    K.col_c = (R)cos(th);
+    K.col_s = (R)sin(th);
+    K.col_yshift = (int)(h / a->P.dx + 0.5);
+  }
+  int step(const void* in, void* out, int t, cudaStream_t st) override {
+    set_substep(t);
     const size_t gbytes = sizeof(R) * 4 * a->ncell;
     AQ_CUDA_TRY(cudaMemsetAsync(a->grid, 0, gbytes, st));
     k_ad_p2g<D, HF, R><<<grid_for(a->n, 128), 128, 0, st>>>(K, (const R*)in, a->n, (R*)a->grid);
@@ -648,7 +705,8 @@ struct AdImpl final : AdBase {
     AQ_CUDA_TRY(cudaGetLastError());
     return AQ_OK;
   }
-  int step_bwd(const void* s_in, const void* ab_out, void* ab_in, cudaStream_t st) override {
+  int step_bwd(const void* s_in, const void* ab_out, void* ab_in, int t, cudaStream_t st) override {
+    set_substep(t);
     const size_t gbytes = sizeof(R) * 4 * a->ncell;
     // recompute the grid of this substep
     AQ_CUDA_TRY(cudaMemsetAsync(a->grid, 0, gbytes, st));
@@ -739,6 +797,32 @@ int aq_adjoint_create(const aq_params* P, aq_adjoint** out) {
   return AQ_OK;
 }
 
+int aq_adjoint_set_collider(aq_adjoint* a, const float* d_sdf, const float* d_normal, const int32_t* dims,
+                            const int32_t* offset, int32_t center, double theta, double height, double omega,
+                            double height_rate) {
+  if (!a) return AQ_E_ARG;
+  if (!d_sdf) {
+    a->col_on = 0;
+    return AQ_OK;
+  }
+  if (a->D != 3 || !d_normal || !dims || !offset) return AQ_E_ARG;
+  for (int k = 0; k < 3; ++k)
+    if (dims[k] < 1) return AQ_E_ARG;
+  a->col_on = 1;
+  a->col_center = center;
+  a->col_sdf = d_sdf;
+  a->col_nrm = d_normal;
+  for (int k = 0; k < 3; ++k) {
+    a->col_dims[k] = dims[k];
+    a->col_off[k] = offset[k];
+  }
+  a->col_theta = theta;
+  a->col_height = height;
+  a->col_omega = omega;
+  a->col_rate = height_rate;
+  return AQ_OK;
+}
+
 int aq_adjoint_destroy(aq_adjoint* a) {
   if (!a) return AQ_E_ARG;
   cudaDeviceSynchronize();
@@ -766,7 +850,7 @@ int aq_adjoint_forward(aq_adjoint* a, const void* d_s0, int32_t n_substeps, int3
   int cur = 0;
   for (int t = 0; t < n_substeps; ++t) {
     if (t % every == 0) AQ_CUDA_TRY(cudaMemcpyAsync(a->ckpt[t / every], a->seg[cur], sbytes, cudaMemcpyDeviceToDevice, st));
-    const int rc = a->impl->step(a->seg[cur], a->seg[1 - cur], st);
+    const int rc = a->impl->step(a->seg[cur], a->seg[1 - cur], t, st);
     if (rc) return rc;
     cur = 1 - cur;
   }
@@ -789,11 +873,11 @@ int aq_adjoint_backward(aq_adjoint* a, const void* d_seed, void* d_grad_s0, doub
     const int t0 = sgi * every, t1 = std::min(T, t0 + every);
     AQ_CUDA_TRY(cudaMemcpyAsync(a->seg[0], a->ckpt[sgi], sbytes, cudaMemcpyDeviceToDevice, st));
     for (int t = t0; t < t1 - 1; ++t) {
-      const int rc = a->impl->step(a->seg[t - t0], a->seg[t - t0 + 1], st);
+      const int rc = a->impl->step(a->seg[t - t0], a->seg[t - t0 + 1], t, st);
       if (rc) return rc;
     }
     for (int t = t1 - 1; t >= t0; --t) {
-      const int rc = a->impl->step_bwd(a->seg[t - t0], ab[cur], ab[1 - cur], st);
+      const int rc = a->impl->step_bwd(a->seg[t - t0], ab[cur], ab[1 - cur], t, st);
       if (rc) return rc;
       cur = 1 - cur;  // ab[cur] = adjoint of state t
       if (t >= 1) {

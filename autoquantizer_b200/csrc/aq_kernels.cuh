@@ -216,8 +216,13 @@ __device__ __forceinline__ double sub_rn(double a, double b) { return __dsub_rn(
 // signed distance there is below -1e-5 the velocity relative to the
 // collider (omega x r, r = (rotated index - (n, I1, n)) dx) loses its
 // component into the surface along the rotated normal.
-template <class R>
-__device__ __forceinline__ void collide_node(const SimK<R>& K, int I0, int I1, int I2, R (&v)[3]) {
+// KT: any parameter block with the collider fields (SimK, the adjoint's AdK).
+// Returns whether node I is inside the collider, and there the rotated
+// normal and the collider's velocity omega x r: r from the rotated index
+// (sdf_collision) or, with NODE_CV, from the node itself
+// (sdf_collision_no_arg, mpm_solver.py:1510, the reference's autodiff path).
+template <class R, bool NODE_CV = false, class KT>
+__device__ __forceinline__ bool collider_at(const KT& K, int I0, int I1, int I2, R (&nrm)[3], R (&cv)[3]) {
   const int n = K.col_n;
   const int i0 = I0 >= 2 * n ? I0 - 2 * n : I0, i2 = I2 >= 2 * n ? I2 - 2 * n : I2;
   const R c = K.col_c, s = K.col_s;
@@ -230,13 +235,24 @@ __device__ __forceinline__ void collide_node(const SimK<R>& K, int I0, int I1, i
 #pragma unroll
   for (int k = 0; k < 3; ++k) r[k] = max(min(r[k], K.col_hi[k]), K.col_lo[k]);
   const int a = r[0] - K.col_off[0], b = r[1] - K.col_off[1], e = r[2] - K.col_off[2];
-  if (a < 0 || a >= K.col_dims[0] || b < 0 || b >= K.col_dims[1] || e < 0 || e >= K.col_dims[2]) return;
+  if (a < 0 || a >= K.col_dims[0] || b < 0 || b >= K.col_dims[1] || e < 0 || e >= K.col_dims[2]) return false;
   const int64_t q = ((int64_t)a * K.col_dims[1] + b) * K.col_dims[2] + e;
-  if (!(K.col_sdf[q] < -1e-5f)) return;
+  if (!(K.col_sdf[q] < -1e-5f)) return false;
   const R g0 = (R)K.col_nrm[3 * q], g1 = (R)K.col_nrm[3 * q + 1], g2 = (R)K.col_nrm[3 * q + 2];
-  const R nrm[3] = {c * g0 + s * g2, g1, -s * g0 + c * g2};
-  const R rx = (R)(r[0] - n) * K.dx, rz = (R)(r[2] - n) * K.dx;
-  const R cv[3] = {K.col_omega * rz, (R)0, -K.col_omega * rx};
+  nrm[0] = c * g0 + s * g2;
+  nrm[1] = g1;
+  nrm[2] = -s * g0 + c * g2;
+  const R rx = (R)((NODE_CV ? I0 : r[0]) - n) * K.dx, rz = (R)((NODE_CV ? I2 : r[2]) - n) * K.dx;
+  cv[0] = K.col_omega * rz;
+  cv[1] = (R)0;
+  cv[2] = -K.col_omega * rx;
+  return true;
+}
+
+template <class R, bool NODE_CV = false, class KT>
+__device__ __forceinline__ void collide_node(const KT& K, int I0, int I1, int I2, R (&v)[3]) {
+  R nrm[3], cv[3];
+  if (!collider_at<R, NODE_CV>(K, I0, I1, I2, nrm, cv)) return;
   R vr[3], dn = 0;
 #pragma unroll
   for (int k = 0; k < 3; ++k) {

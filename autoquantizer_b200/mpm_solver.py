@@ -722,14 +722,16 @@ class MPMSolver:
 
         from .adjoint import Adjoint, ek_loss, ek_seed
 
-        if self._col is not None:
-            raise NotImplementedError("the adjoint has no SDF collider (sdf_collision_no_arg.grad)")
         if self.has_mat:
             raise ValueError("the adjoint runs single-material scenes")
         self._pull()
         P = self._params()
         n, ns = self.current_idx, self.n_slots()
         adj = Adjoint(P)
+        if self._col is not None:  # from the collider's current angle and height
+            c = self._col
+            th, hh = self.collider_state()
+            adj.set_collider(c["sdf"], c["normal"], c["offset"], int(self.n_grid), th, hh, c["omega"], c["rate"])
         dt = torch.float64 if self.param.precision == "f64" else torch.float32
         if self._dev is not None and self._host is None:
             s0 = self._dev[:n, :ns].to(dt).contiguous()

@@ -291,6 +291,15 @@ int aq_state_error(const void* d_a, int32_t a_f64, const void* d_b, int32_t b_f6
 typedef struct aq_adjoint aq_adjoint;
 int aq_adjoint_create(const aq_params* h_params, aq_adjoint** out);
 int aq_adjoint_destroy(aq_adjoint* adj);
+/* The rotating SDF collider in the adjoint's substeps (sdf_collision_no_arg
+ * and its gradient in the reference's autodiff runs, mpm_solver.py:1491-1516,
+ * 1189-1190): same volumes and arguments as aq_sim_set_collider; at substep
+ * t the angle is theta + omega dt t and the height height + height_rate dt t
+ * (step_collider_difftaichi, :1554-1559).  d_sdf null switches it off.
+ * 3D only. */
+int aq_adjoint_set_collider(aq_adjoint* adj, const float* d_sdf, const float* d_normal, const int32_t* dims,
+                            const int32_t* offset, int32_t center, double theta, double height, double omega,
+                            double height_rate);
 /* Run n_substeps from d_s0, keeping checkpoints; d_sT receives the final
  * state. */
 int aq_adjoint_forward(aq_adjoint* adj, const void* d_s0, int32_t n_substeps, int32_t every, void* d_sT,
