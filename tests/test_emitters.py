@@ -107,3 +107,36 @@ def test_emitters_refuse_overflow():
     s.initialize()
     with pytest.raises(ValueError):
         s.add_cube((0.1, 0.1, 0.1), (0.1, 0.1, 0.1), 101)
+
+
+@pytest.mark.parametrize("theta", [0.0, np.pi / 2])
+def test_add_cube_pushes_particles_out_of_the_rotated_collider(theta):
+    """fill_in_box with the collider (mpm_solver.py:1582-1588) on the host:
+    a bar along x (cells y 8..11, z 28..35) rotated by theta about
+    (32, ., 32); particles whose cell the rotated bar covers move up by 2..5
+    cells along the stored normal, the others stay."""
+    import torch
+
+    cfg, _ = scenes.falling_block_3d(n=20000, n_grid=32)
+    cfg.grid_res, cfg.ub = [64, 32, 64], [61, 29, 61]
+    s = MPMSolver(cfg)
+    s.initialize()
+    sdf = np.full((64, 32, 64), 0.02, dtype=np.float32)
+    sdf[:, 8:12, 28:36] = -0.01
+    normal = np.zeros((64, 32, 64, 3), dtype=np.float32)
+    normal[..., 1] = 1.0
+    # the collider's volumes as host tensors: add_cube reads them on the host
+    s._col = {"sdf": torch.from_numpy(sdf), "normal": torch.from_numpy(normal), "offset": [0, 0, 0],
+              "theta": theta, "height": 0.0, "omega": 5.0, "rate": 0.1}
+    s.add_cube((0.3, 0.2, 0.3), (1.4, 0.3, 1.4), 20000)
+    free = MPMSolver(cfg)
+    free.initialize()
+    free.add_cube((0.3, 0.2, 0.3), (1.4, 0.3, 1.4), 20000)
+    x, x0 = s._staging()[:20000, :3], free._staging()[:20000, :3]
+    cell = (x0 / s.dx + 0.5).astype(int)
+    across = cell[:, 2] if theta == 0.0 else cell[:, 0]  # the bar's cross-section axis
+    inside = (cell[:, 1] >= 8) & (cell[:, 1] < 12) & (across >= 28) & (across < 36)
+    moved = np.any(x != x0, axis=1)
+    assert inside.any() and np.array_equal(moved, inside)
+    dy = (x[moved, 1] - x0[moved, 1]) / s.dx
+    assert np.all((dy >= 2) & (dy <= 5)) and np.all(x[moved][:, [0, 2]] == x0[moved][:, [0, 2]])
