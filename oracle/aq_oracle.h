@@ -17,8 +17,9 @@
  *   substep     mpm_exps/engine/mpm_solver.py:590-758, 1012-1031, 1043-1052
  *   polar 2D    taichi_submission/python/taichi/lang/linalg_impl.py:9-26
  *   collider    mpm_exps/engine/mpm_solver.py:1459-1547 (in aq_oracle_mpm.c)
- *   voxelizer   mpm_exps/engine/voxelizer.py:10-105 (aq_oracle_emit.c; no
- *               reference output to pin it: known-answer meshes in tests/)
+ *   voxelizer   mpm_exps/engine/voxelizer.py:10-105 (aq_oracle_emit.c;
+ *               pinned by the reference's shipped letters emission,
+ *               tests/golden/letters_voxels.npz, and known-answer meshes)
  * Parity of this restatement is pinned by the reference's own quant tests
  * (taichi_submission/tests/python/test_bit_pack*.py, test_dithering.py,
  * test_custom_float*.py, test_fxp_offset.py) ported in tests/.

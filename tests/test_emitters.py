@@ -140,3 +140,24 @@ def test_add_cube_pushes_particles_out_of_the_rotated_collider(theta):
     assert inside.any() and np.array_equal(moved, inside)
     dy = (x[moved, 1] - x0[moved, 1]) / s.dx
     assert np.all((dy >= 2) & (dy <= 5)) and np.all(x[moved][:, [0, 2]] == x0[moved][:, [0, 2]])
+
+
+def _letters():
+    import os
+
+    g = np.load(os.path.join(os.path.dirname(__file__), "golden", "letters_voxels.npz"))
+    res = tuple(int(r) for r in g["res"])
+    mask = np.unpackbits(g["mask_bits"])[: np.prod(res)].reshape(res).astype(bool)
+    return g, mask
+
+
+def test_voxelizer_reproduces_the_reference_letters():
+    """The reference's own emitted letters (mpm_exps/inputs/
+    letters_emit_one_frame.npy: 63,856 particles from auto_quant.ply at a
+    128^3 grid, 2 per inside voxel) occupy exactly the voxels the oracle's
+    voxelizer finds inside the mesh (tests/golden/make_letters_golden.py)."""
+    g, mask = _letters()
+    v = O.voxelize(g["triangles"].astype(np.float64), mask.shape, 1 / 256, 3, 1e-8)
+    assert set(np.unique(v)) <= {0, 1}
+    assert int(mask.sum()) == 31928 and np.array_equal(v > 0, mask)
+    assert int(g["n_particles"]) == 2 * int(mask.sum()) and g["per_voxel"].tolist() == [2]

@@ -128,3 +128,26 @@ def test_run_forward_only_dumps_every_frame(tmp_path):
     s.run_forward_only(save_states=True)
     assert sorted(os.listdir(tmp_path)) == ["data_000000.ply", "data_000001.ply", "data_000002.ply"]
     assert s.launches() > 0
+
+
+def test_reference_letters_on_the_gpu():
+    """The CUDA voxelizer and add_mesh on the reference's letters mesh
+    reproduce the voxels of the reference's shipped emission
+    (tests/golden/letters_voxels.npz, made by make_letters_golden.py)."""
+    from test_emitters import _letters
+
+    g, mask = _letters()
+    tri = g["triangles"]
+    vox = Voxelizer(res=(128, 128, 128), dx=1 / 128, super_sample=2)
+    assert vox.res == mask.shape
+    assert np.array_equal(vox.voxelize(tri).cpu().numpy() > 0, mask)
+    cfg, _ = scenes.falling_block_3d(n=64000, n_grid=128)
+    s = MPMSolver(cfg)
+    s.initialize()
+    t = [float(x) for x in g["translation"]]
+    n = s.add_mesh(tri, sample_density=1, velocity=(0.0, -2.0, 0.0), translation=t)
+    assert n == int(g["n_particles"]) == 63856
+    idx = np.floor((s._staging()[:n, :3] - t) * 128 + 1e-9).astype(int)
+    got = np.zeros_like(mask)
+    got[idx[:, 0], idx[:, 1], idx[:, 2]] = True
+    assert np.array_equal(got, mask)
