@@ -65,7 +65,8 @@ class Experiment:
     f64_data = None  # unquantized loss the error-bound mode measures against
     modes = (CR, EB)
 
-    def config(self):
+    def config(self, kind="forward"):
+        """kind: "ad", "ranges" or "forward" (the drivers' set-ups differ)."""
         raise NotImplementedError
 
     def init(self, mpm):
@@ -82,7 +83,7 @@ class Elastic2D(Experiment):
     file_name = "elastic_2d.npy"
     f64_data = 6893.409
 
-    def config(self):
+    def config(self, kind="forward"):
         c = MPMConfig()
         c.dim = 2
         c.E = 5e1
@@ -132,7 +133,7 @@ class Fluid2D(Experiment):
     file_name = "fluid_2d_t16385_dt0.0002_p10000_g128.npy"
     modes = (CR,)
 
-    def config(self):
+    def config(self, kind="forward"):
         c = MPMConfig()
         c.dim = 2
         c.E = 5e4
@@ -171,13 +172,14 @@ class Fluid2D(Experiment):
 
 
 class FallingBlock3D(Experiment):
-    """The 3D elastic block of the adjoint benchmark, with the scheme recipe
-    of run_mpm_elastic_3d.py:331-341."""
+    """The 3D elastic block of the adjoint benchmark, with the 2D drivers'
+    range recipe (positions range 1 on the unit domain, the other ranges
+    doubled)."""
 
     name = "falling_block_3d"
     file_name = "falling_block_3d.npy"
 
-    def config(self):
+    def config(self, kind="forward"):
         from . import scenes
 
         c, vals = scenes.falling_block_3d()
@@ -205,7 +207,166 @@ class FallingBlock3D(Experiment):
         return bits + 1, ranges
 
 
-EXPERIMENTS = {e.name: e for e in (Elastic2D, Fluid2D, FallingBlock3D)}
+class Letters3D(Experiment):
+    """The 3D elastic letters experiment (run_mpm_elastic_3d.py): config
+    :249-290 (the high-resolution forward run) and, for the gradient and
+    range passes, the low-resolution set-up (use_low_res); scheme :323-333;
+    the letters mesh inputs/auto_quant.ply (load_mesh with scale (0.1, 0.1,
+    2), offset (0.02, 0.02, 0.5), :249), emitted by add_mesh at
+    translation (0.90, 1.6, 0.1) and (2.2, 1.6, 0.1) (add_letters, :45-61).
+    The pipeline emits the first frame's letters only; the reference emits
+    again every emit_step frames."""
+
+    name = "elastic_3d"
+    file_name = "elastic_3d.npy"
+    modes = (CR,)
+    inputs = "inputs"
+
+    def config(self, kind="forward"):
+        c = MPMConfig()
+        c.dim = 3
+        c.E, c.la, c.nu = 5e5, 5e4, 0.2
+        c.g = 9.8 * 2.5
+        c.bound = [3, 3, 3]
+        c.p_rho = 1000.0
+        c.use_fluid = False
+        if kind == "ad":  # use_low_res with default_fp f64 (:240-244, :265-271)
+            c.n_particles = 100 ** 3
+            c.dt = 1e-4
+            c.n_grid = 128
+            c.n_timesteps = 1024 * 16 + 1
+            self.sample_density = 1
+            c.precision = "f64"
+        else:  # high resolution (:272-280); detect_range keeps 500^3 particles, 16k substeps (:307-316)
+            c.n_particles = int(3e8) if kind == "forward" else 500 ** 3
+            c.dt = 7.5e-5
+            c.n_grid = 128 * 2
+            c.n_timesteps = 1024 * 40 + 1 if kind == "forward" else 1024 * 16
+            self.sample_density = 8
+        c.steps = 128
+        c.p_vol = (1 / c.n_grid * 0.5) ** c.dim
+        c.quantized_properties = {"x": 1, "v": 1, "C": 1, "F": 1}
+        c.use_dithering = True
+        c.use_bitpack = True
+        c.use_bound_clip = True
+        c.quant_bits = np.array([32] * 24)
+        c.quant_ranges = np.array([4.0] * 24)
+        c.grid_res = [4 * c.n_grid, 2 * c.n_grid, 2 * c.n_grid]
+        return c
+
+    def mesh(self):
+        from .mesh_io import load_mesh
+
+        return load_mesh(os.path.join(self.inputs, "auto_quant.ply"), scale=(0.1, 0.1, 2), offset=(0.02, 0.02, 0.5))
+
+    def init(self, mpm):
+        mpm.initialize()
+        tri = self.mesh()
+        for t in ((0.90, 1.6, 0.1), (2.2, 1.6, 0.1)):
+            mpm.add_mesh(tri, velocity=(0.0, -4.0, 0.0), translation=t, sample_density=self.sample_density)
+
+    def scheme(self, grads, ranges, mode, eps):
+        if mode != CR:
+            raise ValueError("elastic_3d runs the compression-rate mode only")
+        ranges = np.array(ranges, dtype=np.float64) * 2.0
+        ranges[:3] = 4.0
+        bits, _ = LagrangianCR(np.asarray(grads) * ranges ** 2, r=eps)
+        return bits + 1, ranges
+
+
+class Propeller3D(Experiment):
+    """The 3D fluid-and-propeller experiment (run_mpm_fluid_3d.py): the
+    gradient and range set-up ad_or_ranges :101-146 (1e6 particles, 64
+    grid, domain 2 x 1 x 2, two slabs, collider inputs/propeller_higher*.npz
+    on the autodiff schedule: height rate 0.15), the forward set-up :164-227
+    (4e8 particles, 256 grid, domain 4 x 1 x 4, one slab, collider
+    inputs/propeller_2x2_larger*.npz, height rate 0.1) and the scheme of
+    solve() :149-161 (quantized ranges :203-209)."""
+
+    name = "fluid_3d"
+    file_name = "fluid_3d.npy"
+    modes = (CR,)
+    inputs = "inputs"
+
+    def config(self, kind="forward"):
+        c = MPMConfig()
+        c.dim = 3
+        c.use_fluid = True
+        c.use_friction = False
+        c.p_rho = 1000.0
+        c.la = 5e5
+        c.E = 5e4
+        c.bound = [3, 3, 3]
+        c.quantized_properties = {"x": 1, "v": 1, "C": 1, "J": 1}
+        if kind in ("ad", "ranges"):
+            c.n_particles = 100 ** 3
+            c.dt = 4e-4
+            c.n_grid = 64
+            c.n_timesteps = 1024 * 8 + 1
+            c.p_vol = (1 / c.n_grid) ** 3
+            c.ub = [c.n_grid * 2 - 3, c.n_grid - 3, c.n_grid * 2 - 3]
+            c.grid_res = [2 * c.n_grid, c.n_grid, 2 * c.n_grid]
+            c.precision = "f64" if kind == "ad" else "f32"
+            self.kind = "ad"
+        else:
+            c.n_particles = int(4e8)
+            c.dt = 1e-4
+            c.n_grid = 128 * 2
+            c.n_timesteps = 1024 * 32 + 1
+            c.p_vol = (4 * 4 * 0.3) / c.n_particles
+            c.g = 9.8
+            c.lb = [3, 3, 3]
+            c.ub = [c.n_grid * 4 - 3, c.n_grid - 3, c.n_grid * 4 - 3]
+            c.grid_res = [4 * c.n_grid, c.n_grid, 4 * c.n_grid]
+            c.use_dithering = True
+            c.use_bitpack = True
+            c.use_bound_clip = True
+            self.kind = "forward"
+        c.quant_bits = np.array([32] * 16)
+        c.quant_ranges = np.array([2.0] * 16)
+        return c
+
+    def collider(self):
+        stem = "propeller_higher" if getattr(self, "kind", "forward") == "ad" else "propeller_2x2_larger"
+        sdf = np.load(os.path.join(self.inputs, stem + ".npz"))["sdf"]
+        normal = np.load(os.path.join(self.inputs, stem + "_normal.npz"))["sdf"]
+        return sdf, normal
+
+    def init(self, mpm):
+        mpm.initialize()
+        c = mpm.param
+        sdf, normal = self.collider()
+        rate = 0.15 if self.kind == "ad" else 0.1
+        mpm.init_sdf_value(sdf, normal, offset=[0, 0, 0], omega=5.0, height_rate=rate)
+        dx = 1 / c.n_grid
+        b = c.bound
+        if self.kind == "ad":
+            ub = [c.n_grid * 2 - b[0] - 1, c.n_grid - b[1], c.n_grid * 2 - b[2] - 1]
+            for y0 in (b[1] * dx, b[1] * dx + 0.2):
+                mpm.add_cube((b[0] * dx, y0, b[2] * dx), (ub[0] * dx, 0.2, ub[2] * dx), c.n_particles // 2)
+        else:
+            lb, ub = c.lb, c.ub
+            mpm.add_cube(((lb[0] + 0.5) * dx, (lb[1] + 0.5) * dx, (lb[2] + 0.5) * dx),
+                         ((ub[0] - lb[0] - 0.5) * dx, 0.3, (ub[0] - lb[0] - 0.5) * dx), c.n_particles)
+
+    def scheme(self, grads, ranges, mode, eps):
+        """Bits from the solve() recipe (positions range 2 there), returned
+        with the quantized ranges of the forward run (positions 4, y 1)."""
+        if mode != CR:
+            raise ValueError("fluid_3d runs the compression-rate mode only")
+        r = np.array(ranges, dtype=np.float64)
+        r[6:15] *= 24
+        r[3:6] *= 1.5
+        r[-1] *= 1.5
+        rs = r.copy()
+        rs[:3] = 2.0
+        bits, _ = LagrangianCR(np.asarray(grads) * rs ** 2, r=eps)
+        r[:3] = 4.0
+        r[1] = 1.0
+        return bits + 1, r
+
+
+EXPERIMENTS = {e.name: e for e in (Elastic2D, Fluid2D, FallingBlock3D, Letters3D, Propeller3D)}
 
 
 def _paths(exp, root):
@@ -290,12 +451,14 @@ def main(argv=None):
     ap.add_argument("-m", "--mode", type=int, default=CR, help="0 compression rate, 1 error bound")
     ap.add_argument("-N", "--runs", type=int, default=20)
     ap.add_argument("--root", default=".")
+    ap.add_argument("--inputs", default="inputs", help="folder of the 3D experiments' meshes and collider volumes")
     ap.add_argument("--timesteps", type=int, default=None)
     ap.add_argument("--json", action="store_true")
     args = ap.parse_args(argv)
 
     exp = EXPERIMENTS[args.experiment]()
-    cfg = exp.config()
+    exp.inputs = args.inputs
+    cfg = exp.config("ad" if args.ad else "ranges" if args.ranges else "forward")
     if args.timesteps:
         cfg.n_timesteps = args.timesteps
     if args.ad:

@@ -16,7 +16,10 @@ Writes reference_data.json:
   * outputs of the compression-rate solver that run_mpm_fluid_2d.py
     defines locally (:129-145; only that function is taken out of the
     script with ast and run, since the script itself imports Taichi), with
-    that driver's solve() recipe (:162-178).
+    that driver's solve() recipe (:162-178);
+  * outputs of the reference's LagrangianCR with the range recipes of the
+    3D drivers' solve() (run_mpm_elastic_3d.py:323-333,
+    run_mpm_fluid_3d.py:149-161).
 Nothing at test time reads the reference checkout; tests read the JSON.
 """
 import ast
@@ -80,6 +83,23 @@ def main(ref):
         bits, fun = ns["LagrangianCR"](g * r ** 2, r=rate)
         out["driver_solver"].append({"driver": "fluid_2d", "key": key, "mode": "CR", "eps": rate,
                                      "ranges": r.tolist(), "bits": bits.tolist(), "fun": float(fun)})
+    # solve() of run_mpm_elastic_3d.py (:323-333) and run_mpm_fluid_3d.py
+    # (:149-161): their own range recipes, the reference's LagrangianCR
+    for driver, key in (("elastic_3d", "elastic_3d/elastic_3d.npy"), ("fluid_3d", "fluid_3d/fluid_3d.npy")):
+        for rate in (0.3, 0.512, 0.7):
+            g = np.array(out["grads"][key])
+            r = np.array(out["ranges"][key], dtype=np.float64)
+            if driver == "elastic_3d":
+                r[:] *= 2.0
+                r[:3] = 4.0
+            else:
+                r[6:15] *= 24
+                r[3:6] *= 1.5
+                r[-1] *= 1.5
+                r[:3] = 2.0
+            bits, fun = ana.LagrangianCR(g * (r ** 2), r=rate)
+            out["driver_solver"].append({"driver": driver, "key": key, "mode": "CR", "eps": rate,
+                                         "ranges": r.tolist(), "bits": bits.tolist(), "fun": float(fun)})
     with open(os.path.join(HERE, "reference_data.json"), "w") as f:
         json.dump(out, f, indent=1)
     print("wrote", os.path.join(HERE, "reference_data.json"))

@@ -36,8 +36,9 @@ def test_elastic_2d_solve_matches_reference_solver(mode):
 def test_fluid_2d_solve_matches_the_drivers_own_solver():
     exp = D.Fluid2D()
     g, r = np.array(GOLD["grads"][F2]), np.array(GOLD["ranges"][F2])
-    assert GOLD["driver_solver"]
-    for c in GOLD["driver_solver"]:
+    cases = [c for c in GOLD["driver_solver"] if c["driver"] == "fluid_2d"]
+    assert cases
+    for c in cases:
         bits, ranges = exp.scheme(g, r, D.CR, c["eps"])
         assert bits.tolist() == c["bits"], c["eps"]
         assert ranges.tolist() == c["ranges"]
@@ -138,3 +139,95 @@ def test_adjoint_report_groups_partition_the_3d_record():
     assert sorted(sum(g, [])) == list(range(24)) and len(g) == len(AR.GROUP_NAMES) == 12
     v = np.arange(24, dtype=np.float64)
     assert np.array_equal([v[s].sum() for s in g], group_fields_3d(v))
+
+
+@pytest.mark.parametrize("driver,cls", [("elastic_3d", D.Letters3D), ("fluid_3d", D.Propeller3D)])
+def test_3d_drivers_solve_matches_reference_solver(driver, cls):
+    """The 3D drivers' solve() recipes (run_mpm_elastic_3d.py:323-333,
+    run_mpm_fluid_3d.py:149-161) against the reference's LagrangianCR on
+    its shipped gradients and ranges."""
+    exp = cls()
+    key = "%s/%s.npy" % (driver, driver)
+    g, r = np.array(GOLD["grads"][key]), np.array(GOLD["ranges"][key])
+    cases = [c for c in GOLD["driver_solver"] if c["driver"] == driver]
+    assert len(cases) == 3
+    for c in cases:
+        bits, ranges = exp.scheme(g, r, D.CR, c["eps"])
+        assert bits.tolist() == [b + 1 for b in c["bits"]], c["eps"]
+        if driver == "elastic_3d":
+            assert ranges.tolist() == c["ranges"]
+        else:  # solved with positions at 2, run with positions at 4 and y at 1
+            want = np.array(c["ranges"])
+            want[:3] = [4.0, 1.0, 4.0]
+            assert ranges.tolist() == want.tolist()
+    with pytest.raises(ValueError):
+        exp.scheme(g, r, D.EB, 0.1)
+
+
+def test_fluid_3d_scheme_reproduces_the_drivers_recorded_bits():
+    """run_mpm_fluid_3d.py:201 records the bits its solve() gave at a 0.5
+    compression target: [21, 22, 21, 15, 18, 15, 12, 16, 13, 14, 13, 14, 14,
+    15, 13, 17]; the scheme at eps 0.512 (the value solve() uses) gives
+    them."""
+    key = "fluid_3d/fluid_3d.npy"
+    bits, _ = D.Propeller3D().scheme(np.array(GOLD["grads"][key]), np.array(GOLD["ranges"][key]), D.CR, 0.512)
+    assert bits.tolist() == [21, 22, 21, 15, 18, 15, 12, 16, 13, 14, 13, 14, 14, 15, 13, 17]
+
+
+class _Recorder(_FakeSolver):
+    def __init__(self, cfg):
+        super().__init__(cfg)
+        self.calls = []
+
+    def add_mesh(self, tri, **kw):
+        self.calls.append(("add_mesh", tri.shape, kw))
+
+    def init_sdf_value(self, sdf, normal, **kw):
+        self.calls.append(("init_sdf_value", sdf.shape, normal.shape, kw))
+
+
+def test_3d_experiment_setups(tmp_path):
+    """Scene set-up of the 3D drivers with stand-in input files: the meshes
+    and collider volumes are read from --inputs, the letters are emitted at
+    the reference's translations, the propeller scene gets the collider on
+    the autodiff schedule and the reference's slabs."""
+    from autoquantizer_b200 import mesh_io
+
+    inp = tmp_path / "inputs"
+    inp.mkdir()
+    v = np.array([[0, 0, 0], [1, 0, 0], [0, 1, 0]], dtype=np.float32)
+    with open(inp / "auto_quant.ply", "wb") as f:
+        f.write(b"ply\nformat binary_little_endian 1.0\nelement vertex 3\nproperty float x\nproperty float y\n"
+                b"property float z\nelement face 1\nproperty list uchar uint vertex_indices\nend_header\n")
+        f.write(v.tobytes() + np.uint8(3).tobytes() + np.array([0, 1, 2], "<u4").tobytes())
+    for stem in ("propeller_higher", "propeller_2x2_larger"):
+        np.savez(inp / (stem + ".npz"), sdf=np.zeros((4, 5, 6), np.float32))
+        np.savez(inp / (stem + "_normal.npz"), sdf=np.zeros((4, 5, 6, 3), np.float32))
+    assert mesh_io.load_mesh(str(inp / "auto_quant.ply")).shape == (1, 9)
+
+    le = D.Letters3D()
+    le.inputs = str(inp)
+    cfg = le.config("forward")
+    assert (cfg.n_particles, cfg.n_grid, cfg.dt, cfg.E, cfg.la, cfg.nu) == (int(3e8), 256, 7.5e-5, 5e5, 5e4, 0.2)
+    m = _Recorder(cfg)
+    le.init(m)
+    assert [c[2]["translation"] for c in m.calls] == [(0.90, 1.6, 0.1), (2.2, 1.6, 0.1)]
+    assert all(c[2]["sample_density"] == 8 and c[2]["velocity"] == (0.0, -4.0, 0.0) for c in m.calls)
+
+    pr = D.Propeller3D()
+    pr.inputs = str(inp)
+    cfg = pr.config("ad")
+    assert (cfg.n_particles, cfg.n_grid, cfg.dt, cfg.la) == (100 ** 3, 64, 4e-4, 5e5)
+    assert cfg.ub == [125, 61, 125] and cfg.grid_res == [128, 64, 128]
+    m = _Recorder(cfg)
+    pr.init(m)
+    assert m.calls[0][0] == "init_sdf_value" and m.calls[0][3]["height_rate"] == 0.15
+    dx = 1 / 64
+    assert m.calls[0][1] == (4, 5, 6)
+    assert [c[0] for c in m.cubes] == [[3 * dx, 3 * dx, 3 * dx], [3 * dx, 3 * dx + 0.2, 3 * dx]]
+    assert all(c[2] == 100 ** 3 // 2 for c in m.cubes)
+    cfg = pr.config("forward")
+    assert (cfg.n_particles, cfg.n_grid, cfg.ub) == (int(4e8), 256, [1021, 253, 1021])
+    m = _Recorder(cfg)
+    pr.init(m)
+    assert m.calls[0][3]["height_rate"] == 0.1 and len(m.cubes) == 1 and m.cubes[0][2] == int(4e8)
