@@ -409,3 +409,41 @@ def test_oracle_collider_holds_a_block_on_a_static_slab():
         ys.append(o.get_state()[:, 1].min())
     assert ys[0] < 0.40 - 0.04  # free fall over 0.1 s: 0.5 g t^2 = 0.049
     assert ys[1] > 0.375 - 0.01  # held at the slab's top (node 13 = 0.406, stencil reach one cell)
+
+
+# taichi_submission/tests/python/test_custom_float_time_integration.py:10-66:
+# midpoint integration of a point around the unit circle, 1000 steps of
+# 2 pi / 1000, the position stored after every step as f32, as a 16-bit
+# fixed point with scale 2^-14 (range 2), as floats with 13-bit signed
+# significands and their own 6-bit exponents, or with one shared 6-bit
+# exponent; the position after half a turn must be (-1, 0) and after a
+# full turn (1, 0) to 2e-2 (3e-2 for the final y).
+@pytest.mark.parametrize("kind", ["f32", "fixed", "exponent", "shared"])
+def test_custom_float_time_integration(kind):
+    specs = {"f32": None,
+             "fixed": [fixed(16, 2.0)] * 2,
+             "exponent": [fexp(13, 6)] * 2,
+             "shared": [shexp(13, 6, True)] * 2}[kind]
+    L = O.build_layout(specs) if specs else None
+
+    def store(p):
+        p = np.asarray(p, dtype=np.float32).astype(np.float64)
+        return p if L is None else O.decode(L, O.encode(L, p[None]))[0]
+
+    def v_at(p):
+        return np.array([-p[1], p[0]], dtype=np.float32)
+
+    x = store([1.0, 0.0])
+    n = 1000
+    dt = np.float32(math.pi * 2 / n)
+    px, py = [], []
+    for _ in range(n):
+        xf = x.astype(np.float32)
+        v_mid = v_at(xf + np.float32(0.5) * dt * v_at(xf))
+        x = store(xf + v_mid * dt)
+        px.append(x[0])
+        py.append(x[1])
+    assert px[n // 2 - 1] == approx(-1, abs=2e-2)
+    assert py[n // 2 - 1] == approx(0, abs=2e-2)
+    assert px[-1] == approx(1, abs=2e-2)
+    assert py[-1] == approx(0, abs=3e-2)
