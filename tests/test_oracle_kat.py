@@ -447,3 +447,33 @@ def test_custom_float_time_integration(kind):
     assert py[n // 2 - 1] == approx(0, abs=2e-2)
     assert px[-1] == approx(1, abs=2e-2)
     assert py[-1] == approx(0, abs=3e-2)
+
+
+def test_custom_int_implicit_cast():
+    # test_custom_int.py:4-16: a float stored into int(13, signed) truncates
+    L = O.build_layout([qint(13, True)])
+    assert O.decode(L, O.encode(L, np.array([[10.3]])))[0, 0] == 10
+    assert O.decode(L, O.encode(L, np.array([[-10.7]])))[0, 0] == -10
+
+
+def test_bit_struct_load_and_store():
+    # test_bit_struct.py:38-78 (13/14/5-bit fields) and :92-133 (three
+    # fields of the given widths at their extreme and ordinary values)
+    L = O.build_layout([qint(13, True), qint(14, False), qint(5, True)])
+    cases = np.array([[2**12 - 1, 2**14 - 1, -(2**3)], [2**11 - 1, 2**13 - 1, -(2**2)],
+                      [0, 0, 0], [123, 4567, 8], [10, 31, 11]], dtype=np.float64)
+    assert (O.decode(L, O.encode(L, cases)) == cases).all()
+    for bits, vals in [([3, 3, 2], [2**2 - 1, 2**3 - 1, -2**1]), ([4, 7, 5], [2**3 - 1, 2**7 - 1, -2**4]),
+                       ([17, 11, 4], [2**16 - 1, 2**10 - 1, -2**3]), ([32, 23, 9], [2**31 - 1, 2**23 - 1, -2**8]),
+                       ([7, 12, 13], [2**6 - 1, 2**12 - 1, -2**12]), ([18, 22, 24], [2**17 - 1, 2**22 - 1, -2**23]),
+                       ([5, 5, 6], [15, 5, 20]), ([10, 10, 12], [11, 19, 2020])]:
+        L = O.build_layout([qint(bits[0], True), qint(bits[1], False), qint(bits[2], True)])
+        v = np.array([vals], dtype=np.float64)
+        assert (O.decode(L, O.encode(L, v)) == v).all(), bits
+
+
+def test_custom_int_full_struct():
+    # test_bit_struct.py:81-90: a 32-bit signed int filling its word
+    L = O.build_layout([qint(32, True)])
+    for v in (15, 12, -2**31, 2**31 - 1):
+        assert O.decode(L, O.encode(L, np.array([[v]], dtype=np.float64)))[0, 0] == v
