@@ -138,3 +138,42 @@ def test_c2_record_words_match_oracle_at_full_size():
                            rng.uniform(0.6, 1.4, (n, 1))], 1)
     wg = gpu_encode(L, vals, seed=42, step=3999)
     assert np.array_equal(wg, O.encode(Lo, vals, seed=42, step=3999))
+
+
+@pytest.mark.parametrize("kind", ["fixed", "exponent", "shared"])
+def test_time_integration_through_the_gpu_codec(kind):
+    """test_custom_float_time_integration.py:10-66 with every store going
+    through aq_encode / aq_decode: the circle closes to 2e-2 (3e-2 for the
+    final y), and every stored position equals the oracle codec's."""
+    import math
+
+    rec = Q.BitPack()
+    if kind == "fixed":
+        rec.place(Q.fixed(16, True, 2.0), Q.fixed(16, True, 2.0))
+    elif kind == "exponent":
+        rec.place(Q.qfloat(13, 6, True), Q.qfloat(13, 6, True))
+    else:
+        rec.place(Q.qfloat(13, 6, True), Q.qfloat(13, 6, True), shared_exponent=True)
+    L = rec.build()
+    OL = O.build_layout(rec.spec_tuples(), *rec.compute_and_dithering())
+
+    def store(p):
+        p = np.asarray(p, dtype=np.float32).astype(np.float64)[None]
+        w = gpu_encode(L, p)
+        assert np.array_equal(w, O.encode(OL, p))
+        return gpu_decode(L, w)[0]
+
+    def v_at(p):
+        return np.array([-p[1], p[0]], dtype=np.float32)
+
+    x = store([1.0, 0.0])
+    n = 1000
+    dt = np.float32(math.pi * 2 / n)
+    px, py = [], []
+    for _ in range(n):
+        xf = x.astype(np.float32)
+        x = store(xf + v_at(xf + np.float32(0.5) * dt * v_at(xf)) * dt)
+        px.append(x[0])
+        py.append(x[1])
+    assert abs(px[n // 2 - 1] + 1) <= 2e-2 and abs(py[n // 2 - 1]) <= 2e-2
+    assert abs(px[-1] - 1) <= 2e-2 and abs(py[-1]) <= 3e-2
