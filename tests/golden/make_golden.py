@@ -19,7 +19,8 @@ Writes reference_data.json:
     that driver's solve() recipe (:162-178);
   * outputs of the reference's LagrangianCR with the range recipes of the
     3D drivers' solve() (run_mpm_elastic_3d.py:323-333,
-    run_mpm_fluid_3d.py:149-161).
+    run_mpm_fluid_3d.py:149-161);
+  * the reference's MPMConfig defaults (mpm_exps/mpm_config.py).
 Nothing at test time reads the reference checkout; tests read the JSON.
 """
 import ast
@@ -100,6 +101,11 @@ def main(ref):
             bits, fun = ana.LagrangianCR(g * (r ** 2), r=rate)
             out["driver_solver"].append({"driver": driver, "key": key, "mode": "CR", "eps": rate,
                                          "ranges": r.tolist(), "bits": bits.tolist(), "fun": float(fun)})
+    # MPMConfig defaults (mpm_exps/mpm_config.py, imported from the checkout)
+    spec = importlib.util.spec_from_file_location("ref_mpm_config", os.path.join(ref, "mpm_exps", "mpm_config.py"))
+    cfg_mod = importlib.util.module_from_spec(spec)
+    spec.loader.exec_module(cfg_mod)
+    out["mpm_config_defaults"] = dict(vars(cfg_mod.MPMConfig()))
     with open(os.path.join(HERE, "reference_data.json"), "w") as f:
         json.dump(out, f, indent=1)
     print("wrote", os.path.join(HERE, "reference_data.json"))

@@ -231,3 +231,14 @@ def test_3d_experiment_setups(tmp_path):
     m = _Recorder(cfg)
     pr.init(m)
     assert m.calls[0][3]["height_rate"] == 0.1 and len(m.cubes) == 1 and m.cubes[0][2] == int(4e8)
+
+
+def test_mpm_config_defaults_match_the_reference():
+    """Every field of the reference's MPMConfig (mpm_exps/mpm_config.py)
+    exists here with the same default, so drivers run unchanged."""
+    from autoquantizer_b200.mpm_config import MPMConfig
+
+    ours = vars(MPMConfig())
+    for k, v in GOLD["mpm_config_defaults"].items():
+        assert k in ours, k
+        assert ours[k] == pytest.approx(v) if isinstance(v, float) else ours[k] == v, k
