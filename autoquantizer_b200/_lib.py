@@ -27,7 +27,7 @@ EXPORTS = [
     "aq_layout_build", "aq_encode", "aq_decode", "aq_sim_create", "aq_sim_destroy", "aq_sim_set_state",
     "aq_sim_get_state", "aq_sim_set_words", "aq_sim_get_words", "aq_sim_substeps", "aq_sim_loss",
     "aq_sim_field_stats", "aq_sim_set_collider", "aq_sim_collider_get", "aq_sim_grid_mass", "aq_voxelize", "aq_adjoint_set_collider",
-    "aq_sim_ranges_enable", "aq_sim_ranges_get", "aq_sim_status", "aq_sim_step_count", "aq_sim_launches",
+    "aq_sim_ranges_enable", "aq_sim_ranges_get", "aq_sim_status", "aq_sim_step_count", "aq_sim_set_step_count", "aq_sim_launches",
     "aq_state_error", "aq_error_string", "aq_abi_version", "aq_sim_profile_enable", "aq_sim_profile_get",
     "aq_sim_kernel_is_jit", "aq_adjoint_create", "aq_adjoint_destroy", "aq_adjoint_forward", "aq_adjoint_backward",
     "aq_mlp_param_count", "aq_mlp_to_bf16", "aq_mlp_forward", "aq_mlp_backward", "aq_mlp_mse_grad", "aq_mlp_adam",
@@ -110,6 +110,7 @@ def lib():
         "aq_sim_ranges_get": ([vp, C.POINTER(C.c_double), C.POINTER(C.c_double), vp], C.c_int),
         "aq_sim_status": ([vp, C.POINTER(C.c_uint32), C.POINTER(C.c_int64), i32, vp], C.c_int),
         "aq_sim_step_count": ([vp, C.POINTER(C.c_int64)], C.c_int),
+        "aq_sim_set_step_count": ([vp, i64], C.c_int),
         "aq_sim_launches": ([vp, C.POINTER(C.c_int64)], C.c_int),
         "aq_sim_kernel_is_jit": ([vp, C.POINTER(C.c_int32)], C.c_int),
         "aq_state_error": ([vp, i32, vp, i32, i64, i32, C.POINTER(C.c_double), C.POINTER(C.c_double), vp],

@@ -953,6 +953,12 @@ int aq_sim_step_count(const aq_sim* s, int64_t* h_out) {
   return AQ_OK;
 }
 
+int aq_sim_set_step_count(aq_sim* s, int64_t step) {
+  if (!s || step < 0) return AQ_E_ARG;
+  s->step = step;
+  return AQ_OK;
+}
+
 int aq_sim_kernel_is_jit(const aq_sim* s, int32_t* h_out) {
   if (!s || !h_out) return AQ_E_ARG;
   *h_out = s->jit_fn ? 1 : 0;

@@ -544,6 +544,57 @@ class MPMSolver:
             self._ensure_sim()
         return data
 
+    def step_count(self):
+        """Substeps run by the simulator (the dithering step index)."""
+        if self._sim is None:
+            return 0
+        v = C.c_int64()
+        _lib.check(_lib.lib().aq_sim_step_count(self._sim, C.byref(v)), "aq_sim_step_count")
+        return v.value
+
+    def save_checkpoint(self, fn):
+        """The packed state as .npz: the records' words in particle order, the
+        layout they follow (slot specs), the substep count and the
+        collider's angle and height; load_checkpoint resumes from it with
+        the same dithering draws as an uninterrupted run."""
+        words = self.words()
+        col = self.collider_state()
+        np.savez_compressed(fn, words=words, n_particles=np.int64(self.current_idx),
+                            specs=np.array(self.record().spec_tuples(), dtype=np.float64),
+                            step=np.int64(self.step_count()), seed=np.int64(int(self.param.seed)),
+                            collider=np.array(col if col is not None else [np.nan, np.nan]))
+        return fn
+
+    def load_checkpoint(self, fn):
+        """Resume from save_checkpoint's file: the layout must be this
+        solver's; the particle count becomes the file's."""
+        d = np.load(fn)
+        specs = np.array(self.record().spec_tuples(), dtype=np.float64)
+        if d["specs"].shape != specs.shape or not np.array_equal(d["specs"], specs):
+            raise ValueError("load_checkpoint: the file's record layout differs from this solver's")
+        n = int(d["n_particles"])
+        if n > self.n_particles:
+            raise ValueError("load_checkpoint: %d particles exceed n_particles=%d" % (n, self.n_particles))
+        if int(d["seed"]) != int(self.param.seed):
+            raise ValueError("load_checkpoint: the file was written with seed %d" % int(d["seed"]))
+        self._pull()
+        self._staging()
+        self._dev = None
+        self.current_idx = n
+        self._drop_sim()
+        col = d["collider"]
+        if self._col is not None and np.all(np.isfinite(col)):
+            self._col["theta"], self._col["height"] = float(col[0]), float(col[1])
+        self.set_words(d["words"])
+        self.set_step_count(int(d["step"]))
+        if self._col is not None:
+            self._apply_collider()
+
+    def set_step_count(self, step):
+        """Set the dithering step index (aq_sim_set_step_count)."""
+        self._ensure_sim()
+        _lib.check(_lib.lib().aq_sim_set_step_count(self._sim, int(step)), "aq_sim_set_step_count")
+
     fetch_mat_data_np = fetch_data_np
     fetch_scalar_data_np = fetch_data_np
     push_mat_data_np = push_data_np

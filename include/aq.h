@@ -253,6 +253,10 @@ int aq_sim_ranges_get(aq_sim* sim, double* h_max, double* h_min, void* stream);
 int aq_sim_status(aq_sim* sim, uint32_t* h_flags, int64_t* h_fallbacks,
                   int32_t clear, void* stream);
 int aq_sim_step_count(const aq_sim* sim, int64_t* h_out);
+/* Set the substep counter (the dithering generator's step index), e.g. when
+ * resuming from saved records so that the continuation draws the same
+ * uniforms as an uninterrupted run. */
+int aq_sim_set_step_count(aq_sim* sim, int64_t step);
 /* 1 if the substep kernel in use was compiled for this layout by NVRTC, 0 if
  * it is the generic nvcc-built kernel.  No reference counterpart (Taichi
  * always JIT-compiles, taichi_submission/taichi/backends/cuda/jit_cuda.cpp). */

@@ -242,3 +242,31 @@ def test_mpm_config_defaults_match_the_reference():
     for k, v in GOLD["mpm_config_defaults"].items():
         assert k in ours, k
         assert ours[k] == pytest.approx(v) if isinstance(v, float) else ours[k] == v, k
+
+
+def test_checkpoint_file_round_trip(tmp_path):
+    """save_checkpoint / load_checkpoint plumbing on CPU (the device calls
+    replaced by recorders): words, particle count, substep count and the
+    layout check."""
+    from autoquantizer_b200 import scenes
+    from autoquantizer_b200.mpm_solver import MPMSolver
+
+    cfg, vals = scenes.falling_block_3d(n=500, n_grid=16)
+    a = MPMSolver(cfg)
+    a.set_particles(vals[:300])
+    W = a.layout().n_words
+    words = np.arange(300 * W, dtype=np.uint64).reshape(300, W) * np.uint64(0x9E3779B97F4A7C15)
+    a.words = lambda: words
+    a.step_count = lambda: 77
+    fn = a.save_checkpoint(str(tmp_path / "ck.npz"))
+
+    b = MPMSolver(cfg)
+    got = {}
+    b.set_words = lambda w: got.setdefault("words", np.array(w))
+    b.set_step_count = lambda st: got.setdefault("step", st)
+    b.load_checkpoint(fn)
+    assert b.current_idx == 300 and got["step"] == 77 and np.array_equal(got["words"], words)
+
+    other, _ = scenes.dam_break_2d(n=100, n_grid=16)
+    with pytest.raises(ValueError):
+        MPMSolver(other).load_checkpoint(fn)
