@@ -161,3 +161,17 @@ def test_voxelizer_reproduces_the_reference_letters():
     assert set(np.unique(v)) <= {0, 1}
     assert int(mask.sum()) == 31928 and np.array_equal(v > 0, mask)
     assert int(g["n_particles"]) == 2 * int(mask.sum()) and g["per_voxel"].tolist() == [2]
+
+
+def test_voxelizer_geometry():
+    """voxelizer.py:17-40: every axis rounded up to a power of two, times
+    the super-sampling; spacing dx / super_sample; jitter by precision."""
+    from autoquantizer_b200.voxelizer import Voxelizer
+
+    v = Voxelizer(res=(48, 100, 128), dx=1 / 48, super_sample=2)
+    assert v.res == (128, 256, 256) and v.dx == 1 / 96 and v.inv_dx == 96 and v.padding == 3
+    assert v.jitter_scale == 1e-8 and Voxelizer((8, 8, 8), 0.1, 1, precision="f32").jitter_scale == 1e-4
+    with pytest.raises(ValueError):
+        Voxelizer((8, 8), 0.1)
+    with pytest.raises(ValueError):
+        Voxelizer((8, 8, 8), 0.1, precision="f16")
