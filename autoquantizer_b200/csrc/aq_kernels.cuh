@@ -22,15 +22,17 @@
 //              work item per occupied block (block, first record, count).
 //
 // k_step, persistent CTAs of CH = 128 threads claiming work items (whole
-// cell blocks) from a counter:
-//   1. stage the block's grid tile in shared memory, applying grid_op to
-//      every node (G2P source);
+// cell blocks, the fullest first) from a counter:
+//   1. stage the block's grid tile (7^3 nodes in 3D: the block, the cell
+//      below it and the stencil) in shared memory, applying grid_op (and
+//      the SDF collider when compiled in) to every node (G2P source);
 //   2. the 4 warps take the block's records 32 at a time (units), without
 //      CTA barriers between units; per unit each lane loads its record into
-//      its shared slot and
+//      registers (layout-specialized build, short records) or its shared
+//      slot, and
 //      a. G2P of substep k: gather 3^d nodes (z-separable sums), new v, C,
-//         x, F|J; bit_pack_assign into the shared record, which also yields
-//         the values a later decode returns; record written back to HBM;
+//         x, F|J; bit_pack_assign into the record, which also yields the
+//         values a later decode returns; record written back to HBM;
 //      b. P2G of substep k+1 from those values into the warp's private tile
 //         of float4 nodes with plain shared-memory read-add-writes, offset
 //         by offset with __syncwarp ordering (lanes that share a base cell
