@@ -114,3 +114,12 @@ def test_dam_break_record_is_152_bits():
     L = rec.build()
     assert L.total_bits == 152 and L.n_words == 3
     assert cfg.v_exp_bits == 6
+
+
+def test_every_entry_point_is_mapped_in_the_integration_notes():
+    """INTEGRATION.md names, for every function include/aq.h declares, the
+    reference interface it replaces (families may be named with a `*`)."""
+    doc = open(os.path.join(ROOT, "INTEGRATION.md")).read()
+    families = [p[:-1] for p in re.findall(r"`(aq_[a-z_0-9]+\*)`", doc)]
+    missing = [f for f in declared_functions() if "`%s`" % f not in doc and not any(f.startswith(p) for p in families)]
+    assert not missing, missing
