@@ -211,6 +211,7 @@ class MPMSolver:
         return self._host
 
     def _drop_sim(self):
+        self._rabs_host = None  # range detection restarts with a new simulator
         if self._sim is not None:
             if self._col is not None:  # carry the collider's angle and height over
                 th, hh = C.c_double(), C.c_double()
@@ -808,6 +809,7 @@ class MPMSolver:
         """Range detection (run_forward_detect_ranges, mpm_solver.py:933-945):
         running max/min of every scalar after each substep."""
         self._ensure_sim()
+        self._rabs_host = None
         _lib.check(_lib.lib().aq_sim_ranges_enable(self._sim, 1, _lib.stream_ptr()), "aq_sim_ranges_enable")
         self.substeps(self.n_timestep - 1 if n is None else n)
         _lib.check(_lib.lib().aq_sim_ranges_enable(self._sim, 0, _lib.stream_ptr()), "aq_sim_ranges_enable")
@@ -820,6 +822,60 @@ class MPMSolver:
         mn = (C.c_double * ns)()
         _lib.check(_lib.lib().aq_sim_ranges_get(self._sim, mx, mn, _lib.stream_ptr()), "aq_sim_ranges_get")
         self._rmax, self._rmin = np.array(mx[:]), np.array(mn[:])
+        h = getattr(self, "_rabs_host", None)  # the state detect_bound_kernel saw first
+        if h is not None:
+            self._rmax, self._rmin = np.maximum(self._rmax, h), np.minimum(self._rmin, -h)
+
+    # ------------------------------------- the drivers' own substep loops
+
+    def nlogn_step_forward(self, s):
+        """One forward substep (the drivers' range-detection loop,
+        run_mpm_elastic_2d.py:173-183)."""
+        self.substep(s)
+
+    def substep_difftaichi(self, s, t=None):
+        """One substep of the autodiff path (mpm_solver.py:791-797)."""
+        self.substep(s)
+
+    def detect_bound_kernel(self, s=0):
+        """Fold the current state into the running ranges (mpm_solver.py:
+        943-950): the first call takes this state's max |q| per scalar and
+        switches the simulator's in-kernel range detection on, which then
+        covers every later substep."""
+        self._ensure_sim()
+        if getattr(self, "_rabs_host", None) is None:
+            self._rabs_host = self.field_stats()[:, 3].copy()
+            _lib.check(_lib.lib().aq_sim_ranges_enable(self._sim, 1, _lib.stream_ptr()), "aq_sim_ranges_enable")
+
+    def step_collider(self):
+        """The drivers call this after every substep (mpm_solver.py:1542-1547);
+        the simulator already advances the collider by omega dt and
+        height_rate dt inside each substep, so there is nothing left to do."""
+
+    def step_collider_difftaichi(self, step):
+        """Put the collider at substep `step` of the autodiff schedule:
+        angle omega dt step, height 0.15 dt step (mpm_solver.py:1554-1559)."""
+        if self._col is None:
+            return
+        self._col["theta"] = self._col["omega"] * self.dt * step
+        self._col["height"] = 0.15 * self.dt * step
+        if self._sim is not None:
+            self._apply_collider()
+
+    @staticmethod
+    def cnt_ending_zero(s):
+        """Trailing zero bits of s + 1 (mpm_solver.py:1200-1207)."""
+        cnt, s = 0, s + 1
+        while s % 2 == 0:
+            cnt += 1
+            s >>= 1
+        return cnt
+
+    def dump_grad(self, s=0, fn=None):
+        """Print the per-scalar sensitivities (mpm_solver.py:1328-1331)."""
+        grads = np.hstack(self.get_gradients())
+        print(grads)
+        return grads
 
     def get_limits(self):
         """mpm_solver.py:981-992: [2]*dim for x, then max(|max|, |min|) of

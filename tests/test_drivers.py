@@ -270,3 +270,22 @@ def test_checkpoint_file_round_trip(tmp_path):
     other, _ = scenes.dam_break_2d(n=100, n_grid=16)
     with pytest.raises(ValueError):
         MPMSolver(other).load_checkpoint(fn)
+
+
+def test_driver_loop_helpers_on_the_host():
+    """The small methods the reference drivers call in their own loops."""
+    from autoquantizer_b200 import scenes
+    from autoquantizer_b200.mpm_solver import MPMSolver
+
+    assert [MPMSolver.cnt_ending_zero(s) for s in range(8)] == [0, 1, 0, 2, 0, 1, 0, 3]
+    cfg, vals = scenes.falling_block_3d(n=100, n_grid=16)
+    s = MPMSolver(cfg)
+    s.step_collider()  # nothing to do: the simulator advances the collider itself
+    s._grads = [np.arange(3.0), np.arange(3.0, 6.0)]
+    assert s.dump_grad(0).tolist() == [0, 1, 2, 3, 4, 5]
+    import torch
+
+    s._col = {"sdf": torch.zeros((2, 2, 2)), "normal": torch.zeros((2, 2, 2, 3)), "offset": [0, 0, 0],
+              "theta": 0.0, "height": 0.0, "omega": 5.0, "rate": 0.1}
+    s.step_collider_difftaichi(10)
+    assert s.collider_state() == (pytest.approx(5.0 * cfg.dt * 10), pytest.approx(0.15 * cfg.dt * 10))
