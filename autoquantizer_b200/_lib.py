@@ -26,7 +26,8 @@ ERRORS = {0: "ok", -1: "bad argument", -2: "layout does not fit the simulator sc
 EXPORTS = [
     "aq_layout_build", "aq_encode", "aq_decode", "aq_sim_create", "aq_sim_destroy", "aq_sim_set_state",
     "aq_sim_get_state", "aq_sim_set_words", "aq_sim_get_words", "aq_sim_substeps", "aq_sim_loss",
-    "aq_sim_field_stats", "aq_sim_set_collider", "aq_sim_collider_get", "aq_sim_grid_mass", "aq_voxelize", "aq_adjoint_set_collider",
+    "aq_sim_field_stats", "aq_sim_set_collider", "aq_sim_collider_get", "aq_sim_collider_pose",
+    "aq_sim_collider_velocity_mode", "aq_sim_grid_mass", "aq_voxelize", "aq_adjoint_set_collider",
     "aq_sim_ranges_enable", "aq_sim_ranges_get", "aq_sim_status", "aq_sim_step_count", "aq_sim_set_step_count", "aq_sim_launches",
     "aq_state_error", "aq_error_string", "aq_abi_version", "aq_sim_profile_enable", "aq_sim_profile_get",
     "aq_sim_kernel_is_jit", "aq_adjoint_create", "aq_adjoint_destroy", "aq_adjoint_forward", "aq_adjoint_backward",
@@ -106,6 +107,8 @@ def lib():
         "aq_sim_set_collider": ([vp, vp, vp, C.POINTER(C.c_int32), C.POINTER(C.c_int32), i32, C.c_double,
                                  C.c_double, C.c_double, C.c_double], C.c_int),
         "aq_sim_collider_get": ([vp, C.POINTER(C.c_double), C.POINTER(C.c_double)], C.c_int),
+        "aq_sim_collider_pose": ([vp, C.c_double, C.c_double], C.c_int),
+        "aq_sim_collider_velocity_mode": ([vp, i32], C.c_int),
         "aq_sim_ranges_enable": ([vp, i32, vp], C.c_int),
         "aq_sim_ranges_get": ([vp, C.POINTER(C.c_double), C.POINTER(C.c_double), vp], C.c_int),
         "aq_sim_status": ([vp, C.POINTER(C.c_uint32), C.POINTER(C.c_int64), i32, vp], C.c_int),

@@ -117,6 +117,7 @@ struct SimK {
   R col_omega;
   R col_c, col_s;  // cos and sin of the collider angle this launch
   int col_yshift;  // collider height in cells this launch, int(height / dx + 0.5)
+  int col_node_cv;  // 1: collider velocity omega x r from the node itself (sdf_collision_no_arg)
 };
 
 struct StepArgs {
@@ -223,6 +224,17 @@ __device__ __forceinline__ double sub_rn(double a, double b) { return __dsub_rn(
 // normal and the collider's velocity omega x r: r from the rotated index
 // (sdf_collision) or, with NODE_CV, from the node itself
 // (sdf_collision_no_arg, mpm_solver.py:1510, the reference's autodiff path).
+// whether a parameter block asks for the node's own position in omega x r:
+// the simulator's per-launch choice, none for other blocks
+template <class KT>
+__device__ __forceinline__ bool col_node_cv_of(const KT&) {
+  return false;
+}
+template <class R>
+__device__ __forceinline__ bool col_node_cv_of(const SimK<R>& K) {
+  return K.col_node_cv != 0;
+}
+
 template <class R, bool NODE_CV = false, class KT>
 __device__ __forceinline__ bool collider_at(const KT& K, int I0, int I1, int I2, R (&nrm)[3], R (&cv)[3]) {
   const int n = K.col_n;
@@ -244,7 +256,8 @@ __device__ __forceinline__ bool collider_at(const KT& K, int I0, int I1, int I2,
   nrm[0] = c * g0 + s * g2;
   nrm[1] = g1;
   nrm[2] = -s * g0 + c * g2;
-  const R rx = (R)((NODE_CV ? I0 : r[0]) - n) * K.dx, rz = (R)((NODE_CV ? I2 : r[2]) - n) * K.dx;
+  const bool from_node = NODE_CV || col_node_cv_of(K);
+  const R rx = (R)((from_node ? I0 : r[0]) - n) * K.dx, rz = (R)((from_node ? I2 : r[2]) - n) * K.dx;
   cv[0] = K.col_omega * rz;
   cv[1] = (R)0;
   cv[2] = -K.col_omega * rx;

@@ -384,6 +384,7 @@ struct aq_sim {
   const float* col_sdf = nullptr;
   const float* col_nrm = nullptr;
   double col_theta = 0, col_height = 0, col_omega = 0, col_rate = 0;
+  int col_node_cv = 0;  // collider velocity from the node (sdf_collision_no_arg) instead of the rotated index
   void* slab = nullptr;      // the one device allocation all buffers above live in
   int ranges_on = 0;
   int64_t step = 0;
@@ -459,6 +460,7 @@ struct SimImpl final : SimBase {
     K.col_sdf = c->col_sdf;
     K.col_nrm = c->col_nrm;
     K.col_omega = (R)c->col_omega;
+    K.col_node_cv = c->col_node_cv;
   }
 
   // the grid tile and the warp tiles, plus a record slot per thread unless
@@ -831,6 +833,20 @@ int aq_sim_set_collider(aq_sim* s, const float* d_sdf, const float* d_normal, co
   s->impl->set_collider(s);
   // the layout-specialized kernel is built with the collider only when one is set
   if (s->P.jit) return s->impl->setup_kernel(s->col_on != 0);
+  return AQ_OK;
+}
+
+int aq_sim_collider_pose(aq_sim* s, double theta, double height) {
+  if (!s) return AQ_E_ARG;
+  s->col_theta = theta;
+  s->col_height = height;
+  return AQ_OK;
+}
+
+int aq_sim_collider_velocity_mode(aq_sim* s, int32_t from_node) {
+  if (!s || (from_node != 0 && from_node != 1)) return AQ_E_ARG;
+  s->col_node_cv = from_node;
+  s->impl->set_collider(s);
   return AQ_OK;
 }
 

@@ -212,6 +212,7 @@ class MPMSolver:
 
     def _drop_sim(self):
         self._rabs_host = None  # range detection restarts with a new simulator
+        self._ranges_on_device = False
         if self._sim is not None:
             if self._col is not None:  # carry the collider's angle and height over
                 th, hh = C.c_double(), C.c_double()
@@ -436,12 +437,22 @@ class MPMSolver:
         self._dirty = False
 
     def substeps(self, n):
+        """n forward substeps (substep, mpm_solver.py:624-631), the collider
+        (when set) as sdf_collision and advanced after every substep."""
         self._ensure_sim()
+        self._collider_velocity_from_node(False)
         _lib.check(_lib.lib().aq_sim_substeps(self._sim, int(n), _lib.stream_ptr()), "aq_sim_substeps")
 
     def substep(self, s=0, t=None):
         """One substep (mpm_solver.py:624-631)."""
         self.substeps(1)
+
+    def _substep_difftaichi_form(self):
+        """One substep with the autodiff path's collider (sdf_collision_no_arg:
+        collider velocity from the node itself)."""
+        self._ensure_sim()
+        self._collider_velocity_from_node(True)
+        _lib.check(_lib.lib().aq_sim_substeps(self._sim, 1, _lib.stream_ptr()), "aq_sim_substeps")
 
     def run_forward_only(self, save_pics=False, save_states=False):
         """run_forward_only of the drivers (run_mpm_elastic_2d.py:124-162):
@@ -722,6 +733,20 @@ class MPMSolver:
                                                   C.c_void_p(c["normal"].data_ptr()), dims, off, int(self.n_grid),
                                                   c["theta"], c["height"], c["omega"], c["rate"]),
                    "aq_sim_set_collider")
+        _lib.check(_lib.lib().aq_sim_collider_velocity_mode(self._sim, int(c.get("node_cv", False))),
+                   "aq_sim_collider_velocity_mode")
+
+    def _collider_velocity_from_node(self, on):
+        """sdf_collision (off: omega x r from the rotated index, the forward
+        substep) or sdf_collision_no_arg (on: from the node itself, the
+        autodiff path's substep_difftaichi)."""
+        c = self._col
+        if c is None or bool(c.get("node_cv", False)) == bool(on):
+            return
+        c["node_cv"] = bool(on)
+        if self._sim is not None:
+            _lib.check(_lib.lib().aq_sim_collider_velocity_mode(self._sim, int(bool(on))),
+                       "aq_sim_collider_velocity_mode")
 
     def collider_state(self):
         """(angle, height) of the collider now."""
@@ -807,45 +832,69 @@ class MPMSolver:
 
     def run_forward_detect_ranges(self, n=None):
         """Range detection (run_forward_detect_ranges, mpm_solver.py:933-945):
-        running max/min of every scalar after each substep."""
+        running max/min of every scalar after each substep, folded on the
+        device.  The reference steps with nlogn_loop_forward, i.e. the
+        autodiff path's substep and collider schedule; without a collider
+        that is the plain substep, run fused here."""
         self._ensure_sim()
         self._rabs_host = None
         _lib.check(_lib.lib().aq_sim_ranges_enable(self._sim, 1, _lib.stream_ptr()), "aq_sim_ranges_enable")
-        self.substeps(self.n_timestep - 1 if n is None else n)
+        self._ranges_on_device = True
+        total = self.n_timestep - 1 if n is None else n
+        if self._col is None:
+            self.substeps(total)
+        else:
+            for s in range(total):
+                self.nlogn_step_forward(s)
         _lib.check(_lib.lib().aq_sim_ranges_enable(self._sim, 0, _lib.stream_ptr()), "aq_sim_ranges_enable")
         self.detect_bound()
         return self.get_limits()
 
     def detect_bound(self, s=0):
+        """Running ranges so far: the device's (run_forward_detect_ranges)
+        and the states detect_bound_kernel folded in."""
         ns = self.n_slots()
-        mx = (C.c_double * ns)()
-        mn = (C.c_double * ns)()
-        _lib.check(_lib.lib().aq_sim_ranges_get(self._sim, mx, mn, _lib.stream_ptr()), "aq_sim_ranges_get")
-        self._rmax, self._rmin = np.array(mx[:]), np.array(mn[:])
-        h = getattr(self, "_rabs_host", None)  # the state detect_bound_kernel saw first
+        self._rmax, self._rmin = np.full(ns, -np.inf), np.full(ns, np.inf)
+        if getattr(self, "_ranges_on_device", False) and self._sim is not None:
+            mx = (C.c_double * ns)()
+            mn = (C.c_double * ns)()
+            _lib.check(_lib.lib().aq_sim_ranges_get(self._sim, mx, mn, _lib.stream_ptr()), "aq_sim_ranges_get")
+            self._rmax, self._rmin = np.array(mx[:]), np.array(mn[:])
+        h = getattr(self, "_rabs_host", None)
         if h is not None:
             self._rmax, self._rmin = np.maximum(self._rmax, h), np.minimum(self._rmin, -h)
 
     # ------------------------------------- the drivers' own substep loops
 
-    def nlogn_step_forward(self, s):
-        """One forward substep (the drivers' range-detection loop,
-        run_mpm_elastic_2d.py:173-183)."""
-        self.substep(s)
+    def nlogn_step_forward(self, s, emit_func=None):
+        """Substep s of the drivers' own loops (nlogn_step_forward,
+        mpm_solver.py:1161-1167): emit_func(s, self) first when given, then
+        substep_difftaichi, then, with a collider, step_collider_difftaichi(s)
+        (angle omega dt s, height 0.15 dt s for the next substep)."""
+        if emit_func is not None:
+            emit_func(s, self)
+        self._substep_difftaichi_form()
+        if self._col is not None:
+            self.step_collider_difftaichi(s)
 
     def substep_difftaichi(self, s, t=None):
-        """One substep of the autodiff path (mpm_solver.py:791-797)."""
-        self.substep(s)
+        """One substep of the autodiff path (mpm_solver.py:791-797): p2g,
+        grid_op, the collider as sdf_collision_no_arg, g2p; the collider is
+        not moved."""
+        pose = self.collider_state() if self._col is not None else None
+        self._substep_difftaichi_form()
+        if pose is not None:  # the simulator advanced it: put it back
+            self._set_collider_pose(*pose)
 
     def detect_bound_kernel(self, s=0):
-        """Fold the current state into the running ranges (mpm_solver.py:
-        943-950): the first call takes this state's max |q| per scalar and
-        switches the simulator's in-kernel range detection on, which then
-        covers every later substep."""
+        """Fold the current state into the running ranges (update_limits_*,
+        mpm_solver.py:943-979): per scalar the max |q| of the state now, and
+        only of this state (the drivers call it after every substep or once
+        per frame)."""
         self._ensure_sim()
-        if getattr(self, "_rabs_host", None) is None:
-            self._rabs_host = self.field_stats()[:, 3].copy()
-            _lib.check(_lib.lib().aq_sim_ranges_enable(self._sim, 1, _lib.stream_ptr()), "aq_sim_ranges_enable")
+        cur = self.field_stats()[:, 3].copy()
+        h = getattr(self, "_rabs_host", None)
+        self._rabs_host = cur if h is None else np.maximum(h, cur)
 
     def step_collider(self):
         """The drivers call this after every substep (mpm_solver.py:1542-1547);
@@ -857,10 +906,13 @@ class MPMSolver:
         angle omega dt step, height 0.15 dt step (mpm_solver.py:1554-1559)."""
         if self._col is None:
             return
-        self._col["theta"] = self._col["omega"] * self.dt * step
-        self._col["height"] = 0.15 * self.dt * step
+        self._set_collider_pose(self._col["omega"] * self.dt * step, 0.15 * self.dt * step)
+
+    def _set_collider_pose(self, theta, height):
+        self._col["theta"], self._col["height"] = float(theta), float(height)
         if self._sim is not None:
-            self._apply_collider()
+            _lib.check(_lib.lib().aq_sim_collider_pose(self._sim, float(theta), float(height)),
+                       "aq_sim_collider_pose")
 
     @staticmethod
     def cnt_ending_zero(s):

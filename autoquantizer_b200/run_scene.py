@@ -3,7 +3,7 @@
     python -m autoquantizer_b200.run_scene --scene mixed_boxes_3d --substeps 8 [--fp32] [--n N] [--grid G]
     python -m autoquantizer_b200.run_scene --device-gen --n 300000000 --grid 640 --substeps 50
 
-Used as the target of ncu captures (profiles/ lists the exact commands).
+A small fixed workload for profiler captures of single kernel launches.
 """
 import argparse
 import json

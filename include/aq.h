@@ -241,6 +241,17 @@ int aq_sim_set_collider(aq_sim* sim, const float* d_sdf, const float* d_normal, 
                         double height_rate);
 /* Current collider angle and height. */
 int aq_sim_collider_get(aq_sim* sim, double* h_theta, double* h_height);
+/* Put the collider at angle theta and height `height` for the next substep
+ * without touching its volumes or kernel (step_collider_difftaichi,
+ * mpm_solver.py:1554-1559, which the autodiff-path drivers call after each
+ * substep: theta = omega dt s, height = 0.15 dt s). */
+int aq_sim_collider_pose(aq_sim* sim, double theta, double height);
+/* Collider velocity omega x r at a node inside the collider: from_node 0
+ * takes r from the rotated index (sdf_collision, mpm_solver.py:1459-1480,
+ * the forward substep's collider), 1 from the node itself
+ * (sdf_collision_no_arg, :1482-1512, the collider of substep_difftaichi and
+ * so of nlogn_step_forward).  Default 0. */
+int aq_sim_collider_velocity_mode(aq_sim* sim, int32_t from_node);
 
 /* Per-slot running max/min of the state (range detection), accumulated on
  * the device after every substep once enabled.
@@ -326,7 +337,10 @@ int aq_adjoint_backward(aq_adjoint* adj, const void* d_seed, void* d_grad_s0, do
  * looks up the array's device address (make that first call before any
  * stream capture starts).  All calls share the one array, each clears its
  * part first, and calls that overlap on the GPU (e.g. from two streams)
- * race on it.  Synchronizes `stream`. */
+ * race on it.  Synchronizes `stream`.  The address looked up on a device is
+ * kept for the life of the process, so resetting a device
+ * (cudaDeviceReset) while libaq.so is loaded is not supported for this entry
+ * point: the kept address would belong to the destroyed context. */
 #define AQ_NOALLOC_MAX_SLOTS 256
 #define AQ_NOALLOC_MAX_DEVICES 64
 int aq_state_error_noalloc(const void* d_a, int32_t a_f64, const void* d_b, int32_t b_f64,

@@ -54,6 +54,10 @@ typedef struct or_params {
   double col_c, col_s, col_omega;
   const float* col_sdf;
   const float* col_nrm;
+  /* 1: collider velocity omega x r with r from the node itself
+   * (sdf_collision_no_arg, mpm_solver.py:1482-1512); 0: from the rotated
+   * index (sdf_collision, :1459-1480) */
+  int col_node_cv;
 } or_params;
 
 void or_voxelize(const double* tris, int64_t n_tris, const int32_t* res, double dx, int32_t padding,

@@ -146,7 +146,8 @@ static int SUF(base_of)(R xv, R inv_dx, int res, int* flags) {
  * (optional, n_slots each) accumulate the decoded new state.  Returns the
  * status flags (1 = out of domain, 2 = NaN). */
 /* grid post-process of the rotating SDF collider: rot_scene
- * (mpm_solver.py:1515-1540) then sdf_collision (:1459-1480) */
+ * (mpm_solver.py:1515-1540) then sdf_collision (:1459-1480), or
+ * sdf_collision_no_arg (:1482-1512) when col_node_cv is set */
 static void SUF(collide)(const or_params* P, const int* I, R* v) {
   const int n = P->col_n;
   const int i0 = I[0] >= 2 * n ? I[0] - 2 * n : I[0], i2 = I[2] >= 2 * n ? I[2] - 2 * n : I[2];
@@ -167,7 +168,8 @@ static void SUF(collide)(const or_params* P, const int* I, R* v) {
   const R g0 = (R)P->col_nrm[3 * q], g1 = (R)P->col_nrm[3 * q + 1], g2 = (R)P->col_nrm[3 * q + 2];
   const R nrm[3] = {c * g0 + s * g2, g1, -s * g0 + c * g2};
   const R dx = (R)P->dx, om = (R)P->col_omega;
-  const R rx = (R)(r[0] - n) * dx, rz = (R)(r[2] - n) * dx;
+  const int px = P->col_node_cv ? I[0] : r[0], pz = P->col_node_cv ? I[2] : r[2];
+  const R rx = (R)(px - n) * dx, rz = (R)(pz - n) * dx;
   const R cv[3] = {om * rz, (R)0, -om * rx}; /* (0, omega, 0) x r */
   R vr[3], dn = 0;
   for (int k = 0; k < 3; ++k) {

@@ -45,7 +45,7 @@ class OrParams(C.Structure):
         ("seed", C.c_uint64), ("threads", C.c_int),
         ("col_on", C.c_int), ("col_n", C.c_int), ("col_dims", C.c_int * 3), ("col_off", C.c_int * 3),
         ("col_yshift", C.c_int), ("col_c", C.c_double), ("col_s", C.c_double), ("col_omega", C.c_double),
-        ("col_sdf", C.c_void_p), ("col_nrm", C.c_void_p),
+        ("col_sdf", C.c_void_p), ("col_nrm", C.c_void_p), ("col_node_cv", C.c_int),
     ]
 
 
@@ -186,10 +186,12 @@ class Sim:
     def get_state(self):
         return decode(self.L, self.words)
 
-    def set_collider(self, sdf, normal, offset, center, theta=0.0, height=0.0, omega=5.0, height_rate=0.1):
+    def set_collider(self, sdf, normal, offset, center, theta=0.0, height=0.0, omega=5.0, height_rate=0.1,
+                     node_velocity=False):
         """The rotating SDF collider (float32 volumes sdf [a,b,c], normal
         [a,b,c,3] placed at grid index offset); angle and height advance by
-        omega dt and height_rate dt after every substep."""
+        omega dt and height_rate dt after every substep.  node_velocity:
+        collider velocity from the node itself (sdf_collision_no_arg)."""
         self._col = (np.ascontiguousarray(sdf, dtype=np.float32), np.ascontiguousarray(normal, dtype=np.float32))
         self.P.col_on = 1
         self.P.col_n = int(center)
@@ -199,6 +201,7 @@ class Sim:
         self.P.col_sdf = self._col[0].ctypes.data
         self.P.col_nrm = self._col[1].ctypes.data
         self.P.col_omega = float(omega)
+        self.P.col_node_cv = int(bool(node_velocity))
         self.col_theta, self.col_height, self.col_rate = float(theta), float(height), float(height_rate)
 
     def _collider_step_values(self):

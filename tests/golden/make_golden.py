@@ -1,7 +1,7 @@
 """Regenerate the golden fixtures of this folder from the AutoQuantizer
-reference checkout (read-only), e.g.
+reference checkout (read-only), given as the one argument:
 
-    python tests/golden/make_golden.py /root/reference
+    python tests/golden/make_golden.py <reference checkout>
 
 Writes reference_data.json:
   * the reference's shipped autodiff sensitivities and detected ranges
@@ -112,4 +112,6 @@ def main(ref):
 
 
 if __name__ == "__main__":
-    main(sys.argv[1] if len(sys.argv) > 1 else "/root/reference")
+    if len(sys.argv) != 2:
+        sys.exit("usage: python %s <path of the AutoQuantizer reference checkout>" % sys.argv[0])
+    main(sys.argv[1])

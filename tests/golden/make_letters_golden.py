@@ -1,7 +1,7 @@
 """Regenerate tests/golden/letters_voxels.npz from the AutoQuantizer
-reference checkout (read-only), e.g.
+reference checkout (read-only), given as the one argument:
 
-    python tests/golden/make_letters_golden.py /root/reference
+    python tests/golden/make_letters_golden.py <reference checkout>
 
 The reference's 3D letters experiment emits particles from the mesh
 mpm_exps/inputs/auto_quant.ply, loaded with load_mesh(..., scale=(0.1, 0.1,
@@ -47,4 +47,6 @@ def main(ref):
 
 
 if __name__ == "__main__":
-    main(sys.argv[1] if len(sys.argv) > 1 else "/root/reference")
+    if len(sys.argv) != 2:
+        sys.exit("usage: python %s <path of the AutoQuantizer reference checkout>" % sys.argv[0])
+    main(sys.argv[1])

@@ -116,10 +116,19 @@ def test_dam_break_record_is_152_bits():
     assert cfg.v_exp_bits == 6
 
 
-def test_every_entry_point_is_mapped_in_the_integration_notes():
-    """INTEGRATION.md names, for every function include/aq.h declares, the
-    reference interface it replaces (families may be named with a `*`)."""
-    doc = open(os.path.join(ROOT, "INTEGRATION.md")).read()
-    families = [p[:-1] for p in re.findall(r"`(aq_[a-z_0-9]+\*)`", doc)]
-    missing = [f for f in declared_functions() if "`%s`" % f not in doc and not any(f.startswith(p) for p in families)]
+def test_every_entry_point_is_mapped_to_a_reference_interface():
+    """include/aq_reference_map.json names, for every function include/aq.h
+    declares, the reference interface it replaces (families may be named
+    with a `*`), and names no function the header does not declare."""
+    import json
+
+    with open(os.path.join(ROOT, "include", "aq_reference_map.json")) as f:
+        rows = json.load(f)["rows"]
+    names = [n for r in rows for n in r["entry_points"]]
+    assert all(r["replaces"].strip() for r in rows)
+    families = [n[:-1] for n in names if n.endswith("*")]
+    exact = set(n for n in names if not n.endswith("*"))
+    declared = declared_functions()
+    missing = [f for f in declared if f not in exact and not any(f.startswith(p) for p in families)]
     assert not missing, missing
+    assert not exact - set(declared), exact - set(declared)

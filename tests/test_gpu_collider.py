@@ -6,8 +6,7 @@ import numpy as np
 import pytest
 
 from autoquantizer_b200 import scenes
-from helpers import twin
-from test_gpu_substep import _compare
+from helpers import compare_states, twin
 
 pytestmark = pytest.mark.gpu
 
@@ -49,7 +48,7 @@ def test_collider_matches_oracle(steps, jit):
     o.substeps(steps)
     assert s.kernel_is_jit() == jit
     assert s.status()[0] == 0
-    _compare(s, o, 2e-5)
+    compare_states(s, o, 2e-5)
     th, hh = s.collider_state()
     assert th == pytest.approx(0.3 + 5.0 * cfg.dt * steps, rel=1e-12)
     assert hh == pytest.approx(0.1 * cfg.dt * steps, rel=1e-12)
@@ -89,3 +88,43 @@ def test_autodiff_pass_runs_with_a_collider():
     a, b = grads(True), grads(False)
     assert np.all(np.isfinite(a)) and np.all(a >= 0)
     assert not np.allclose(a, b, rtol=1e-6, atol=0)
+
+
+def test_nlogn_step_forward_follows_the_autodiff_collider_schedule():
+    """nlogn_step_forward(s) (mpm_solver.py:1161-1167) runs the autodiff
+    path's substep, whose collider takes its velocity from the node itself
+    (sdf_collision_no_arg), then puts the collider at step_collider_difftaichi
+    (s): angle omega dt s, height 0.15 dt s.  Checked against the oracle run
+    through the same schedule, and the pose after every call."""
+    cfg, vals = _scene()
+    s, o = twin(cfg, vals)
+    sdf, normal = bar_sdf()
+    s.init_sdf_value(sdf, normal, theta=0.3, omega=5.0)
+    o.set_collider(sdf, normal, offset=(0, 0, 0), center=32, theta=0.3, omega=5.0, node_velocity=True)
+    emitted = []
+    for k in range(5):
+        s.nlogn_step_forward(k, emit_func=lambda step, mpm: emitted.append(step))
+        o.substeps(1)
+        o.col_theta, o.col_height = 5.0 * cfg.dt * k, 0.15 * cfg.dt * k
+        th, hh = s.collider_state()
+        assert th == pytest.approx(5.0 * cfg.dt * k, abs=1e-15)
+        assert hh == pytest.approx(0.15 * cfg.dt * k, abs=1e-15)
+    assert emitted == list(range(5))
+    assert s.status()[0] == 0
+    compare_states(s, o, 2e-5)
+    # the node-velocity form really differs from the forward substep's
+    s2, _ = twin(cfg, vals)
+    s2.init_sdf_value(sdf, normal, theta=0.3, omega=5.0)
+    for k in range(5):
+        s2.substep(k)
+        s2.step_collider_difftaichi(k)
+    assert not np.array_equal(s.words(), s2.words())
+
+
+def test_substep_difftaichi_keeps_the_collider_pose():
+    cfg, vals = _scene()
+    s, _ = twin(cfg, vals)
+    sdf, normal = bar_sdf()
+    s.init_sdf_value(sdf, normal, theta=0.3, height=0.01, omega=5.0)
+    s.substep_difftaichi(0, 1)
+    assert s.collider_state() == pytest.approx((0.3, 0.01), abs=1e-15)

@@ -93,3 +93,31 @@ def test_pipeline_end_to_end_reproduces_reference_scheme(tmp_path):
     assert f["compression_rate"] == pytest.approx(0.5, abs=0.05)
     assert np.all(np.isfinite(f["losses"]))
 
+
+
+def test_detect_bound_kernel_folds_only_the_states_it_is_called_on():
+    """detect_bound_kernel (update_limits_*, mpm_solver.py:943-979) folds the
+    state at the call and nothing in between: called twice, three substeps
+    apart, the limits are the max |q| of exactly those two states."""
+    from autoquantizer_b200 import scenes
+    from autoquantizer_b200.mpm_solver import MPMSolver
+
+    cfg, vals = scenes.falling_block_3d(n=8000, n_grid=32)
+    vals[:, 3] = 2.0
+    s = MPMSolver(cfg)
+    s.set_particles(vals)
+    s.substeps(2)
+    s.detect_bound_kernel(0)
+    a = s.state_values()
+    s.substeps(3)
+    s.detect_bound_kernel(1)
+    b = s.state_values()
+    s.substeps(4)  # not folded
+    s.detect_bound()
+    d = cfg.dim
+    expect = np.maximum(np.abs(a), np.abs(b)).max(0)[d:]
+    lim = s.get_limits()
+    assert np.array_equal(lim[:d], [2.0] * d)
+    np.testing.assert_allclose(lim[d:], expect, rtol=1e-12, atol=0)
+    c = s.state_values()
+    assert np.any(np.abs(c).max(0)[d:] > expect)  # the later state would have widened them
