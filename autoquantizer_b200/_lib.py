@@ -16,7 +16,7 @@ AQ_MAX_MATERIALS = 4
 
 AQ_FIXED, AQ_INT, AQ_FLOAT_EXP, AQ_SHARED_EXP, AQ_RAW_F32, AQ_RAW_F64 = range(6)
 AQ_MAT_FLUID, AQ_MAT_ELASTIC, AQ_MAT_COROTATED = range(3)
-AQ_ST_OUT_OF_DOMAIN, AQ_ST_NAN, AQ_ST_FALLBACK = 0x1, 0x2, 0x4
+AQ_ST_OUT_OF_DOMAIN, AQ_ST_NAN, AQ_ST_FALLBACK, AQ_ST_POOL_FULL = 0x1, 0x2, 0x4, 0x8
 
 ERRORS = {0: "ok", -1: "bad argument", -2: "layout does not fit the simulator schema", -3: "CUDA error",
           -4: "device allocation failed", -5: "call not valid in the current state",
@@ -27,7 +27,7 @@ EXPORTS = [
     "aq_layout_build", "aq_encode", "aq_decode", "aq_sim_create", "aq_sim_destroy", "aq_sim_set_state",
     "aq_sim_get_state", "aq_sim_set_words", "aq_sim_get_words", "aq_sim_substeps", "aq_sim_loss",
     "aq_sim_field_stats", "aq_sim_set_collider", "aq_sim_collider_get", "aq_sim_collider_pose",
-    "aq_sim_collider_velocity_mode", "aq_sim_grid_mass", "aq_voxelize", "aq_adjoint_set_collider",
+    "aq_sim_collider_velocity_mode", "aq_sim_sparse_blocks", "aq_sim_grid_mass", "aq_voxelize", "aq_adjoint_set_collider",
     "aq_sim_ranges_enable", "aq_sim_ranges_get", "aq_sim_status", "aq_sim_step_count", "aq_sim_set_step_count", "aq_sim_launches",
     "aq_state_error", "aq_error_string", "aq_abi_version", "aq_sim_profile_enable", "aq_sim_profile_get",
     "aq_sim_kernel_is_jit", "aq_adjoint_create", "aq_adjoint_destroy", "aq_adjoint_forward", "aq_adjoint_backward",
@@ -65,7 +65,8 @@ class Params(C.Structure):
                 ("use_bound_clip", C.c_int32), ("sort_interval", C.c_int32), ("jit", C.c_int32),
                 ("dx", C.c_double), ("dt", C.c_double), ("p_vol", C.c_double), ("p_mass", C.c_double),
                 ("gravity", C.c_double), ("lb", C.c_double * 3), ("ub", C.c_double * 3),
-                ("mat", Material * AQ_MAX_MATERIALS), ("n_particles", C.c_int64), ("seed", C.c_uint64)]
+                ("mat", Material * AQ_MAX_MATERIALS), ("n_particles", C.c_int64), ("seed", C.c_uint64),
+                ("sparse", C.c_int32), ("reserved", C.c_int32)]
 
 
 class AqError(RuntimeError):
@@ -109,6 +110,7 @@ def lib():
         "aq_sim_collider_get": ([vp, C.POINTER(C.c_double), C.POINTER(C.c_double)], C.c_int),
         "aq_sim_collider_pose": ([vp, C.c_double, C.c_double], C.c_int),
         "aq_sim_collider_velocity_mode": ([vp, i32], C.c_int),
+        "aq_sim_sparse_blocks": ([vp, C.POINTER(C.c_int64), C.POINTER(C.c_int64), vp], C.c_int),
         "aq_sim_ranges_enable": ([vp, i32, vp], C.c_int),
         "aq_sim_ranges_get": ([vp, C.POINTER(C.c_double), C.POINTER(C.c_double), vp], C.c_int),
         "aq_sim_status": ([vp, C.POINTER(C.c_uint32), C.POINTER(C.c_int64), i32, vp], C.c_int),

@@ -8,7 +8,8 @@ substep is hand-written CUDA (libaq: aq_adjoint_*), checkpointed every
 `every` substeps with each segment recomputed during the backward pass.
 
     adj = Adjoint(params)                      # aq_params of an unquantized state
-    sT = adj.forward(s0, n_substeps, every)    # (n x n_slots) cuda tensors
+    sT = adj.forward(s0, n_substeps, every)    # (n x n_slots) cuda tensors;
+                                               # every = 0: logarithmic stash
     g0, sens = adj.backward(dL_dsT)            # dL/ds0 and per-slot sum of
                                                # (dL/ds_t)^2, t = 1..T-1
 

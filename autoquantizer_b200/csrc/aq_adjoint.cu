@@ -37,6 +37,7 @@
 #include <string.h>
 
 #include <algorithm>
+#include <cub/device/device_radix_sort.cuh>
 #include <new>
 #include <vector>
 
@@ -614,6 +615,41 @@ __global__ void k_ad_accum(const R* __restrict__ ab, int64_t n, int ns, double* 
   for (int s = threadIdx.x; s < ns; s += blockDim.x) atomicAdd(&sens[s], shs[s]);
 }
 
+// Particle order for locality: the key of a particle is its base cell
+// (row-major), clamped to the grid; sorting the state by it once per forward
+// pass puts the particles a warp scatters from and gathers into next to
+// each other on the grid (they move little over an adjoint horizon).
+template <class R>
+__global__ void k_ad_keys(const R* __restrict__ st, int64_t n, int ns, int D, int r0, int r1, int r2, R inv_dx,
+                          int32_t* __restrict__ keys, int32_t* __restrict__ idx) {
+  const int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  const int res[3] = {r0, r1, r2};
+  int64_t key = 0;
+  for (int d = 0; d < D; ++d) {
+    const R t = st[i * ns + d] * inv_dx - (R)0.5;
+    int b = t == t ? (int)floor(t) : 0;
+    b = min(max(b, 0), res[d] - 1);
+    key = key * res[d] + b;
+  }
+  keys[i] = (int32_t)key;
+  idx[i] = (int32_t)i;
+}
+
+// rows of a state: out[i] = in[perm[i]] (gather) or out[perm[i]] = in[i]
+template <class R>
+__global__ void k_ad_permute(const R* __restrict__ in, R* __restrict__ out, const int32_t* __restrict__ perm, int64_t n,
+                             int ns, int gather) {
+  const int64_t k = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (k >= n * ns) return;
+  const int64_t i = k / ns, s = k - i * ns;
+  const int64_t j = perm[i];
+  if (gather)
+    out[i * ns + s] = in[j * ns + s];
+  else
+    out[j * ns + s] = in[i * ns + s];
+}
+
 // --------------------------------------------------------------- host
 
 struct AdBase {
@@ -622,6 +658,8 @@ struct AdBase {
   virtual int step(const void* in, void* out, int t, cudaStream_t st) = 0;
   virtual int step_bwd(const void* s_in, const void* ab_out, void* ab_in, int t, cudaStream_t st) = 0;
   virtual int accum(const void* ab, double* sens, cudaStream_t st) = 0;
+  virtual int sort_keys(const void* s0, int32_t* keys, int32_t* idx, cudaStream_t st) = 0;
+  virtual int permute(const void* in, void* out, bool gather, cudaStream_t st) = 0;
 };
 
 }  // namespace aq
@@ -634,9 +672,12 @@ struct aq_adjoint {
   void* grid = nullptr;  // (m, P) per node
   void* gv = nullptr;    // grid velocity per node
   void* gvb = nullptr;   // velocity adjoint, then (m, P) adjoint
-  std::vector<void*> ckpt;  // states at multiples of the checkpoint interval
-  std::vector<void*> seg;   // states of one segment (recomputed)
+  std::vector<void*> ckpt;  // states at multiples of the checkpoint interval (every > 0), or the initial state
+  std::vector<void*> seg;   // states of one segment (recomputed); two ping-pong states (every == 0)
+  std::vector<void*> stash;  // bisection checkpointing: one state per recursion level, plus a scratch state
   int T = 0, every = 0;
+  int32_t* perm = nullptr;  // sorted position -> caller's particle index (length n)
+  int64_t recomputed = 0;   // forward substeps run again by the last backward pass
   double* dsens = nullptr;
   aq::AdBase* impl = nullptr;
   // SDF collider (aq_adjoint_set_collider): caller-owned volumes; at
@@ -726,7 +767,87 @@ struct AdImpl final : AdBase {
     AQ_CUDA_TRY(cudaGetLastError());
     return AQ_OK;
   }
+  int sort_keys(const void* s0, int32_t* keys, int32_t* idx, cudaStream_t st) override {
+    k_ad_keys<R><<<grid_for(a->n, 256), 256, 0, st>>>((const R*)s0, a->n, a->NS, D, K.res[0], K.res[1], K.res[2],
+                                                      K.inv_dx, keys, idx);
+    AQ_CUDA_TRY(cudaGetLastError());
+    return AQ_OK;
+  }
+  int permute(const void* in, void* out, bool gather, cudaStream_t st) override {
+    k_ad_permute<R><<<grid_for(a->n * a->NS, 256), 256, 0, st>>>((const R*)in, (R*)out, a->perm, a->n, a->NS,
+                                                                 gather ? 1 : 0);
+    AQ_CUDA_TRY(cudaGetLastError());
+    return AQ_OK;
+  }
 };
+
+// Sort the particles by base cell: a->perm[sorted position] = caller's index.
+static int ad_make_perm(aq_adjoint* a, const void* d_s0, cudaStream_t st) {
+  if (!a->perm) AQ_CUDA_TRY(cudaMalloc((void**)&a->perm, sizeof(int32_t) * a->n));
+  int32_t* tmp = nullptr;  // keys in, keys out, idx in
+  AQ_CUDA_TRY(cudaMallocAsync((void**)&tmp, sizeof(int32_t) * 3 * a->n, st));
+  int32_t *kin = tmp, *kout = tmp + a->n, *iin = tmp + 2 * a->n;
+  int rc = a->impl->sort_keys(d_s0, kin, iin, st);
+  int bits = 1;
+  while (bits < 31 && (int64_t(1) << bits) < a->ncell) ++bits;
+  size_t tb = 0;
+  // keys are non-negative: sorted as unsigned over their low `bits` bits
+  uint32_t *uk = reinterpret_cast<uint32_t*>(kin), *uo = reinterpret_cast<uint32_t*>(kout);
+  if (rc == AQ_OK &&
+      cub::DeviceRadixSort::SortPairs(nullptr, tb, uk, uo, iin, a->perm, (int)a->n, 0, bits, st) != cudaSuccess)
+    rc = AQ_E_CUDA;
+  void* temp = nullptr;
+  if (rc == AQ_OK && cudaMallocAsync(&temp, tb ? tb : 1, st) != cudaSuccess) rc = AQ_E_NOMEM;
+  if (rc == AQ_OK &&
+      cub::DeviceRadixSort::SortPairs(temp, tb, uk, uo, iin, a->perm, (int)a->n, 0, bits, st) != cudaSuccess)
+    rc = AQ_E_CUDA;
+  if (temp) cudaFreeAsync(temp, st);
+  cudaFreeAsync(tmp, st);
+  return rc;
+}
+
+// Run substeps t0 .. t0 + k - 1 from the state in `in` (k >= 1), landing the
+// state t0 + k in `dst` and using `tmp` as the other buffer; `in` is kept.
+static int ad_run(aq_adjoint* a, const void* in, int t0, int k, void* dst, void* tmp, cudaStream_t st) {
+  void* bufs[2] = {dst, tmp};
+  int j = (k % 2 == 1) ? 0 : 1;  // so that the last substep writes dst
+  const void* src = in;
+  for (int i = 0; i < k; ++i) {
+    void* out = bufs[j];
+    const int rc = a->impl->step(src, out, t0 + i, st);
+    if (rc) return rc;
+    src = out;
+    j ^= 1;
+  }
+  a->recomputed += k;
+  return AQ_OK;
+}
+
+// Bisection checkpointing (the reference's logarithmic stash,
+// run_forward_with_ad_nlogn / rerun_from / cnt_ending_zero,
+// mpm_solver.py:1093-1137,1201-1207, restated as a recursion): to reverse
+// substeps [t0, t1) from the state t0 in `buf`, run forward to the midpoint
+// m, keep the state m in this level's stash, reverse [m, t1) with it, then
+// reverse [t0, m) from `buf` (reusing the level's stash, which is free
+// again).  Memory: one state per level (ceil(log2 T)); recomputation: about
+// T log2(T) / 2 substeps.  ab[cur] holds the adjoint of state t1 on entry and
+// of state t0 on return.
+static int ad_reverse_bisect(aq_adjoint* a, int t0, int t1, const void* buf, int level, void** ab, int& cur,
+                             cudaStream_t st) {
+  if (t1 - t0 == 1) {
+    int rc = a->impl->step_bwd(buf, ab[cur], ab[1 - cur], t0, st);
+    if (rc) return rc;
+    cur = 1 - cur;
+    if (t0 >= 1 && (rc = a->impl->accum(ab[cur], a->dsens, st))) return rc;
+    return AQ_OK;
+  }
+  const int m = t0 + (t1 - t0 + 1) / 2;
+  void* mid = a->stash[level];
+  int rc = ad_run(a, buf, t0, m - t0, mid, a->stash.back(), st);
+  if (rc) return rc;
+  if ((rc = ad_reverse_bisect(a, m, t1, mid, level + 1, ab, cur, st))) return rc;
+  return ad_reverse_bisect(a, t0, m, buf, level, ab, cur, st);
+}
 
 template <int D, class R>
 static AdBase* make_ad(aq_adjoint* a) {
@@ -741,6 +862,9 @@ static void free_ad(aq_adjoint* a) {
     if (p) cudaFree(p);
   for (void* p : a->seg)
     if (p) cudaFree(p);
+  for (void* p : a->stash)
+    if (p) cudaFree(p);
+  if (a->perm) cudaFree(a->perm);
   if (a->grid) cudaFree(a->grid);
   if (a->gv) cudaFree(a->gv);
   if (a->gvb) cudaFree(a->gvb);
@@ -832,30 +956,38 @@ int aq_adjoint_destroy(aq_adjoint* a) {
 
 int aq_adjoint_forward(aq_adjoint* a, const void* d_s0, int32_t n_substeps, int32_t every, void* d_sT,
                        void* stream) {
-  if (!a || !d_s0 || !d_sT || n_substeps < 1 || every < 1) return AQ_E_ARG;
+  if (!a || !d_s0 || !d_sT || n_substeps < 1 || every < 0) return AQ_E_ARG;
   cudaStream_t st = as_stream(stream);
   const size_t sbytes = a->rsz * a->NS * a->n;
-  const int nck = (n_substeps + every - 1) / every;
+  const bool bisect = every == 0;
+  const int nck = bisect ? 1 : (n_substeps + every - 1) / every;
+  const int nseg = bisect ? 2 : every + 1;
   for (void* p : a->ckpt) cudaFree(p);
   a->ckpt.assign(nck, nullptr);
   for (int k = 0; k < nck; ++k) AQ_CUDA_TRY(cudaMalloc(&a->ckpt[k], sbytes));
-  if ((int)a->seg.size() != every + 1) {
+  if ((int)a->seg.size() != nseg) {
     for (void* p : a->seg) cudaFree(p);
-    a->seg.assign(every + 1, nullptr);
-    for (int k = 0; k <= every; ++k) AQ_CUDA_TRY(cudaMalloc(&a->seg[k], sbytes));
+    a->seg.assign(nseg, nullptr);
+    for (int k = 0; k < nseg; ++k) AQ_CUDA_TRY(cudaMalloc(&a->seg[k], sbytes));
   }
+  for (void* p : a->stash) cudaFree(p);
+  a->stash.clear();
   a->T = n_substeps;
   a->every = every;
-  AQ_CUDA_TRY(cudaMemcpyAsync(a->seg[0], d_s0, sbytes, cudaMemcpyDeviceToDevice, st));
+  // the state is kept sorted by base cell (a->perm); the caller's order is
+  // restored for d_sT here and for the gradients in aq_adjoint_backward
+  int rc = ad_make_perm(a, d_s0, st);
+  if (rc) return rc;
+  if ((rc = a->impl->permute(d_s0, a->seg[0], true, st))) return rc;
   int cur = 0;
   for (int t = 0; t < n_substeps; ++t) {
-    if (t % every == 0) AQ_CUDA_TRY(cudaMemcpyAsync(a->ckpt[t / every], a->seg[cur], sbytes, cudaMemcpyDeviceToDevice, st));
-    const int rc = a->impl->step(a->seg[cur], a->seg[1 - cur], t, st);
+    if ((bisect && t == 0) || (!bisect && t % every == 0))
+      AQ_CUDA_TRY(cudaMemcpyAsync(a->ckpt[bisect ? 0 : t / every], a->seg[cur], sbytes, cudaMemcpyDeviceToDevice, st));
+    rc = a->impl->step(a->seg[cur], a->seg[1 - cur], t, st);
     if (rc) return rc;
     cur = 1 - cur;
   }
-  AQ_CUDA_TRY(cudaMemcpyAsync(d_sT, a->seg[cur], sbytes, cudaMemcpyDeviceToDevice, st));
-  return AQ_OK;
+  return a->impl->permute(a->seg[cur], d_sT, false, st);
 }
 
 int aq_adjoint_backward(aq_adjoint* a, const void* d_seed, void* d_grad_s0, double* h_sens, void* stream) {
@@ -865,11 +997,23 @@ int aq_adjoint_backward(aq_adjoint* a, const void* d_seed, void* d_grad_s0, doub
   void* ab[2] = {nullptr, nullptr};
   AQ_CUDA_TRY(cudaMallocAsync(&ab[0], sbytes, st));
   AQ_CUDA_TRY(cudaMallocAsync(&ab[1], sbytes, st));
-  AQ_CUDA_TRY(cudaMemcpyAsync(ab[0], d_seed, sbytes, cudaMemcpyDeviceToDevice, st));
+  int rc0 = a->impl->permute(d_seed, ab[0], true, st);  // into the sorted order of the forward pass
+  if (rc0) return rc0;
   AQ_CUDA_TRY(cudaMemsetAsync(a->dsens, 0, sizeof(double) * a->NS, st));
   int cur = 0;  // ab[cur] = adjoint of state t+1
   const int T = a->T, every = a->every;
-  for (int sgi = (T - 1) / every; sgi >= 0; --sgi) {
+  a->recomputed = 0;
+  if (every == 0) {
+    int levels = 1;
+    while ((1 << levels) < T) ++levels;
+    if (a->stash.empty()) {
+      a->stash.assign(levels + 1, nullptr);  // one per level, the last one is scratch
+      for (void*& p : a->stash) AQ_CUDA_TRY(cudaMalloc(&p, sbytes));
+    }
+    const int rc = ad_reverse_bisect(a, 0, T, a->ckpt[0], 0, ab, cur, st);
+    if (rc) return rc;
+  }
+  for (int sgi = every == 0 ? -1 : (T - 1) / every; sgi >= 0; --sgi) {
     const int t0 = sgi * every, t1 = std::min(T, t0 + every);
     AQ_CUDA_TRY(cudaMemcpyAsync(a->seg[0], a->ckpt[sgi], sbytes, cudaMemcpyDeviceToDevice, st));
     for (int t = t0; t < t1 - 1; ++t) {
@@ -886,7 +1030,10 @@ int aq_adjoint_backward(aq_adjoint* a, const void* d_seed, void* d_grad_s0, doub
       }
     }
   }
-  if (d_grad_s0) AQ_CUDA_TRY(cudaMemcpyAsync(d_grad_s0, ab[cur], sbytes, cudaMemcpyDeviceToDevice, st));
+  if (d_grad_s0) {
+    const int rc = a->impl->permute(ab[cur], d_grad_s0, false, st);
+    if (rc) return rc;
+  }
   if (h_sens) AQ_CUDA_TRY(cudaMemcpyAsync(h_sens, a->dsens, sizeof(double) * a->NS, cudaMemcpyDeviceToHost, st));
   AQ_CUDA_TRY(cudaFreeAsync(ab[0], st));
   AQ_CUDA_TRY(cudaFreeAsync(ab[1], st));

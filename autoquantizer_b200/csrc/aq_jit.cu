@@ -153,7 +153,7 @@ bool jit_available() {
   return g_nv.ok && g_dr.ok;
 }
 
-void* jit_k_step(int D, bool HF, bool HM, bool f64, bool col, const aq_layout& L, std::string* err) {
+void* jit_k_step(int D, bool HF, bool HM, bool f64, bool col, bool sparse, const aq_layout& L, std::string* err) {
   std::lock_guard<std::mutex> g(g_mu);
   init_once();
   if (!g_nv.ok || !g_dr.ok) {
@@ -161,8 +161,8 @@ void* jit_k_step(int D, bool HF, bool HM, bool f64, bool col, const aq_layout& L
     return nullptr;
   }
   char name[160];
-  snprintf(name, sizeof name, "aq::k_step<%d, %s, %s, %s, aq::JitLayout, %s>", D, HF ? "true" : "false",
-           HM ? "true" : "false", f64 ? "double" : "float", col ? "true" : "false");
+  snprintf(name, sizeof name, "aq::k_step<%d, %s, %s, %s, aq::JitLayout, %s, %s>", D, HF ? "true" : "false",
+           HM ? "true" : "false", f64 ? "double" : "float", col ? "true" : "false", sparse ? "true" : "false");
   std::string src = "#include \"aq_kernels.cuh\"\nnamespace aq {\n";
   src += jit_layout_source(L);
   src += "}\n";

@@ -10,9 +10,9 @@
 namespace aq {
 
 bool jit_available();
-// Compile (or fetch from the in-process cache) k_step<D, HF, HM, R, JitLayout>
-// for layout L; returns a CUfunction, or null with *err set.
-void* jit_k_step(int D, bool HF, bool HM, bool f64, bool col, const aq_layout& L, std::string* err);
+// Compile (or fetch from the in-process cache) k_step<D, HF, HM, R, JitLayout,
+// col, sparse> for layout L; returns a CUfunction, or null with *err set.
+void* jit_k_step(int D, bool HF, bool HM, bool f64, bool col, bool sparse, const aq_layout& L, std::string* err);
 std::string jit_layout_source(const aq_layout& L);
 
 // Whether the layout-specialized k_step keeps a record's words in

@@ -136,6 +136,12 @@ struct StepArgs {
   uint64_t sk;          // dithering key of the G2P substep
   int do_g2p, do_p2g, ranges;
   int raw_in;           // grid_in holds P2G sums: apply grid_op while reading
+  // sparse grids (k_step's SP): grid block -> pool slot (-1: none), the
+  // slots handed out so far, each slot's block, the pools' capacity
+  int32_t* bptr;
+  int32_t* n_alloc;
+  int32_t* pool_blk;
+  int pool_cap;
 };
 
 // Layout from the kernel parameter (nvcc build).
@@ -202,6 +208,44 @@ __device__ __forceinline__ void atomic_min_d(double* a, double v) {
     if (prev == old) break;
     old = prev;
   }
+}
+
+// ------------------------------------------------------------ sparse grids
+// A sparse grid stores its nodes in pools of node blocks (the BS^D nodes of
+// one grid block, row-major inside it), reached through a table from grid
+// block (row-major over blocks) to pool slot; -1: the block holds no node,
+// which reads as zero.  Both pools (P2G target and G2P source) share the
+// table.  Slots are handed out by one counter; the pools' slots at and
+// beyond it are kept zero.
+
+template <int D>
+__device__ __forceinline__ int64_t block_of(const int (&nb)[3], int i0, int i1, int i2) {
+  constexpr int BS = Geo<D>::BS;
+  return D == 3 ? ((int64_t)(i0 / BS) * nb[1] + i1 / BS) * nb[2] + i2 / BS : (int64_t)(i0 / BS) * nb[1] + i1 / BS;
+}
+
+template <int D>
+__device__ __forceinline__ int64_t node_in_slot(int slot, int i0, int i1, int i2) {
+  constexpr int BS = Geo<D>::BS;
+  const int l0 = i0 & (BS - 1), l1 = i1 & (BS - 1), l2 = i2 & (BS - 1);
+  return (int64_t)slot * 64 + (D == 3 ? (l0 * BS + l1) * BS + l2 : l0 * BS + l1);
+}
+
+// Slot of block blk for a write, handed out now if the block has none: take
+// a slot from the counter, then install it unless another thread installed
+// one first (the slot taken is then left unused, still zero).  No waiting.
+// -1: the pools are full.  Out of line: it runs for few writes.
+static __device__ __noinline__ int claim_slot(int32_t* bptr, int32_t* n_alloc, int32_t* pool_blk, int cap, int64_t blk) {
+  const int s = bptr[blk];
+  if (s >= 0) return s;
+  const int mine = atomicAdd(n_alloc, 1);
+  if (mine >= cap) return -1;
+  const int old = atomicCAS(bptr + blk, -1, mine);
+  if (old == -1) {
+    pool_blk[mine] = (int32_t)blk;
+    return mine;
+  }
+  return old;
 }
 
 // grid_op (mpm_solver.py:633-665) of one node (m, m v) at grid index I:
@@ -406,8 +450,9 @@ __device__ __forceinline__ void bspline(const R* x, const SimK<R>& K, int* base,
 // ------------------------------------------------------------ the step
 
 // COL: compiled with the SDF collider (the library's own build always is;
-// the layout-specialized build only when a collider is set).
-template <int D, bool HF, bool HM, class R, class LA, bool COL = true>
+// the layout-specialized build only when a collider is set).  SP: sparse
+// grids (grid_in / grid_out are node pools reached through A.bptr).
+template <int D, bool HF, bool HM, class R, class LA, bool COL = true, bool SP = false>
 __global__ void __launch_bounds__(CH, AQ_STEP_MIN_BLOCKS(R, LA)) k_step(const __grid_constant__ aq_layout Lp, const SimK<R> K,
                                                 const StepArgs A) {
   typedef Sch<D, HF, HM> S;
@@ -426,6 +471,7 @@ __global__ void __launch_bounds__(CH, AQ_STEP_MIN_BLOCKS(R, LA)) k_step(const __
   uint64_t* srec = reinterpret_cast<uint64_t*>(ptile + NWARP * TNP);  // CH x WS: each thread's record (RtLayout)
   __shared__ int sbox[6];  // tile-coordinate box of the item's P2G base cells (min[3], max[3])
   __shared__ int s_next;   // the CTA's next work item, claimed from A.item_ctr
+  __shared__ int sslot[27];  // sparse grids: pool slots of the 3^D grid blocks around the item's block
 
   const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
   const int nitems = *A.n_items;
@@ -468,6 +514,24 @@ __global__ void __launch_bounds__(CH, AQ_STEP_MIN_BLOCKS(R, LA)) k_step(const __
       o[1] = (blk % K.nb[1]) * G::BS - 1;
       o[0] = (blk / K.nb[1]) * G::BS - 1;
     }
+    // block coordinates of the item; a tile node lies in the blocks ob - 1 .. ob + 1
+    const int ob0 = (o[0] + 1) / G::BS, ob1 = (o[1] + 1) / G::BS, ob2 = D == 3 ? (o[2] + 1) / G::BS : 0;
+    if (SP) {
+      if (tid < (D == 3 ? 27 : 9)) {
+        const int e0 = D == 3 ? tid / 9 : tid / 3, e1 = D == 3 ? (tid / 3) % 3 : tid % 3, e2 = D == 3 ? tid % 3 : 1;
+        const int b0 = ob0 + e0 - 1, b1 = ob1 + e1 - 1, b2 = ob2 + e2 - 1;
+        int sl = -1;
+        if (b0 >= 0 && b0 < K.nb[0] && b1 >= 0 && b1 < K.nb[1] && (D == 2 || (b2 >= 0 && b2 < K.nb[2])))
+          sl = A.bptr[D == 3 ? ((int64_t)b0 * K.nb[1] + b1) * K.nb[2] + b2 : (int64_t)b0 * K.nb[1] + b1];
+        sslot[tid] = sl;
+      }
+      __syncthreads();
+    }
+    // pool slot of an in-grid tile node, from the item's table
+    auto tile_slot = [&](int g0, int g1, int g2) -> int {
+      const int a0 = g0 / G::BS - ob0 + 1, a1 = g1 / G::BS - ob1 + 1, a2 = D == 3 ? g2 / G::BS - ob2 + 1 : 0;
+      return sslot[D == 3 ? (a0 * 3 + a1) * 3 + a2 : a0 * 3 + a1];
+    };
     if (A.do_g2p) {  // stage the grid tile (m, v after grid_op)
       for (int j = tid; j < TNP; j += CH) {
         int l0, l1, l2 = 0;
@@ -485,7 +549,12 @@ __global__ void __launch_bounds__(CH, AQ_STEP_MIN_BLOCKS(R, LA)) k_step(const __
                         (D == 2 || (g2 >= 0 && g2 < K.res[2]));
         R4 g = zero4;
         if (ok) {
-          g = gin[cell_index<D>(K.res, g0, g1, g2)];
+          if (SP) {
+            const int sl = tile_slot(g0, g1, g2);
+            if (sl >= 0) g = gin[node_in_slot<D>(sl, g0, g1, g2)];
+          } else {
+            g = gin[cell_index<D>(K.res, g0, g1, g2)];
+          }
           if (A.raw_in) g = grid_op_node<D, R, COL>(K, g, g0, g1, g2);
         }
         gtile[j] = g;
@@ -577,7 +646,12 @@ __global__ void __launch_bounds__(CH, AQ_STEP_MIN_BLOCKS(R, LA)) k_step(const __
                   g = gtile[lb + (D == 3 ? a * G::XS + b * T + c : a * T + b)];
                 } else {
                   const int n0 = base[0] + a, n1 = base[1] + b, n2 = D == 3 ? base[2] + c : 0;
-                  g = gin[cell_index<D>(K.res, n0, n1, n2)];
+                  if (SP) {
+                    const int sl = A.bptr[block_of<D>(K.nb, n0, n1, n2)];
+                    g = sl >= 0 ? gin[node_in_slot<D>(sl, n0, n1, n2)] : zero4;
+                  } else {
+                    g = gin[cell_index<D>(K.res, n0, n1, n2)];
+                  }
                   if (A.raw_in) g = grid_op_node<D, R, COL>(K, g, n0, n1, n2);
                 }
                 const R gv[3] = {g.y, g.z, g.w};
@@ -773,6 +847,23 @@ __global__ void __launch_bounds__(CH, AQ_STEP_MIN_BLOCKS(R, LA)) k_step(const __
                 }
               }
           } else if (mine) {  // outside the tile: straight to the global grid
+            // sparse grids: slots of the (at most 2^D) blocks under the stencil
+            int fsl[D == 3 ? 8 : 4];
+            const int fb0 = base[0] / G::BS, fb1 = base[1] / G::BS, fb2 = D == 3 ? base[2] / G::BS : 0;
+            if (SP) {
+#pragma unroll 1
+              for (int qb = 0; qb < (D == 3 ? 8 : 4); ++qb) {
+                const int c0 = fb0 + (D == 3 ? qb >> 2 : qb >> 1), c1 = fb1 + (D == 3 ? (qb >> 1) & 1 : qb & 1),
+                          c2 = D == 3 ? fb2 + (qb & 1) : 0;
+                int sl = -1;
+                if (c0 < K.nb[0] && c1 < K.nb[1] && (D == 2 || c2 < K.nb[2])) {
+                  const int64_t bk = D == 3 ? ((int64_t)c0 * K.nb[1] + c1) * K.nb[2] + c2 : (int64_t)c0 * K.nb[1] + c1;
+                  sl = claim_slot(A.bptr, A.n_alloc, A.pool_blk, A.pool_cap, bk);
+                  if (sl < 0) fl |= AQ_ST_POOL_FULL;
+                }
+                fsl[qb] = sl;
+              }
+            }
 #pragma unroll
             for (int a = 0; a < 3; ++a)
 #pragma unroll
@@ -792,8 +883,16 @@ __global__ void __launch_bounds__(CH, AQ_STEP_MIN_BLOCKS(R, LA)) k_step(const __
                     if (D == 3 && c == 2) s += (R)2 * Aff[d * D + 2];
                     mv[d] = weight * s;
                   }
-                  R4* g = gout + cell_index<D>(K.res, base[0] + a, base[1] + b, D == 3 ? base[2] + c : 0);
-                  red_add_node(g, weight * K.p_mass, mv[0], mv[1], mv[2]);
+                  const int n0 = base[0] + a, n1 = base[1] + b, n2 = D == 3 ? base[2] + c : 0;
+                  if (SP) {
+                    const int qb = D == 3 ? ((n0 / G::BS - fb0) << 2) | ((n1 / G::BS - fb1) << 1) | (n2 / G::BS - fb2)
+                                          : ((n0 / G::BS - fb0) << 1) | (n1 / G::BS - fb1);
+                    const int sl = fsl[qb];
+                    if (sl >= 0)
+                      red_add_node(gout + node_in_slot<D>(sl, n0, n1, n2), weight * K.p_mass, mv[0], mv[1], mv[2]);
+                  } else {
+                    red_add_node(gout + cell_index<D>(K.res, n0, n1, n2), weight * K.p_mass, mv[0], mv[1], mv[2]);
+                  }
                 }
           }
           __syncwarp();
@@ -828,7 +927,16 @@ __global__ void __launch_bounds__(CH, AQ_STEP_MIN_BLOCKS(R, LA)) k_step(const __
         const int g0 = o[0] + l0, g1 = o[1] + l1, g2 = o[2] + l2;
         if (g0 < 0 || g0 >= K.res[0] || g1 < 0 || g1 >= K.res[1] || (D == 3 && (g2 < 0 || g2 >= K.res[2])))
           continue;
-        red_add_node(gout + cell_index<D>(K.res, g0, g1, g2), sum.x, sum.y, sum.z, sum.w);
+        if (SP) {
+          int sl = tile_slot(g0, g1, g2);
+          if (sl < 0) sl = claim_slot(A.bptr, A.n_alloc, A.pool_blk, A.pool_cap, block_of<D>(K.nb, g0, g1, g2));
+          if (sl >= 0)
+            red_add_node(gout + node_in_slot<D>(sl, g0, g1, g2), sum.x, sum.y, sum.z, sum.w);
+          else
+            fl |= AQ_ST_POOL_FULL;
+        } else {
+          red_add_node(gout + cell_index<D>(K.res, g0, g1, g2), sum.x, sum.y, sum.z, sum.w);
+        }
       }
     }
     if (tid == 0) s_next = atomicAdd(A.item_ctr, 1);

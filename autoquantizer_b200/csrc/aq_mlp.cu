@@ -5,12 +5,13 @@
 //
 // Parameter vector layout (float32 master, bf16 working copy, same order):
 //   W1[h][in], b1[h], W2[h][h], b2[h], W3[out][h], b3[out]
-// Biases are applied in fp32 from the master copy; weights are read as bf16
-// and every dot product accumulates in fp32.
+// Biases are applied in fp32 from the master copy; weights are read as bf16.
 // Activations saved by the forward pass for the backward pass (fp32):
 //   z1[B][h], a1[B][h], z2[B][h], a2[B][h]
-// The layers are small (4 MFLOP per pass at batch 512): one thread per
-// output element with the operand rows read through L1, no tensor cores.
+// Every contraction (forward, input gradient, weight gradient) runs on the
+// bf16 tensor cores with fp32 accumulation: the operands, weights and
+// activations alike, enter the products rounded to bf16 (round to nearest
+// even); biases, pre-activations, GELU and its derivative stay fp32.
 #include <cuda_bf16.h>
 #include <math.h>
 
@@ -24,47 +25,150 @@ __device__ __forceinline__ float gelu_grad(float z) {
   return 0.5f * (1.0f + erff(z * 0.70710678118654752f)) + z * 0.39894228040143268f * expf(-0.5f * z * z);
 }
 
-// Y[b][n] = act(sum_k X[b][k] W[n][k] + bias[n]); Z (pre-activation) optional
-__global__ void k_dense_fwd(const float* __restrict__ X, const __nv_bfloat16* __restrict__ W,
-                            const float* __restrict__ bias, float* __restrict__ Z, float* __restrict__ Y, int B, int K,
-                            int N, int act) {
-  const int i = blockIdx.x * blockDim.x + threadIdx.x;
-  if (i >= B * N) return;
-  const int b = i / N, n = i - b * N;
-  const float* x = X + (size_t)b * K;
-  const __nv_bfloat16* w = W + (size_t)n * K;
-  float acc = bias[n];
-  for (int k = 0; k < K; ++k) acc = fmaf(x[k], __bfloat162float(w[k]), acc);
-  if (Z) Z[i] = acc;
-  Y[i] = act ? gelu(acc) : acc;
+// ------------------------------------------------------ tensor-core GEMM
+//
+// C[m][n] = sum_k A(m, k) B(n, k) on bf16 tensor cores (mma.sync m16n8k16,
+// fp32 accumulation) with a fused epilogue.  Operands are read from global
+// memory in either major order and staged in shared memory as bf16 rows of
+// k (fp32 sources are rounded to nearest even on the way in):
+//   forward   Y = X W^T          A = X [M][K] (K-major), B = W [N][K] (K-major)
+//   x-grad    dX = dZ W          A = dZ [M][K] (K-major), B(n, k) = W[k][n] (MN-major)
+//   w-grad    dW = dZ^T X        A(m, k) = dZ[k][m] (MN-major), B(n, k) = X[k][n] (MN-major)
+// A CTA of 4 warps computes a 64 x 64 tile of C in k chunks of 64; each
+// warp a 32 x 32 quarter as 2 x 4 mma tiles of 16 x 8.
+
+constexpr int GT = 64;       // CTA tile edge (m and n)
+constexpr int GK = 64;       // k chunk
+constexpr int GKP = GK + 8;  // padded row of the staged chunk (bf16): conflict-free 32-bit fragment loads
+
+enum { EPI_FWD = 0, EPI_XGRAD = 1, EPI_STORE = 2 };
+
+template <class T>
+__device__ __forceinline__ float ld_f(const T* p, int64_t i);
+template <>
+__device__ __forceinline__ float ld_f<float>(const float* p, int64_t i) {
+  return p[i];
+}
+template <>
+__device__ __forceinline__ float ld_f<__nv_bfloat16>(const __nv_bfloat16* p, int64_t i) {
+  return __bfloat162float(p[i]);
 }
 
-// dW[n][k] = sum_b dZ[b][n] X[b][k];  db[n] = sum_b dZ[b][n]
-__global__ void k_dense_wgrad(const float* __restrict__ dZ, const float* __restrict__ X, float* __restrict__ dW,
-                              float* __restrict__ db, int B, int K, int N) {
-  const int i = blockIdx.x * blockDim.x + threadIdx.x;
-  if (i >= N * (K + 1)) return;
-  const int n = i / (K + 1), k = i - n * (K + 1);
-  float acc = 0.f;
-  if (k < K) {
-    for (int b = 0; b < B; ++b) acc = fmaf(dZ[(size_t)b * N + n], X[(size_t)b * K + k], acc);
-    dW[(size_t)n * K + k] = acc;
-  } else {
-    for (int b = 0; b < B; ++b) acc += dZ[(size_t)b * N + n];
-    db[n] = acc;
+// Stage rows [r0, r0 + GT) x k [k0, k0 + GK) of an operand into s[GT][GKP]
+// (zeros outside [R, K)).  kmajor: element (r, k) at src[r * ld + k], else
+// at src[k * ld + r].
+template <class T>
+__device__ __forceinline__ void stage(__nv_bfloat16 (*s)[GKP], const T* src, int64_t ld, bool kmajor, int r0, int R,
+                                      int k0, int K) {
+  for (int i = threadIdx.x; i < GT * GK / 2; i += blockDim.x) {
+    int r, kk;
+    if (kmajor) {  // consecutive threads along k
+      r = i / (GK / 2);
+      kk = 2 * (i - r * (GK / 2));
+    } else {  // consecutive threads along r
+      kk = 2 * (i / GT);
+      r = i - (kk / 2) * GT;
+    }
+    const int gr = r0 + r, gk = k0 + kk;
+    float v0 = 0.f, v1 = 0.f;
+    if (gr < R) {
+      if (gk < K) v0 = ld_f(src, kmajor ? (int64_t)gr * ld + gk : (int64_t)gk * ld + gr);
+      if (gk + 1 < K) v1 = ld_f(src, kmajor ? (int64_t)gr * ld + gk + 1 : (int64_t)(gk + 1) * ld + gr);
+    }
+    *reinterpret_cast<__nv_bfloat162*>(&s[r][kk]) = __floats2bfloat162_rn(v0, v1);
   }
 }
 
-// dX[b][k] = (sum_n dZ[b][n] W[n][k]) * (gelu'(Zprev[b][k]) if act)
-__global__ void k_dense_xgrad(const float* __restrict__ dZ, const __nv_bfloat16* __restrict__ W,
-                              const float* __restrict__ Zprev, float* __restrict__ dX, int B, int K, int N, int act) {
-  const int i = blockIdx.x * blockDim.x + threadIdx.x;
-  if (i >= B * K) return;
-  const int b = i / K, k = i - b * K;
-  float acc = 0.f;
-  for (int n = 0; n < N; ++n) acc = fmaf(dZ[(size_t)b * N + n], __bfloat162float(W[(size_t)n * K + k]), acc);
-  dX[i] = act ? acc * gelu_grad(Zprev[i]) : acc;
+__device__ __forceinline__ void mma_bf16(float (&d)[4], uint32_t a0, uint32_t a1, uint32_t a2, uint32_t a3,
+                                         uint32_t b0, uint32_t b1) {
+  asm volatile(
+      "mma.sync.aligned.m16n8k16.row.col.f32.bf16.bf16.f32 {%0, %1, %2, %3}, {%4, %5, %6, %7}, {%8, %9}, "
+      "{%0, %1, %2, %3};\n"
+      : "+f"(d[0]), "+f"(d[1]), "+f"(d[2]), "+f"(d[3])
+      : "r"(a0), "r"(a1), "r"(a2), "r"(a3), "r"(b0), "r"(b1));
 }
+
+// epi: EPI_FWD   Z = acc + bias[n] (stored when Z), out = act ? gelu(Z) : Z
+//      EPI_XGRAD out = act ? acc * gelu'(aux[m][n]) : acc
+//      EPI_STORE out = acc
+template <class TA, class TB, int EPI>
+__global__ void __launch_bounds__(128) k_gemm_bf16(const TA* __restrict__ A, int64_t lda, int a_kmajor,
+                                                   const TB* __restrict__ B, int64_t ldb, int b_kmajor, int M, int N,
+                                                   int K, const float* __restrict__ bias, const float* __restrict__ aux,
+                                                   float* __restrict__ Z, float* __restrict__ out, int act) {
+  __shared__ __align__(16) __nv_bfloat16 sA[GT][GKP];
+  __shared__ __align__(16) __nv_bfloat16 sB[GT][GKP];
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  const int g = lane >> 2, t = lane & 3;
+  const int m0 = blockIdx.x * GT, n0 = blockIdx.y * GT;
+  const int wm = (warp >> 1) * 32, wn = (warp & 1) * 32;
+  float acc[2][4][4];
+#pragma unroll
+  for (int i = 0; i < 2; ++i)
+#pragma unroll
+    for (int j = 0; j < 4; ++j)
+#pragma unroll
+      for (int e = 0; e < 4; ++e) acc[i][j][e] = 0.f;
+  for (int k0 = 0; k0 < K; k0 += GK) {
+    stage(sA, A, lda, a_kmajor != 0, m0, M, k0, K);
+    stage(sB, B, ldb, b_kmajor != 0, n0, N, k0, K);
+    __syncthreads();
+#pragma unroll
+    for (int kk = 0; kk < GK; kk += 16) {
+      uint32_t af[2][4], bf[4][2];
+#pragma unroll
+      for (int i = 0; i < 2; ++i) {
+        const int r = wm + 16 * i + g;
+        af[i][0] = *reinterpret_cast<const uint32_t*>(&sA[r][kk + 2 * t]);
+        af[i][1] = *reinterpret_cast<const uint32_t*>(&sA[r + 8][kk + 2 * t]);
+        af[i][2] = *reinterpret_cast<const uint32_t*>(&sA[r][kk + 2 * t + 8]);
+        af[i][3] = *reinterpret_cast<const uint32_t*>(&sA[r + 8][kk + 2 * t + 8]);
+      }
+#pragma unroll
+      for (int j = 0; j < 4; ++j) {
+        const int c = wn + 8 * j + g;
+        bf[j][0] = *reinterpret_cast<const uint32_t*>(&sB[c][kk + 2 * t]);
+        bf[j][1] = *reinterpret_cast<const uint32_t*>(&sB[c][kk + 2 * t + 8]);
+      }
+#pragma unroll
+      for (int i = 0; i < 2; ++i)
+#pragma unroll
+        for (int j = 0; j < 4; ++j) mma_bf16(acc[i][j], af[i][0], af[i][1], af[i][2], af[i][3], bf[j][0], bf[j][1]);
+    }
+    __syncthreads();
+  }
+#pragma unroll
+  for (int i = 0; i < 2; ++i)
+#pragma unroll
+    for (int j = 0; j < 4; ++j)
+#pragma unroll
+      for (int e = 0; e < 4; ++e) {
+        const int m = m0 + wm + 16 * i + g + (e >= 2 ? 8 : 0);
+        const int n = n0 + wn + 8 * j + 2 * t + (e & 1);
+        if (m >= M || n >= N) continue;
+        const int64_t o = (int64_t)m * N + n;
+        float v = acc[i][j][e];
+        if (EPI == EPI_FWD) {
+          v += bias[n];
+          if (Z) Z[o] = v;
+          if (act) v = gelu(v);
+        } else if (EPI == EPI_XGRAD) {
+          if (act) v *= gelu_grad(aux[o]);
+        }
+        out[o] = v;
+      }
+}
+
+// db[n] = sum_b dZ[b][n] in fp32 (one thread per column)
+__global__ void k_colsum(const float* __restrict__ dZ, int B, int N, float* __restrict__ db) {
+  const int n = blockIdx.x * blockDim.x + threadIdx.x;
+  if (n >= N) return;
+  float acc = 0.f;
+  for (int b = 0; b < B; ++b) acc += dZ[(size_t)b * N + n];
+  db[n] = acc;
+}
+
+static dim3 gemm_grid(int M, int N) { return dim3((unsigned)((M + GT - 1) / GT), (unsigned)((N + GT - 1) / GT)); }
 
 // Adam (Kingma & Ba 2015) on the fp32 master parameters, then the bf16 copy
 __global__ void k_adam(float* __restrict__ p, __nv_bfloat16* __restrict__ pb, float* __restrict__ m,
@@ -155,10 +259,12 @@ int aq_mlp_forward(int32_t in, int32_t h, int32_t out, const float* d_params, co
     a1 = tmp;
     a2 = tmp + (size_t)B * h;
   }
-  k_dense_fwd<<<grid_for((int64_t)B * h, 128), 128, 0, st>>>(d_x, wb + o.w1, d_params + o.b1, z1, a1, B, in, h, 1);
-  k_dense_fwd<<<grid_for((int64_t)B * h, 128), 128, 0, st>>>(a1, wb + o.w2, d_params + o.b2, z2, a2, B, h, h, 1);
-  k_dense_fwd<<<grid_for((int64_t)B * out, 128), 128, 0, st>>>(a2, wb + o.w3, d_params + o.b3, nullptr, d_y, B, h,
-                                                                out, 0);
+  k_gemm_bf16<float, __nv_bfloat16, EPI_FWD><<<gemm_grid(B, h), 128, 0, st>>>(
+      d_x, in, 1, wb + o.w1, in, 1, B, h, in, d_params + o.b1, nullptr, z1, a1, 1);
+  k_gemm_bf16<float, __nv_bfloat16, EPI_FWD><<<gemm_grid(B, h), 128, 0, st>>>(
+      a1, h, 1, wb + o.w2, h, 1, B, h, h, d_params + o.b2, nullptr, z2, a2, 1);
+  k_gemm_bf16<float, __nv_bfloat16, EPI_FWD><<<gemm_grid(B, out), 128, 0, st>>>(
+      a2, h, 1, wb + o.w3, h, 1, B, out, h, d_params + o.b3, nullptr, nullptr, d_y, 0);
   AQ_CUDA_TRY(cudaGetLastError());
   if (tmp) AQ_CUDA_TRY(cudaFreeAsync(tmp, st));
   return AQ_OK;
@@ -178,13 +284,22 @@ int aq_mlp_backward(int32_t in, int32_t h, int32_t out, const uint16_t* d_params
   AQ_CUDA_TRY(cudaMallocAsync((void**)&dz, sizeof(float) * 2 * (size_t)B * h, st));
   float* dz2 = dz;
   float* dz1 = dz + (size_t)B * h;
-  k_dense_wgrad<<<grid_for((int64_t)out * (h + 1), 128), 128, 0, st>>>(d_dy, a2, d_grad + o.w3, d_grad + o.b3, B, h,
-                                                                        out);
-  k_dense_xgrad<<<grid_for((int64_t)B * h, 128), 128, 0, st>>>(d_dy, wb + o.w3, z2, dz2, B, h, out, 1);
-  k_dense_wgrad<<<grid_for((int64_t)h * (h + 1), 128), 128, 0, st>>>(dz2, a1, d_grad + o.w2, d_grad + o.b2, B, h, h);
-  k_dense_xgrad<<<grid_for((int64_t)B * h, 128), 128, 0, st>>>(dz2, wb + o.w2, z1, dz1, B, h, h, 1);
-  k_dense_wgrad<<<grid_for((int64_t)h * (in + 1), 128), 128, 0, st>>>(dz1, d_x, d_grad + o.w1, d_grad + o.b1, B, in,
-                                                                       h);
+  // layer 3: dW3 = dy^T a2, db3, dz2 = (dy W3) * gelu'(z2)
+  k_gemm_bf16<float, float, EPI_STORE><<<gemm_grid(out, h), 128, 0, st>>>(
+      d_dy, out, 0, a2, h, 0, out, h, B, nullptr, nullptr, nullptr, d_grad + o.w3, 0);
+  k_colsum<<<grid_for(out, 128), 128, 0, st>>>(d_dy, B, out, d_grad + o.b3);
+  k_gemm_bf16<float, __nv_bfloat16, EPI_XGRAD><<<gemm_grid(B, h), 128, 0, st>>>(
+      d_dy, out, 1, wb + o.w3, h, 0, B, h, out, nullptr, z2, nullptr, dz2, 1);
+  // layer 2
+  k_gemm_bf16<float, float, EPI_STORE><<<gemm_grid(h, h), 128, 0, st>>>(
+      dz2, h, 0, a1, h, 0, h, h, B, nullptr, nullptr, nullptr, d_grad + o.w2, 0);
+  k_colsum<<<grid_for(h, 128), 128, 0, st>>>(dz2, B, h, d_grad + o.b2);
+  k_gemm_bf16<float, __nv_bfloat16, EPI_XGRAD><<<gemm_grid(B, h), 128, 0, st>>>(
+      dz2, h, 1, wb + o.w2, h, 0, B, h, h, nullptr, z1, nullptr, dz1, 1);
+  // layer 1
+  k_gemm_bf16<float, float, EPI_STORE><<<gemm_grid(h, in), 128, 0, st>>>(
+      dz1, h, 0, d_x, in, 0, h, in, B, nullptr, nullptr, nullptr, d_grad + o.w1, 0);
+  k_colsum<<<grid_for(h, 128), 128, 0, st>>>(dz1, B, h, d_grad + o.b1);
   AQ_CUDA_TRY(cudaGetLastError());
   AQ_CUDA_TRY(cudaFreeAsync(dz, st));
   return AQ_OK;

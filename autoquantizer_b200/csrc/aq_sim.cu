@@ -14,6 +14,9 @@
 #include <string.h>
 
 #include <algorithm>
+#include <cub/device/device_radix_sort.cuh>
+#include <cub/device/device_run_length_encode.cuh>
+#include <cub/device/device_scan.cuh>
 #include <new>
 #include <string>
 
@@ -135,8 +138,9 @@ __global__ void k_items_count(const int32_t* __restrict__ start, int nblk, int32
   if (c > 0) atomicAdd(item_info + 1 + item_bucket(c), 1);
 }
 
+// blk_of (sparse grids): the grid block of each compact block index, else null
 __global__ void k_items(const int32_t* __restrict__ start, int nblk, int4* __restrict__ items,
-                        int32_t* __restrict__ item_info) {
+                        int32_t* __restrict__ item_info, const int32_t* __restrict__ blk_of) {
   __shared__ int off[IB];
   if (threadIdx.x == 0) {
     int acc = 0;
@@ -152,7 +156,162 @@ __global__ void k_items(const int32_t* __restrict__ start, int nblk, int4* __res
   const int s = start[(int64_t)b * 64], c = start[(int64_t)(b + 1) * 64] - s;
   if (c <= 0) return;
   const int k = item_bucket(c);
-  items[off[k] + atomicAdd(item_info + 1 + IB + k, 1)] = make_int4(b, s, c, 0);
+  items[off[k] + atomicAdd(item_info + 1 + IB + k, 1)] = make_int4(blk_of ? blk_of[b] : b, s, c, 0);
+}
+
+// ------------------------------------------------- sparse-grid binning
+// The dense binning above counts records per cell of the whole grid; a
+// sparse grid's index space can be far larger than the particles need, so
+// its binning works on occupied blocks only:
+//   k_sbin       grid block and cell-in-block of every record
+//   radix sort   records by grid block (CUB), run-length encoding of the
+//                sorted blocks: the occupied blocks, their record counts
+//   k_occ_keys   compact key (occupied block, cell) and rank in the cell
+//   k_cstart     per occupied block, the exclusive scan of its 64 cell
+//                counts from the block's first record
+// then k_scatter and the work items as in the dense case, with the compact
+// keys and offsets; k_activate hands out pool slots to the 3^D blocks
+// around every occupied block.
+
+template <int D, class R>
+__global__ void __launch_bounds__(256) k_sbin(const __grid_constant__ aq_layout L, const SimK<R> K,
+                                              const uint64_t* __restrict__ words, int64_t n,
+                                              uint32_t* __restrict__ blk_out, int32_t* __restrict__ cslot,
+                                              int32_t* __restrict__ iota, unsigned* __restrict__ status) {
+  const int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  const uint64_t* w = words + i * K.W;
+  unsigned fl = 0;
+  int b[3] = {0, 0, 0};
+#pragma unroll
+  for (int d = 0; d < D; ++d) b[d] = base_of<R>(decode_slot<R>(L, d, w), K, d, fl);
+  constexpr int BS = Geo<D>::BS;
+  blk_out[i] = (uint32_t)block_of<D>(K.nb, b[0], b[1], b[2]);
+  // the dense keys' cell order inside a block (k_bin)
+  cslot[i] = D == 3 ? ((b[1] % BS) * BS + b[0] % BS) * BS + b[2] % BS : (b[0] % BS) * BS + b[1] % BS;
+  iota[i] = (int32_t)i;
+  if (fl) atomicOr(status, fl);
+}
+
+// occupied block of sorted record j by binary search in the blocks' first
+// records; compact key o * 64 + cell and rank within the cell
+__global__ void k_occ_keys(const int32_t* __restrict__ order, const int32_t* __restrict__ cslot,
+                           const int32_t* __restrict__ occ_first, const int32_t* __restrict__ n_occ_p, int64_t n,
+                           int32_t* __restrict__ keys, int32_t* __restrict__ ranks, int32_t* __restrict__ ccount) {
+  const int64_t j = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (j >= n) return;
+  int lo = 0, hi = *n_occ_p - 1;  // last o with occ_first[o] <= j
+  while (lo < hi) {
+    const int mid = (lo + hi + 1) >> 1;
+    if (occ_first[mid] <= j)
+      lo = mid;
+    else
+      hi = mid - 1;
+  }
+  const int p = order[j];
+  const int key = lo * 64 + cslot[p];
+  keys[p] = key;
+  ranks[p] = atomicAdd(&ccount[key], 1);
+}
+
+// one warp per occupied block: cstart[o * 64 + k] = first record of the
+// block + the counts of its cells before k; cstart[n_occ * 64] = n
+__global__ void k_cstart(const int32_t* __restrict__ ccount, const int32_t* __restrict__ occ_first,
+                         const int32_t* __restrict__ n_occ_p, int64_t n, int32_t* __restrict__ cstart) {
+  const int n_occ = *n_occ_p;
+  const int lane = threadIdx.x & 31;
+  const int o = (int)(((int64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5);
+  if (o >= n_occ) {
+    if (o == n_occ && lane == 0) cstart[(int64_t)n_occ * 64] = (int32_t)n;
+    return;
+  }
+  const int c0 = ccount[(int64_t)o * 64 + 2 * lane], c1 = ccount[(int64_t)o * 64 + 2 * lane + 1];
+  int x = c0 + c1;
+#pragma unroll
+  for (int k = 1; k < 32; k <<= 1) {
+    const int y = __shfl_up_sync(0xffffffffu, x, k);
+    if (lane >= k) x += y;
+  }
+  const int before = occ_first[o] + x - c0 - c1;
+  cstart[(int64_t)o * 64 + 2 * lane] = before;
+  cstart[(int64_t)o * 64 + 2 * lane + 1] = before + c0;
+}
+
+// Empty the pools for a new set of active blocks: zero the slots handed out
+// so far in both pools, and their table entries
+template <class R4>
+__global__ void k_pool_reset(int32_t* __restrict__ bptr, int32_t* __restrict__ pool_blk,
+                             const int32_t* __restrict__ n_alloc, int cap, R4* __restrict__ p0, R4* __restrict__ p1) {
+  const int used = min(*n_alloc, cap);
+  R4 z;
+  z.x = z.y = z.z = z.w = 0;
+  for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < (int64_t)used * 64;
+       i += (int64_t)gridDim.x * blockDim.x) {
+    p0[i] = z;
+    p1[i] = z;
+    if ((i & 63) == 0) {
+      const int64_t s = i >> 6;
+      if (pool_blk[s] >= 0) bptr[pool_blk[s]] = -1;
+      pool_blk[s] = -1;
+    }
+  }
+}
+
+// zero the slots handed out so far in one pool (the P2G target)
+template <class R4>
+__global__ void k_pool_clear(const int32_t* __restrict__ n_alloc, int cap, R4* __restrict__ pool) {
+  const int used = min(*n_alloc, cap);
+  R4 z;
+  z.x = z.y = z.z = z.w = 0;
+  for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < (int64_t)used * 64;
+       i += (int64_t)gridDim.x * blockDim.x)
+    pool[i] = z;
+}
+
+// pool slots for the 3^D grid blocks around every occupied block
+template <int D>
+__global__ void k_activate(const int32_t* __restrict__ occ_blk, const int32_t* __restrict__ n_occ_p, int nb0, int nb1,
+                           int nb2, int32_t* __restrict__ bptr, int32_t* __restrict__ n_alloc,
+                           int32_t* __restrict__ pool_blk, int cap, unsigned* __restrict__ status) {
+  constexpr int NN = D == 3 ? 27 : 9;
+  const int64_t t = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (t >= (int64_t)*n_occ_p * NN) return;
+  const int o = (int)(t / NN), e = (int)(t - (int64_t)o * NN);
+  const int blk = occ_blk[o];
+  int b0, b1, b2 = 0;
+  if (D == 3) {
+    b2 = blk % nb2;
+    b1 = (blk / nb2) % nb1;
+    b0 = blk / nb2 / nb1;
+  } else {
+    b1 = blk % nb1;
+    b0 = blk / nb1;
+  }
+  const int c0 = b0 + (D == 3 ? e / 9 : e / 3) - 1, c1 = b1 + (D == 3 ? (e / 3) % 3 : e % 3) - 1,
+            c2 = D == 3 ? b2 + e % 3 - 1 : 0;
+  if (c0 < 0 || c0 >= nb0 || c1 < 0 || c1 >= nb1 || (D == 3 && (c2 < 0 || c2 >= nb2))) return;
+  const int64_t nbk = D == 3 ? ((int64_t)c0 * nb1 + c1) * nb2 + c2 : (int64_t)c0 * nb1 + c1;
+  if (claim_slot(bptr, n_alloc, pool_blk, cap, nbk) < 0) atomicOr(status, AQ_ST_POOL_FULL);
+}
+
+// node masses of a sparse grid as a dense float array (zero where no block)
+template <int D, class R4>
+__global__ void k_grid_mass_sparse(const R4* __restrict__ pool, const int32_t* __restrict__ bptr, int r0, int r1,
+                                   int r2, int nb1, int nb2, float* __restrict__ out, int64_t n) {
+  const int nb[3] = {0, nb1, nb2};
+  for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x) {
+    int i0, i1, i2 = 0;
+    if (D == 3) {
+      i2 = (int)(i % r2);
+      i1 = (int)((i / r2) % r1);
+      i0 = (int)(i / r2 / r1);
+    } else {
+      i1 = (int)(i % r1);
+      i0 = (int)(i / r1);
+    }
+    const int sl = bptr[block_of<D>(nb, i0, i1, i2)];
+    out[i] = sl >= 0 ? (float)pool[node_in_slot<D>(sl, i0, i1, i2)].x : 0.f;
+  }
 }
 
 // Exclusive scan of n int32 counts into out[0..n] (out[n] = total), in
@@ -385,6 +544,21 @@ struct aq_sim {
   const float* col_nrm = nullptr;
   double col_theta = 0, col_height = 0, col_omega = 0, col_rate = 0;
   int col_node_cv = 0;  // collider velocity from the node (sdf_collision_no_arg) instead of the rotated index
+  // sparse grid (P.sparse): block table, node pools (grid[] points at them)
+  // and the buffers of the sparse binning; all but the pools and the
+  // occupancy-sized arrays live in the slab
+  int32_t* bptr = nullptr;      // grid block -> pool slot, -1: none
+  int32_t* n_alloc = nullptr;   // [0] slots handed out, [1] occupied blocks of the last binning
+  int32_t* pool_blk = nullptr;  // pool slot -> grid block (-1: free)
+  int pool_cap = 0;             // node blocks per pool
+  int64_t occ_cap = 0;          // occupied blocks ccount / cstart are sized for
+  int32_t *ccount = nullptr, *cstart = nullptr;
+  uint32_t *sblk = nullptr, *sblk_sorted = nullptr;
+  int32_t *order_in = nullptr, *order = nullptr, *cslot = nullptr;
+  int32_t *occ_blk = nullptr, *occ_len = nullptr, *occ_first = nullptr;
+  void* cub_tmp = nullptr;
+  size_t cub_bytes = 0;
+  int blk_bits = 1;  // bits of a grid block index (radix sort)
   void* slab = nullptr;      // the one device allocation all buffers above live in
   int ranges_on = 0;
   int64_t step = 0;
@@ -471,6 +645,7 @@ struct SimImpl final : SimBase {
   }
 
   int sort(cudaStream_t st) override {
+    if (s->P.sparse) return sort_sparse(st);
     aq_sim* S_ = s;
     const int64_t n = S_->n;
     AQ_CUDA_TRY(cudaMemsetAsync(S_->cell_count, 0, sizeof(int32_t) * S_->nkeys, st));
@@ -485,10 +660,109 @@ struct SimImpl final : SimBase {
     k_scatter<<<grid_for(n, SCATTER_T), SCATTER_T, sizeof(uint64_t) * SCATTER_T * S_->W, st>>>(S_->words[S_->cur], S_->pid[S_->cur], S_->words[nxt], S_->pid[nxt],
                                                 S_->keys, S_->ranks, S_->cell_start, n, S_->W);
     k_items_count<<<grid_for(S_->nblk, 256), 256, 0, st>>>(S_->cell_start, S_->nblk, S_->n_items);
-    k_items<<<grid_for(S_->nblk, 256), 256, 0, st>>>(S_->cell_start, S_->nblk, S_->items, S_->n_items);
+    k_items<<<grid_for(S_->nblk, 256), 256, 0, st>>>(S_->cell_start, S_->nblk, S_->items, S_->n_items, nullptr);
     AQ_CUDA_TRY(cudaGetLastError());
     S_->cur = nxt;
     S_->launches += 7;
+    S_->since_sort = 0;
+    S_->sorted = true;
+    return AQ_OK;
+  }
+
+  // Grow a device buffer (contents dropped) to at least `need` elements.
+  template <class T>
+  static int grow(T*& p, int64_t& cap_elems, int64_t need) {
+    if (need <= cap_elems && p) return AQ_OK;
+    if (p) cudaFree(p);
+    p = nullptr;
+    cap_elems = 0;
+    const cudaError_t e = cudaMalloc((void**)&p, sizeof(T) * (size_t)need);
+    if (e != cudaSuccess) {
+      set_last_cuda_error(e, "cudaMalloc (sparse grid)");
+      return AQ_E_NOMEM;
+    }
+    cap_elems = need;
+    return AQ_OK;
+  }
+
+  // Binning of a sparse grid: see the kernels' comment.  Reads the number of
+  // occupied blocks back to the host (one synchronization per re-binning) to
+  // size the per-block arrays and the pools.
+  int sort_sparse(cudaStream_t st) {
+    aq_sim* S_ = s;
+    const int64_t n = S_->n;
+    k_sbin<D, R><<<grid_for(n, 256), 256, 0, st>>>(S_->L, K, S_->words[S_->cur], n, S_->sblk, S_->cslot,
+                                                   S_->order_in, S_->status);
+    size_t tb = S_->cub_bytes;
+    AQ_CUDA_TRY(cub::DeviceRadixSort::SortPairs(S_->cub_tmp, tb, S_->sblk, S_->sblk_sorted, S_->order_in, S_->order,
+                                                (int)n, 0, S_->blk_bits, st));
+    tb = S_->cub_bytes;
+    AQ_CUDA_TRY(cub::DeviceRunLengthEncode::Encode(S_->cub_tmp, tb, S_->sblk_sorted,
+                                                   reinterpret_cast<uint32_t*>(S_->occ_blk), S_->occ_len,
+                                                   S_->n_alloc + 1, (int)n, st));
+    int32_t n_occ = 0;
+    AQ_CUDA_TRY(cudaMemcpyAsync(&n_occ, S_->n_alloc + 1, sizeof(int32_t), cudaMemcpyDeviceToHost, st));
+    AQ_CUDA_TRY(cudaStreamSynchronize(st));
+    if (n_occ < 1 || (int64_t)n_occ * 64 + 1 > 0x7fffffffLL) return AQ_E_LIMIT;  // compact keys are int32
+    tb = S_->cub_bytes;
+    AQ_CUDA_TRY(cub::DeviceScan::ExclusiveSum(S_->cub_tmp, tb, S_->occ_len, S_->occ_first, n_occ, st));
+    int rc;
+    int64_t cc = S_->occ_cap, cs = S_->occ_cap;
+    if (n_occ > S_->occ_cap) {
+      const int64_t want = (int64_t)n_occ + n_occ / 4 + 64;
+      cc = cs = 0;
+      if ((rc = grow(S_->ccount, cc, want * 64))) return rc;
+      if ((rc = grow(S_->cstart, cs, want * 64 + 1))) return rc;
+      S_->occ_cap = want;
+    }
+    AQ_CUDA_TRY(cudaMemsetAsync(S_->ccount, 0, sizeof(int32_t) * 64 * (size_t)n_occ, st));
+    k_occ_keys<<<grid_for(n, 256), 256, 0, st>>>(S_->order, S_->cslot, S_->occ_first, S_->n_alloc + 1, n, S_->keys,
+                                                S_->ranks, S_->ccount);
+    k_cstart<<<grid_for(((int64_t)n_occ + 1) * 32, 256), 256, 0, st>>>(S_->ccount, S_->occ_first, S_->n_alloc + 1, n,
+                                                                       S_->cstart);
+    const int nxt = 1 - S_->cur;
+    k_scatter<<<grid_for(n, SCATTER_T), SCATTER_T, sizeof(uint64_t) * SCATTER_T * S_->W, st>>>(
+        S_->words[S_->cur], S_->pid[S_->cur], S_->words[nxt], S_->pid[nxt], S_->keys, S_->ranks, S_->cstart, n, S_->W);
+    AQ_CUDA_TRY(cudaMemsetAsync(S_->n_items, 0, sizeof(int32_t) * (1 + 2 * IB), st));
+    k_items_count<<<grid_for(n_occ, 256), 256, 0, st>>>(S_->cstart, n_occ, S_->n_items);
+    k_items<<<grid_for(n_occ, 256), 256, 0, st>>>(S_->cstart, n_occ, S_->items, S_->n_items, S_->occ_blk);
+    // the active blocks: empty the pools, then the 3^D blocks around every
+    // occupied block; pools grow (dropping their contents, which the next
+    // launch rebuilds from the records) when the new set may not fit
+    typedef typename R4T<R>::type R4;
+    const int nn = D == 3 ? 27 : 9;
+    k_pool_reset<R4><<<num_sms() * 4, 256, 0, st>>>(S_->bptr, S_->pool_blk, S_->n_alloc, S_->pool_cap,
+                                                    (R4*)S_->grid[0], (R4*)S_->grid[1]);
+    AQ_CUDA_TRY(cudaMemsetAsync(S_->n_alloc, 0, sizeof(int32_t), st));
+    const int64_t need = std::min<int64_t>((int64_t)nn * n_occ, S_->nblk);
+    if (need > S_->pool_cap) {
+      AQ_CUDA_TRY(cudaStreamSynchronize(st));
+      const int64_t want = std::min<int64_t>(need + need / 4 + 256, std::min<int64_t>(S_->nblk, 0x7fffffff));
+      for (int k = 0; k < 2; ++k) {
+        if (S_->grid[k]) cudaFree(S_->grid[k]);
+        S_->grid[k] = nullptr;
+      }
+      if (S_->pool_blk) cudaFree(S_->pool_blk);
+      S_->pool_blk = nullptr;
+      S_->pool_cap = 0;
+      for (int k = 0; k < 2; ++k) {
+        const cudaError_t e = cudaMalloc(&S_->grid[k], sizeof(R4) * 64 * (size_t)want);
+        if (e != cudaSuccess) {
+          set_last_cuda_error(e, "cudaMalloc (sparse grid pool)");
+          return AQ_E_NOMEM;
+        }
+        AQ_CUDA_TRY(cudaMemsetAsync(S_->grid[k], 0, sizeof(R4) * 64 * (size_t)want, st));
+      }
+      AQ_CUDA_TRY(cudaMalloc((void**)&S_->pool_blk, sizeof(int32_t) * (size_t)want));
+      AQ_CUDA_TRY(cudaMemsetAsync(S_->pool_blk, 0xff, sizeof(int32_t) * (size_t)want, st));
+      S_->pool_cap = (int)want;
+    }
+    k_activate<D><<<grid_for((int64_t)n_occ * nn, 256), 256, 0, st>>>(S_->occ_blk, S_->n_alloc + 1, K.nb[0], K.nb[1],
+                                                                       K.nb[2], S_->bptr, S_->n_alloc, S_->pool_blk,
+                                                                       S_->pool_cap, S_->status);
+    AQ_CUDA_TRY(cudaGetLastError());
+    S_->cur = nxt;
+    S_->launches += 10;
     S_->since_sort = 0;
     S_->sorted = true;
     return AQ_OK;
@@ -520,6 +794,10 @@ struct SimImpl final : SimBase {
     a.do_p2g = do_p2g;
     a.ranges = S_->ranges_on;
     a.raw_in = do_g2p;  // grid_in holds the previous P2G sums; grid_op runs as the tile is staged
+    a.bptr = S_->bptr;
+    a.n_alloc = S_->n_alloc;
+    a.pool_blk = S_->pool_blk;
+    a.pool_cap = S_->pool_cap;
     K.col_c = (R)cos(S_->col_theta);
     K.col_s = (R)sin(S_->col_theta);
     K.col_yshift = (int)(S_->col_height / S_->P.dx + 0.5);
@@ -531,6 +809,9 @@ struct SimImpl final : SimBase {
         set_last_cuda_error(cudaErrorLaunchFailure, "cuLaunchKernel(k_step)");
         return AQ_E_CUDA;
       }
+    } else if (S_->P.sparse) {
+      k_step<D, HF, HM, R, RtLayout, true, true><<<S_->step_grid, CH, S_->step_smem, st>>>(S_->L, K, a);
+      AQ_CUDA_TRY(cudaGetLastError());
     } else {
       k_step<D, HF, HM, R, RtLayout><<<S_->step_grid, CH, S_->step_smem, st>>>(S_->L, K, a);
       AQ_CUDA_TRY(cudaGetLastError());
@@ -544,7 +825,13 @@ struct SimImpl final : SimBase {
   int clear_grid(void* g, cudaStream_t st) {
     const bool prof = s->prof_on && s->prof_n[1] < aq_sim::PROF_CAP;
     if (prof) AQ_CUDA_TRY(cudaEventRecord(s->prof_ev[1][2 * s->prof_n[1]], st));
-    AQ_CUDA_TRY(cudaMemsetAsync(g, 0, sizeof(typename R4T<R>::type) * s->ncell, st));
+    if (s->P.sparse) {
+      k_pool_clear<typename R4T<R>::type><<<num_sms() * 4, 256, 0, st>>>(s->n_alloc, s->pool_cap,
+                                                                        (typename R4T<R>::type*)g);
+      AQ_CUDA_TRY(cudaGetLastError());
+    } else {
+      AQ_CUDA_TRY(cudaMemsetAsync(g, 0, sizeof(typename R4T<R>::type) * s->ncell, st));
+    }
     if (prof) AQ_CUDA_TRY(cudaEventRecord(s->prof_ev[1][2 * s->prof_n[1]++ + 1], st));
     return AQ_OK;
   }
@@ -602,7 +889,7 @@ static int setup_step_kernel(aq_sim* s, size_t smem_jit, size_t smem_aot, bool c
   s->jit_fn = nullptr;
   if (s->P.jit) {
     const size_t smem = smem_jit;
-    s->jit_fn = jit_k_step(D, HF, HM, sizeof(R) == 8, col, s->L, &s->jit_error);
+    s->jit_fn = jit_k_step(D, HF, HM, sizeof(R) == 8, col, s->P.sparse != 0, s->L, &s->jit_error);
     if (s->jit_fn && (jit_set_smem(s->jit_fn, (int)smem) != AQ_OK || jit_occupancy(s->jit_fn, CH, smem, &occ) != AQ_OK)) {
       s->jit_fn = nullptr;
       s->jit_error = "cuFuncSetAttribute/occupancy failed";
@@ -612,9 +899,16 @@ static int setup_step_kernel(aq_sim* s, size_t smem_jit, size_t smem_aot, bool c
   if (!s->jit_fn) {
     const size_t smem = smem_aot;
     s->step_smem = smem;
-    AQ_CUDA_TRY(cudaFuncSetAttribute(k_step<D, HF, HM, R, RtLayout>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                     (int)smem));
-    AQ_CUDA_TRY(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, k_step<D, HF, HM, R, RtLayout>, CH, smem));
+    if (s->P.sparse) {
+      AQ_CUDA_TRY(cudaFuncSetAttribute(k_step<D, HF, HM, R, RtLayout, true, true>,
+                                       cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+      AQ_CUDA_TRY(
+          cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, k_step<D, HF, HM, R, RtLayout, true, true>, CH, smem));
+    } else {
+      AQ_CUDA_TRY(cudaFuncSetAttribute(k_step<D, HF, HM, R, RtLayout>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                       (int)smem));
+      AQ_CUDA_TRY(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, k_step<D, HF, HM, R, RtLayout>, CH, smem));
+    }
   }
   if (occ < 1) occ = 1;
   s->step_grid = occ * num_sms();
@@ -648,6 +942,14 @@ static void free_sim(aq_sim* s) {
       for (int j = 0; j < 2 * aq_sim::PROF_CAP; ++j) cudaEventDestroy(s->prof_ev[k][j]);
       delete[] s->prof_ev[k];
     }
+  }
+  if (s->P.sparse) {
+    for (int k = 0; k < 2; ++k)
+      if (s->grid[k]) cudaFree(s->grid[k]);
+    if (s->pool_blk) cudaFree(s->pool_blk);
+    if (s->ccount) cudaFree(s->ccount);
+    if (s->cstart) cudaFree(s->cstart);
+    if (s->cub_tmp) cudaFree(s->cub_tmp);
   }
   if (s->slab) cudaFree(s->slab);
   delete s;
@@ -694,9 +996,18 @@ int aq_sim_create(const aq_params* P, const aq_layout* L, aq_sim** out) {
     nb[d] = (P->res[d] + BS - 1) / BS;
     s->ncell *= P->res[d];
   }
-  s->nblk = nb[0] * nb[1] * nb[2];
-  s->nkeys = (int64_t)s->nblk * 64;
-  s->max_items = s->nblk + 1;
+  const int64_t nblk64 = (int64_t)nb[0] * nb[1] * nb[2];
+  if (P->sparse && nblk64 > 0x7fffffffLL) {
+    delete s;
+    return AQ_E_LIMIT;  // block indices of a sparse grid are int32
+  }
+  if (!P->sparse && nblk64 * 64 > 0x7fffffffLL) {
+    delete s;
+    return AQ_E_LIMIT;  // the dense binning's cell keys are int32
+  }
+  s->nblk = (int)nblk64;
+  s->nkeys = P->sparse ? 0 : (int64_t)s->nblk * 64;
+  s->max_items = P->sparse ? std::min<int64_t>(s->nblk, P->n_particles) + 1 : (int64_t)s->nblk + 1;
   const size_t rsz = P->precision ? sizeof(double) : sizeof(float);
   const int64_t n = s->n;
   const int nt = (int)((s->nkeys + SCAN_TILE - 1) / SCAN_TILE);
@@ -718,13 +1029,26 @@ int aq_sim_create(const aq_params* P, const aq_layout* L, aq_sim** out) {
   alloc((void**)&s->words[1], sizeof(uint64_t) * (n * s->W + 2));
   alloc((void**)&s->pid[0], sizeof(int32_t) * n);
   alloc((void**)&s->pid[1], sizeof(int32_t) * n);
-  alloc(&s->grid[0], rsz * 4 * s->ncell);
-  alloc(&s->grid[1], rsz * 4 * s->ncell);
   alloc((void**)&s->keys, sizeof(int32_t) * n);
   alloc((void**)&s->ranks, sizeof(int32_t) * n);
-  alloc((void**)&s->cell_count, sizeof(int32_t) * s->nkeys);
-  alloc((void**)&s->cell_start, sizeof(int32_t) * (s->nkeys + 1));
-  alloc((void**)&s->scan_sums, sizeof(int32_t) * (nt + 1));
+  if (P->sparse) {  // block table and sparse binning; the pools are sized at the first binning
+    alloc((void**)&s->bptr, sizeof(int32_t) * (size_t)s->nblk);
+    alloc((void**)&s->n_alloc, 2 * sizeof(int32_t));
+    alloc((void**)&s->sblk, sizeof(uint32_t) * n);
+    alloc((void**)&s->sblk_sorted, sizeof(uint32_t) * n);
+    alloc((void**)&s->order_in, sizeof(int32_t) * n);
+    alloc((void**)&s->order, sizeof(int32_t) * n);
+    alloc((void**)&s->cslot, sizeof(int32_t) * n);
+    alloc((void**)&s->occ_blk, sizeof(int32_t) * n);
+    alloc((void**)&s->occ_len, sizeof(int32_t) * n);
+    alloc((void**)&s->occ_first, sizeof(int32_t) * n);
+  } else {
+    alloc(&s->grid[0], rsz * 4 * s->ncell);
+    alloc(&s->grid[1], rsz * 4 * s->ncell);
+    alloc((void**)&s->cell_count, sizeof(int32_t) * s->nkeys);
+    alloc((void**)&s->cell_start, sizeof(int32_t) * (s->nkeys + 1));
+    alloc((void**)&s->scan_sums, sizeof(int32_t) * (nt + 1));
+  }
   alloc((void**)&s->items, sizeof(int4) * s->max_items);
   alloc((void**)&s->n_items, sizeof(int32_t) * (1 + 2 * IB));
   alloc((void**)&s->item_ctr, 2 * sizeof(int32_t));
@@ -743,8 +1067,25 @@ int aq_sim_create(const aq_params* P, const aq_layout* L, aq_sim** out) {
     free_sim(s);
     return AQ_E_NOMEM;
   }
-  e = cudaMemset(s->grid[0], 0, rsz * 4 * s->ncell);
-  if (e == cudaSuccess) e = cudaMemset(s->grid[1], 0, rsz * 4 * s->ncell);
+  if (P->sparse) {
+    e = cudaMemset(s->bptr, 0xff, sizeof(int32_t) * (size_t)s->nblk);
+    if (e == cudaSuccess) e = cudaMemset(s->n_alloc, 0, 2 * sizeof(int32_t));
+    // scratch of the radix sort, run-length encoding and scan over n records
+    size_t b1 = 0, b2 = 0, b3 = 0;
+    while (s->blk_bits < 31 && (int64_t(1) << s->blk_bits) < s->nblk) ++s->blk_bits;
+    if (e == cudaSuccess)
+      e = cub::DeviceRadixSort::SortPairs(nullptr, b1, s->sblk, s->sblk_sorted, s->order_in, s->order, (int)n, 0,
+                                          s->blk_bits);
+    if (e == cudaSuccess)
+      e = cub::DeviceRunLengthEncode::Encode(nullptr, b2, s->sblk_sorted, reinterpret_cast<uint32_t*>(s->occ_blk),
+                                             s->occ_len, s->n_alloc + 1, (int)n);
+    if (e == cudaSuccess) e = cub::DeviceScan::ExclusiveSum(nullptr, b3, s->occ_len, s->occ_first, (int)n);
+    s->cub_bytes = std::max(std::max(b1, b2), std::max(b3, (size_t)256));
+    if (e == cudaSuccess) e = cudaMalloc(&s->cub_tmp, s->cub_bytes);
+  } else {
+    e = cudaMemset(s->grid[0], 0, rsz * 4 * s->ncell);
+    if (e == cudaSuccess) e = cudaMemset(s->grid[1], 0, rsz * 4 * s->ncell);
+  }
   if (e == cudaSuccess) e = cudaMemset(s->words[0], 0, sizeof(uint64_t) * (n * s->W + 2));
   if (e == cudaSuccess) e = cudaMemset(s->status, 0, sizeof(unsigned));
   if (e == cudaSuccess) e = cudaMemset(s->fallbacks, 0, sizeof(unsigned long long));
@@ -850,6 +1191,18 @@ int aq_sim_collider_velocity_mode(aq_sim* s, int32_t from_node) {
   return AQ_OK;
 }
 
+int aq_sim_sparse_blocks(aq_sim* s, int64_t* h_slots, int64_t* h_occupied, void* stream) {
+  if (!s || !h_slots || !h_occupied) return AQ_E_ARG;
+  if (!s->P.sparse) return AQ_E_STATE;
+  cudaStream_t st = as_stream(stream);
+  int32_t v[2] = {0, 0};
+  AQ_CUDA_TRY(cudaMemcpyAsync(v, s->n_alloc, sizeof(v), cudaMemcpyDeviceToHost, st));
+  AQ_CUDA_TRY(cudaStreamSynchronize(st));
+  *h_slots = std::min<int64_t>(v[0], s->pool_cap);
+  *h_occupied = v[1];
+  return AQ_OK;
+}
+
 int aq_sim_collider_get(aq_sim* s, double* h_theta, double* h_height) {
   if (!s || !h_theta || !h_height) return AQ_E_ARG;
   *h_theta = s->col_theta;
@@ -905,6 +1258,24 @@ int aq_sim_grid_mass(aq_sim* s, float* d_out, void* stream) {
   if (!s || !d_out) return AQ_E_ARG;
   cudaStream_t st = as_stream(stream);
   const unsigned nb = (unsigned)std::min<int64_t>(grid_for(s->ncell, 256), (int64_t)num_sms() * 8);
+  if (s->P.sparse) {
+    const int r0 = s->P.res[0], r1 = s->P.res[1], r2 = s->D == 3 ? s->P.res[2] : 1;
+    const int bs = s->D == 3 ? 4 : 8;
+    const int nb1 = (r1 + bs - 1) / bs, nb2 = s->D == 3 ? (r2 + bs - 1) / bs : 1;
+    const void* g = s->grid[s->last_grid];
+    if (!g) return AQ_E_STATE;  // no substep has run yet
+    if (s->D == 3 && s->P.precision)
+      k_grid_mass_sparse<3><<<nb, 256, 0, st>>>((const double4*)g, s->bptr, r0, r1, r2, nb1, nb2, d_out, s->ncell);
+    else if (s->D == 3)
+      k_grid_mass_sparse<3><<<nb, 256, 0, st>>>((const float4*)g, s->bptr, r0, r1, r2, nb1, nb2, d_out, s->ncell);
+    else if (s->P.precision)
+      k_grid_mass_sparse<2><<<nb, 256, 0, st>>>((const double4*)g, s->bptr, r0, r1, r2, nb1, nb2, d_out, s->ncell);
+    else
+      k_grid_mass_sparse<2><<<nb, 256, 0, st>>>((const float4*)g, s->bptr, r0, r1, r2, nb1, nb2, d_out, s->ncell);
+    AQ_CUDA_TRY(cudaGetLastError());
+    s->launches += 1;
+    return AQ_OK;
+  }
   if (s->P.precision)
     k_grid_mass<<<nb, 256, 0, st>>>((const double4*)s->grid[s->last_grid], d_out, s->ncell);
   else

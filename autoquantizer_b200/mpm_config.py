@@ -73,3 +73,7 @@ class MPMConfig(object):
         # compile the substep kernel for the record layout with NVRTC
         # (False: the generic kernel built into libaq.so)
         self.jit = True
+        # sparse grid: store only the grid blocks around particles (the
+        # reference's pointer grid over a 4096^dim index space,
+        # mpm_solver.py:216-253), for domains whose dense grid is too large
+        self.sparse_grid = False

@@ -178,6 +178,7 @@ class MPMSolver:
         P.use_bound_clip = int(self.use_bound_clip)
         P.sort_interval = int(p.sort_interval)
         P.jit = int(getattr(p, "jit", True))
+        P.sparse = int(bool(getattr(p, "sparse_grid", False)))
         P.dx, P.dt, P.p_vol, P.p_mass, P.gravity = self.dx, self.dt, self.p_vol, self.p_mass, self.g
         P.n_particles = self.current_idx
         P.seed = int(p.seed)
@@ -685,6 +686,15 @@ class MPMSolver:
                    "aq_sim_status")
         return f.value, fb.value
 
+    def sparse_blocks(self):
+        """Sparse grid: (pool slots handed out, grid blocks holding particles
+        at the last re-binning)."""
+        self._ensure_sim()
+        a, b = C.c_int64(), C.c_int64()
+        _lib.check(_lib.lib().aq_sim_sparse_blocks(self._sim, C.byref(a), C.byref(b), _lib.stream_ptr()),
+                   "aq_sim_sparse_blocks")
+        return a.value, b.value
+
     def kernel_is_jit(self):
         self._ensure_sim()
         v = C.c_int32()
@@ -794,7 +804,12 @@ class MPMSolver:
         """The autodiff pass (mpm_solver.py:1093-1302, drivers' ad()): forward
         n_timestep-1 substeps on unquantized state with checkpoints, loss
         compute_ek, then the hand-written reverse pass; the per-scalar
-        sensitivities are kept for get_gradients().  Returns the loss."""
+        sensitivities are kept for get_gradients().  Returns the loss.
+        every > 0: a checkpoint every `every` substeps, each segment
+        recomputed once in the reverse pass (memory T/every + every states,
+        T extra substeps); every = 0: the reference's logarithmic stash
+        (memory log2 T states, about T log2(T) / 2 extra substeps), for
+        horizons whose segment states would not fit."""
         import torch
 
         from .adjoint import Adjoint, ek_loss, ek_seed

@@ -11,10 +11,14 @@ default_rng), no dataset.  Particle records (117 MB) and grids (67 MB) exceed
 the 126 MB L2, so no flush is needed between steps.
 
 Reported: particle-substeps/s of the quantized state (`value`), the same
-scene with FP32 particle state, position error of both against an FP64 GPU
-run, the fused kernel's roofline (CUDA-event time per launch vs. the
-measured HBM copy bandwidth), an end-to-end number through the public API
-with host buffers, and the oracle CPU port as baseline.
+scene with FP32 particle state, the errors of both against an FP64 GPU run
+(per field group x, v, C, F, accumulated in FP64 on the device, checked
+against a stated bound: position RMS and the reference drivers' loss test),
+the same scene on a scheme the analytical solver derives at compression
+rate 0.5, the fused kernel's roofline (CUDA-event time per launch vs. the
+measured HBM copy bandwidth), end-to-end numbers through the public API with
+host buffers (frames of 100 substeps and of 1 substep), and the oracle CPU
+port as baseline.
 
 --impl reference times the CPU restatement of the reference's substep
 (oracle/, C + OpenMP, all host cores) on a bounded sample of the same scene:
@@ -60,18 +64,37 @@ def measured_peaks():
     return 6650.0, "fallback"
 
 
-def ncu_traffic():
-    """DRAM bytes per launch of the fused kernel from the committed ncu summary."""
-    p = os.path.join(ROOT, "profiles", "k_step_mixed_boxes_3d.md")
-    if not os.path.exists(p):
-        return None
-    for line in open(p):
-        if line.startswith("dram_bytes_per_launch_full_size:"):
-            try:
-                return float(line.split(":", 1)[1].strip().split()[0])
-            except ValueError:
-                return None
-    return None
+# DRAM bytes (dram__bytes_read.sum + dram__bytes_write.sum) of one k_step
+# launch of this workload, from an ncu capture made apart from the bench (a
+# number printed under a profiler is never a bench value):
+#   ncu --set full --clock-control none -k regex:k_step -s 20 -c 1 \
+#       python -m autoquantizer_b200.run_scene --scene mixed_boxes_3d --substeps 40
+# It is re-captured whenever k_step changes.
+NCU_TRAFFIC_BYTES = 218585856.0
+NCU_TRAFFIC_SOURCE = ("ncu dram__bytes_read.sum + dram__bytes_write.sum, one k_step launch of this workload "
+                      "(run_scene --scene mixed_boxes_3d, launch 21), captured separately")
+
+# field groups of the 3D record: slots [lo, hi)
+GROUPS_3D = (("x", 0, 3), ("v", 3, 6), ("C", 6, 15), ("F", 15, 24))
+
+
+def field_errors(a, b):
+    """Per field group, RMS and max of |a - b| over particles and components
+    (a, b: CUDA float64 n x n_slots states in particle order), the squares
+    and maxima accumulated in FP64 on the device (aq_state_error)."""
+    import ctypes as C
+
+    from autoquantizer_b200 import _lib
+
+    n, ns = a.shape
+    sq = (C.c_double * ns)()
+    mx = (C.c_double * ns)()
+    _lib.check(_lib.lib().aq_state_error(C.c_void_p(a.data_ptr()), 1, C.c_void_p(b.data_ptr()), 1, n, ns, sq, mx,
+                                         _lib.stream_ptr()), "aq_state_error")
+    out = {}
+    for name, lo, hi in GROUPS_3D:
+        out[name] = {"rms": (sum(sq[lo:hi]) / (n * (hi - lo))) ** 0.5, "max": max(mx[lo:hi])}
+    return out
 
 
 class Clocks:
@@ -322,30 +345,41 @@ def run_ours(args, ws, rank, local):
     ms32, _ = timed(f, K)
     value32, ms32 = job_rate(n * K, ms32, ws)
 
-    # ---- FP64 oracle run on the GPU and position errors after W+K substeps
+    # ---- FP64 oracle run on the GPU; per-field errors of both runs after
+    # the same W+K(+extra) substeps, accumulated in FP64 on the device
+    total = W + K + extra
     cfg64, _ = scenes.mixed_boxes_3d(seed=rank, quantized=False, precision="f64")
     d = MPMSolver(cfg64)
     d.set_particles(vals)
-    d.substeps(W + K + extra)
+    d.substeps(total)
     f.substeps(extra)
-    x64 = d.state_tensor(True)[:, :3]
+    ref = d.state_tensor(True)
+    loss64 = d.compute_loss()
     errs = {}
     for name, sol in (("quantized", q), ("fp32_state", f)):
-        dx_ = sol.state_tensor(True)[:, :3] - x64
-        errs[name] = {"x_rms": float(dx_.pow(2).sum(1).mean().sqrt()), "x_max": float(dx_.abs().max())}
-    del d, f
+        fe = field_errors(sol.state_tensor(True), ref)
+        loss = sol.compute_loss()
+        rel = abs(loss - loss64) / abs(loss64)
+        errs[name] = {"fields": fe, "x_rms": fe["x"]["rms"], "x_max": fe["x"]["max"], "loss": loss,
+                      "loss_rel_err": rel,
+                      "within_bound": bool(fe["x"]["rms"] <= args.x_bound and rel <= 3 * args.loss_eps)}
+    del f
+
+    # ---- a scheme derived by the analytical solver at compression rate 0.5
+    cr = None
+    if not args.no_cr:
+        cr = cr_half_run(args, rank, vals, ref, loss64, total, K, W, ws)
+    del d, ref
 
     # ---- end to end through the public API with host buffers: per step the
-    # packed records come from pinned host memory, one frame of substeps
-    # runs, the records and the loss go back to the host.
-    frame = args.frame
+    # packed records come from pinned host memory, a frame of substeps runs,
+    # the records and the loss go back to the host.
     words = q.words()
     h_in = torch.from_numpy(words.view(np.int64)).pin_memory()
     h_out = torch.empty_like(h_in).pin_memory()
     d_words = torch.empty_like(h_in, device="cuda")
-    e2e_steps = max(1, args.e2e_steps)
 
-    def e2e_step():
+    def e2e_step(frame):
         d_words.copy_(h_in, non_blocking=True)
         _lib.check(L.aq_sim_set_words(q._sim, C.c_void_p(d_words.data_ptr()), _lib.stream_ptr()))
         q.substeps(frame)
@@ -353,16 +387,23 @@ def run_ours(args, ws, rank, local):
         h_out.copy_(d_words, non_blocking=True)
         return q.compute_loss()  # device->host read of the step's result
 
-    e2e_step()
-    barrier(ws)
-    torch.cuda.synchronize()
-    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-    e0.record()
-    for _ in range(e2e_steps):
-        e2e_step()
-    e1.record()
-    torch.cuda.synchronize()
-    e2e_val, e2e_ms = job_rate(n * frame * e2e_steps, e0.elapsed_time(e1), ws)
+    def e2e(frame, steps):
+        e2e_step(frame)
+        barrier(ws)
+        torch.cuda.synchronize()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record()
+        for _ in range(steps):
+            e2e_step(frame)
+        e1.record()
+        torch.cuda.synchronize()
+        v, ms_ = job_rate(n * frame * steps, e0.elapsed_time(e1), ws)
+        return {"value": v, "unit": UNIT, "h2d_bytes_per_step": int(h_in.numel() * 8),
+                "d2h_bytes_per_step": int(h_out.numel() * 8 + 8), "substeps_per_step": frame, "steps": steps,
+                "ms_per_step": ms_ / steps}
+
+    e2e_main = e2e(args.frame, max(1, args.e2e_steps))
+    e2e_one = e2e(1, max(3, args.e2e_steps * 4))
 
     # ---- CPU baseline (rank 0, N=1 only)
     cpu = None
@@ -381,23 +422,127 @@ def run_ours(args, ws, rank, local):
                        "l2": "inputs larger than L2 (117 MB records + 67 MB grids), no flush",
                        "parallelism": "replicas" if ws > 1 else "single"},
             "fp32_state": {"value": value32, "unit": UNIT, "ms_per_step": ms32 / K,
-                           "quantized_speedup": value / value32},
+                           "quantized_speedup": value / value32, "record_bytes": S32,
+                           "record": "24 f32 values + 2-bit material id, padded to 13 words"},
             "compression": 96.0 / S,
-            "error_vs_fp64": {"substeps": W + K + extra, **errs},
+            "compression_detail": {"vs_fp32_values_96B": 96.0 / S, "vs_fp32_record_run_%dB" % S32: S32 / S,
+                                   "bit_dense_vs_fp32_values": 768.0 / q.layout().total_bits},
+            "error_vs_fp64": {"substeps": total, **errs,
+                              "bound": {"x_rms": args.x_bound, "loss_rel_err": 3 * args.loss_eps,
+                                        "stated": "requested: position RMS error <= %g (domain [0,1]^3, "
+                                                  "dx = 1/128) and |loss - loss_f64| < 3 eps |loss_f64| with "
+                                                  "eps = %g (the reference drivers' success test, "
+                                                  "run_mpm_elastic_2d.py:205-207; loss = compute_ek)"
+                                                  % (args.x_bound, args.loss_eps)},
+                              "loss_f64": loss64,
+                              "accumulation": "per slot sum of squares and max in FP64 on the device "
+                                              "(aq_state_error); RMS over particles and components of a group"},
+            "cr_half_scheme": cr,
             "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
-                         "frac": achieved / peak, "traffic": ncu_traffic(), "peak_kind": peak_kind,
-                         "kernel": "k_step (fused G2P+P2G)", "avg_launch_ms": step_ms,
+                         "frac": achieved / peak, "traffic": NCU_TRAFFIC_BYTES, "traffic_source": NCU_TRAFFIC_SOURCE,
+                         "peak_kind": peak_kind, "kernel": "k_step (fused G2P+P2G)", "avg_launch_ms": step_ms,
                          "alg_bytes_per_launch": alg_bytes, "grid_clear_avg_ms": grid_ms},
             "cpu_baseline": cpu,
-            "e2e": {"value": e2e_val, "unit": UNIT, "h2d_bytes_per_step": int(h_in.numel() * 8),
-                    "d2h_bytes_per_step": int(h_out.numel() * 8 + 8), "substeps_per_step": frame,
-                    "steps": e2e_steps},
+            "e2e": e2e_main,
+            "e2e_frame1": e2e_one,
             "gpu_launches": int(launches),
             "kernel_jit": q.kernel_is_jit(),
             "status": {"flags": flags, "tile_fallbacks": fallbacks},
             "clocks": ck,
         }
         print(json.dumps(line), flush=True)
+
+
+def cr_half_run(args, rank, vals, ref, loss64, total, K, W, ws):
+    """The same scene on a scheme the analytical solver derives at compression
+    rate 0.5 (LagrangianCR, the drivers' solve() recipe: position ranges 1,
+    other ranges doubled, one sign bit added), all fields fixed point, so
+    that the record with its 2-bit material id fits 6 words (48 B): 2x
+    compression against the 96 B of FP32 values.
+    Sensitivities: the hand-written adjoint (64 substeps, checkpoints every
+    16, loss compute_ek) on a single-material stand-in of the scene, since
+    the adjoint runs the reference's material laws only: the same particles,
+    all elastic with the reference's 3D law at the geometric-mean E and mean
+    nu of the scene's two elastic boxes.  Ranges: the FP32-state run's range
+    detection over the same substeps.  Returns its throughput, compression
+    and errors against the FP64 run."""
+    import torch
+
+    from autoquantizer_b200 import _lib, scenes
+    from autoquantizer_b200.adjoint import Adjoint, ek_seed
+    from autoquantizer_b200.mpm_solver import MPMSolver
+    from autoquantizer_b200.solvers import scheme_from_sensitivities
+
+    cfg, _ = scenes.mixed_boxes_3d(seed=rank, quantized=False)
+    el = [m for m in cfg.materials if m[0] != _lib.AQ_MAT_FLUID]
+    stand = scenes.mixed_boxes_3d(seed=rank, n=4, quantized=False)[0]
+    stand.materials = None
+    stand.use_fluid = False
+    stand.E = float(np.exp(np.mean([np.log(m[1]) for m in el])))
+    stand.nu = float(np.mean([m[2] for m in el]))
+    stand.n_particles = vals.shape[0]
+    s = MPMSolver(stand)
+    s.set_particles(vals[:, :24])
+    adj = Adjoint(s._params())
+    s0 = torch.from_numpy(np.ascontiguousarray(vals[:, :24])).to("cuda", torch.float32)
+    t0 = time.perf_counter()
+    sT = adj.forward(s0, 64, 16)
+    _, sens = adj.backward(ek_seed(sT, 3, s.p_mass, s.g))
+    torch.cuda.synchronize()
+    t_adj = time.perf_counter() - t0
+    adj.close()
+    del sT, s0
+    # ranges: FP32 state with range detection over the same substeps
+    r = MPMSolver(cfg)
+    r.set_particles(vals)
+    limits = r.run_forward_detect_ranges(total)
+    del r
+    budget = 6 * 64 - 2  # six words minus the material id
+    sens = np.maximum(np.asarray(sens, dtype=np.float64), 1e-30 * float(np.max(sens)))
+    raw, _ = scheme_from_sensitivities(sens, limits[:24], 3, mode="CR", eps=0.5)
+    chosen = None
+    for k in range(81):
+        # widths outside what a fixed-point slot holds are clamped (a slot
+        # needs its sign bit and one more; 32 bits is the codec's maximum),
+        # the rate lowered until the clamped widths fit six words
+        rate = 0.5 - 0.0025 * k
+        bits, ranges = scheme_from_sensitivities(sens, limits[:24], 3, mode="CR", eps=rate)
+        bits = np.clip(bits, 2, 32)
+        if int(np.sum(bits)) <= budget:
+            chosen = (rate, bits, ranges)
+            break
+    if chosen is None:
+        return {"error": "no rate in [0.3, 0.5] fits six words", "bits_at_0.5": [int(b) for b in raw]}
+    rate, bits, ranges = chosen
+    cq, _ = scenes.mixed_boxes_3d(seed=rank)
+    cq.quant_bits = np.asarray(bits)
+    cq.quant_ranges = np.asarray(ranges)
+    cq.v_exp_bits = 0
+    sq = MPMSolver(cq)
+    sq.set_particles(vals)
+    S = sq.bytes_per_particle()
+    sq.substeps(W)
+    barrier(ws)
+    torch.cuda.synchronize()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record()
+    sq.substeps(K)
+    e1.record()
+    torch.cuda.synchronize()
+    value, ms = job_rate(vals.shape[0] * K, e0.elapsed_time(e1), ws)
+    sq.substeps(total - W - K)
+    fe = field_errors(sq.state_tensor(True), ref)
+    loss = sq.compute_loss()
+    rel = abs(loss - loss64) / abs(loss64)
+    flags, _ = sq.status()
+    return {"value": value, "unit": UNIT, "ms_per_step": ms / K, "rate": rate, "bits": [int(b) for b in bits],
+            "solver_bits_at_0.5_unclamped": [int(b) for b in raw], "sensitivities_sum_sq": [float(x) for x in sens],
+            "record_bits": sq.layout().total_bits, "bytes_per_particle": S, "compression": 96.0 / S,
+            "fields": fe, "x_rms": fe["x"]["rms"], "loss_rel_err": rel,
+            "within_bound": bool(fe["x"]["rms"] <= args.x_bound and rel <= 3 * args.loss_eps),
+            "status_flags": flags, "adjoint_s": t_adj,
+            "sensitivities": "adjoint on a single-material stand-in (reference 3D elastic law, E %.4g, nu %.3f)"
+                             % (stand.E, stand.nu)}
 
 
 def main():
@@ -410,6 +555,9 @@ def main():
     ap.add_argument("--e2e-steps", type=int, default=3)
     ap.add_argument("--cpu-seconds", type=float, default=15.0)
     ap.add_argument("--no-cpu", action="store_true")
+    ap.add_argument("--no-cr", action="store_true", help="skip the compression-rate-0.5 scheme run")
+    ap.add_argument("--x-bound", type=float, default=1e-4, help="requested position RMS error bound")
+    ap.add_argument("--loss-eps", type=float, default=1e-3, help="eps of the |loss - loss_f64| < 3 eps test")
     args = ap.parse_args()
     args.warmup = max(3, args.warmup)
     ws, rank, local = dist_init()

@@ -51,6 +51,7 @@ extern "C" {
 #define AQ_ST_OUT_OF_DOMAIN 0x1u  /* a particle stencil left the grid; base clamped */
 #define AQ_ST_NAN 0x2u            /* a NaN position was met; base clamped */
 #define AQ_ST_FALLBACK 0x4u       /* a particle left its shared-memory tile (informational) */
+#define AQ_ST_POOL_FULL 0x8u      /* sparse grid: no free node block; contributions to it were dropped */
 
 /* scalar kinds: quantized types of the reference
  *   AQ_FIXED      ti.quant.fixed(frac=bits, signed, range, offset)
@@ -163,6 +164,10 @@ typedef struct aq_params {
   aq_material mat[AQ_MAX_MATERIALS];
   int64_t n_particles;
   uint64_t seed;
+  int32_t sparse;        /* 1: sparse grid (only node blocks near particles are
+                            stored, through a table of one int32 per grid
+                            block; index spaces up to 2^31 blocks), 0: dense */
+  int32_t reserved;
 } aq_params;
 
 #ifndef __CUDACC_RTC__
@@ -239,6 +244,13 @@ int aq_sim_field_stats(aq_sim* sim, const void* d_ref, int32_t ref_f64, double* 
 int aq_sim_set_collider(aq_sim* sim, const float* d_sdf, const float* d_normal, const int32_t* dims,
                         const int32_t* offset, int32_t center, double theta, double height, double omega,
                         double height_rate);
+/* Sparse grids (aq_params.sparse): pool slots (node blocks) handed out so
+ * far and grid blocks holding particles at the last re-binning.  A dense
+ * simulator returns AQ_E_STATE.  Synchronizes `stream`.  Replaces the
+ * reference's view of its pointer grid's active blocks (init_sparse_grids,
+ * mpm_solver.py:216-253). */
+int aq_sim_sparse_blocks(aq_sim* sim, int64_t* h_slots, int64_t* h_occupied, void* stream);
+
 /* Current collider angle and height. */
 int aq_sim_collider_get(aq_sim* sim, double* h_theta, double* h_height);
 /* Put the collider at angle theta and height `height` for the next substep
@@ -316,7 +328,15 @@ int aq_adjoint_set_collider(aq_adjoint* adj, const float* d_sdf, const float* d_
                             const int32_t* offset, int32_t center, double theta, double height, double omega,
                             double height_rate);
 /* Run n_substeps from d_s0, keeping checkpoints; d_sT receives the final
- * state. */
+ * state.  every > 0: a checkpoint every `every` substeps, each segment
+ * recomputed once by aq_adjoint_backward (memory n_substeps/every + every
+ * states).  every = 0: only the initial state is kept and the backward
+ * pass recomputes by bisection, one stashed state per level (the
+ * reference's logarithmic stash, run_forward_with_ad_nlogn / rerun_from /
+ * cnt_ending_zero, mpm_solver.py:1093-1137,1201-1207; memory ceil(log2 T) + 3
+ * states, about T log2(T) / 2 recomputed substeps).  Internally the state is
+ * kept sorted by base cell for locality; d_s0, d_sT and the gradients are in
+ * the caller's particle order. */
 int aq_adjoint_forward(aq_adjoint* adj, const void* d_s0, int32_t n_substeps, int32_t every, void* d_sT,
                        void* stream);
 /* Back-propagate d_seed = dL/d(final state) of the last forward run.

@@ -186,3 +186,44 @@ def test_fd_elastic_3d_with_collider():
     cfg2, vals2 = _scene()
     without = _fd_check(cfg2, vals2, T=8, every=3)
     assert np.max(np.abs(with_col - without) / (np.abs(without) + 1e-30)) > 1e-3
+
+
+@pytest.mark.parametrize("T", [1, 7, 16, 37])
+def test_bisection_checkpointing_matches_segments(T):
+    """every = 0 selects the logarithmic-memory scheme (the reference's
+    nlogn stash, restated as bisection): the same final state, gradient of
+    the initial state and sensitivity sums as checkpoints every 4 substeps
+    (f64; both recompute the same substeps, so they agree to rounding of the
+    grid sums' order)."""
+    import torch
+
+    cfg, vals = scenes.falling_block_3d(n=6000, n_grid=32)
+    _, adj, s0 = _setup(cfg, vals)
+    rng = np.random.default_rng(T)
+    sT_a = adj.forward(s0, T, 4)
+    seed = torch.from_numpy(rng.normal(size=sT_a.shape)).cuda()
+    g_a, sens_a = adj.backward(seed)
+    g_a = g_a.clone()
+    sens_a = np.array(sens_a)
+    sT_b = adj.forward(s0, T, 0)
+    g_b, sens_b = adj.backward(seed)
+    assert torch.allclose(sT_a, sT_b, rtol=1e-12, atol=1e-12)
+    assert torch.allclose(g_a, g_b, rtol=1e-9, atol=1e-9 * float(g_a.abs().max()))
+    np.testing.assert_allclose(sens_b, sens_a, rtol=1e-9, atol=0)
+    adj.close()
+
+
+def test_run_forward_with_ad_nlogn_bisection_matches_segments():
+    """MPMSolver.run_forward_with_ad_nlogn with every=0 (logarithmic stash)
+    and with segments of 8 substeps: same loss and sensitivities."""
+    cfg, vals = scenes.falling_block_3d(n=6000, n_grid=32)
+    cfg.precision = "f64"
+    cfg.n_timesteps = 25
+    out = []
+    for every in (8, 0):
+        s = MPMSolver(cfg)
+        s.set_particles(vals[:, : s.n_slots()])
+        loss = s.run_forward_with_ad_nlogn(every=every)
+        out.append((loss, np.asarray(s.get_gradients(), dtype=np.float64).ravel()))
+    assert out[0][0] == pytest.approx(out[1][0], rel=1e-12)
+    np.testing.assert_allclose(out[1][1], out[0][1], rtol=1e-9)

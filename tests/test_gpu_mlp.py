@@ -1,5 +1,12 @@
 """The surrogate MLP kernels (aq_mlp_*) against the numpy oracle, and the
-trained surrogate against the method without it."""
+trained surrogate against the method without it.
+
+The kernels' contractions run on bf16 tensor cores with fp32 accumulation,
+the oracle restates them in float64 from the same bf16-rounded operands.  An
+activation the kernel computes in fp32 (erff GELU) and the oracle in float64
+can round to neighbouring bf16 values, which moves a downstream sum by one
+bf16 step (2^-7 relative) of one of its terms: hence 2e-3 (relative to the
+largest value) rather than fp32 rounding."""
 import ctypes as C
 
 import numpy as np
@@ -32,7 +39,7 @@ def test_forward_matches_oracle():
     x = np.random.default_rng(5).normal(size=(257, SG.N_IN)).astype(np.float32)
     y = m.forward_raw(x).cpu().numpy()
     yo, _ = MO.forward(p, x, DIMS)
-    assert y == pytest.approx(yo, rel=1e-4, abs=1e-4)
+    assert np.max(np.abs(y - yo)) < 2e-3 * max(1.0, np.abs(yo).max())
 
 
 def test_backward_matches_oracle():
@@ -43,7 +50,7 @@ def test_backward_matches_oracle():
     g = m.grad_raw(x, dy).cpu().numpy()
     go = MO.backward(p, x, dy, DIMS)
     scale = np.abs(go).max()
-    assert np.max(np.abs(g - go)) < 1e-4 * scale
+    assert np.max(np.abs(g - go)) < 2e-3 * scale
 
 
 def test_adam_step_matches_oracle():
