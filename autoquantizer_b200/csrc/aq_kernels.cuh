@@ -118,6 +118,12 @@ struct SimK {
   R col_c, col_s;  // cos and sin of the collider angle this launch
   int col_yshift;  // collider height in cells this launch, int(height / dx + 0.5)
   int col_node_cv;  // 1: collider velocity omega x r from the node itself (sdf_collision_no_arg)
+  // sparse grids (k_step's SP): grid block -> pool slot (-1: none), the
+  // slots handed out so far, each slot's block, the pools' capacity
+  int32_t* bptr;
+  int32_t* n_alloc;
+  int32_t* pool_blk;
+  int pool_cap;
 };
 
 struct StepArgs {
@@ -136,12 +142,6 @@ struct StepArgs {
   uint64_t sk;          // dithering key of the G2P substep
   int do_g2p, do_p2g, ranges;
   int raw_in;           // grid_in holds P2G sums: apply grid_op while reading
-  // sparse grids (k_step's SP): grid block -> pool slot (-1: none), the
-  // slots handed out so far, each slot's block, the pools' capacity
-  int32_t* bptr;
-  int32_t* n_alloc;
-  int32_t* pool_blk;
-  int pool_cap;
 };
 
 // Layout from the kernel parameter (nvcc build).
@@ -190,6 +190,18 @@ __device__ __forceinline__ void red_add_node(double4* g, double m, double a, dou
   atomicAdd(p + 3, c);
 }
 
+// Order-preserving map of doubles to unsigned 64-bit keys (key(a) < key(b)
+// iff a < b, NaN aside): non-negative values get the sign bit set, negative
+// ones are inverted.  Lets shared-memory 64-bit atomicMax/atomicMin keep
+// running extremes without compare-and-swap loops.
+__device__ __forceinline__ unsigned long long ord_key(double v) {
+  const unsigned long long b = (unsigned long long)__double_as_longlong(v);
+  return (b >> 63) ? ~b : (b | 0x8000000000000000ull);
+}
+__device__ __forceinline__ double ord_val(unsigned long long k) {
+  return __longlong_as_double((long long)((k >> 63) ? (k & 0x7fffffffffffffffull) : ~k));
+}
+
 __device__ __forceinline__ void atomic_max_d(double* a, double v) {
   unsigned long long* p = reinterpret_cast<unsigned long long*>(a);
   unsigned long long old = *p;
@@ -229,6 +241,15 @@ __device__ __forceinline__ int64_t node_in_slot(int slot, int i0, int i1, int i2
   constexpr int BS = Geo<D>::BS;
   const int l0 = i0 & (BS - 1), l1 = i1 & (BS - 1), l2 = i2 & (BS - 1);
   return (int64_t)slot * 64 + (D == 3 ? (l0 * BS + l1) * BS + l2 : l0 * BS + l1);
+}
+
+// Pool slot of an in-grid tile node from an item's table of the 3^D blocks
+// around its block (ob: the item's block coordinates)
+template <int D>
+__device__ __forceinline__ int tile_slot(const int* sslot, int ob0, int ob1, int ob2, int g0, int g1, int g2) {
+  constexpr int BS = Geo<D>::BS;
+  const int a0 = g0 / BS - ob0 + 1, a1 = g1 / BS - ob1 + 1, a2 = D == 3 ? g2 / BS - ob2 + 1 : 0;
+  return sslot[D == 3 ? (a0 * 3 + a1) * 3 + a2 : a0 * 3 + a1];
 }
 
 // Slot of block blk for a write, handed out now if the block has none: take
@@ -451,7 +472,7 @@ __device__ __forceinline__ void bspline(const R* x, const SimK<R>& K, int* base,
 
 // COL: compiled with the SDF collider (the library's own build always is;
 // the layout-specialized build only when a collider is set).  SP: sparse
-// grids (grid_in / grid_out are node pools reached through A.bptr).
+// grids (grid_in / grid_out are node pools reached through K.bptr).
 template <int D, bool HF, bool HM, class R, class LA, bool COL = true, bool SP = false>
 __global__ void __launch_bounds__(CH, AQ_STEP_MIN_BLOCKS(R, LA)) k_step(const __grid_constant__ aq_layout Lp, const SimK<R> K,
                                                 const StepArgs A) {
@@ -471,10 +492,16 @@ __global__ void __launch_bounds__(CH, AQ_STEP_MIN_BLOCKS(R, LA)) k_step(const __
   uint64_t* srec = reinterpret_cast<uint64_t*>(ptile + NWARP * TNP);  // CH x WS: each thread's record (RtLayout)
   __shared__ int sbox[6];  // tile-coordinate box of the item's P2G base cells (min[3], max[3])
   __shared__ int s_next;   // the CTA's next work item, claimed from A.item_ctr
-  __shared__ int sslot[27];  // sparse grids: pool slots of the 3^D grid blocks around the item's block
+  __shared__ int sslot[SP ? 27 : 1];  // sparse grids: pool slots of the 3^D blocks around the item's block
+  // range detection: the CTA's running max / min per slot (ord_key order)
+  __shared__ unsigned long long s_rmax[AQ_MAX_SLOTS], s_rmin[AQ_MAX_SLOTS];
 
   const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
   const int nitems = *A.n_items;
+  if (A.ranges && A.do_g2p && tid < NS) {
+    s_rmax[tid] = 0ull;   // below every key
+    s_rmin[tid] = ~0ull;  // above every key
+  }
   const R4* gin = reinterpret_cast<const R4*>(A.grid_in);
   R4* gout = reinterpret_cast<R4*>(A.grid_out);
   unsigned fl = 0, nfall = 0;
@@ -514,24 +541,21 @@ __global__ void __launch_bounds__(CH, AQ_STEP_MIN_BLOCKS(R, LA)) k_step(const __
       o[1] = (blk % K.nb[1]) * G::BS - 1;
       o[0] = (blk / K.nb[1]) * G::BS - 1;
     }
-    // block coordinates of the item; a tile node lies in the blocks ob - 1 .. ob + 1
-    const int ob0 = (o[0] + 1) / G::BS, ob1 = (o[1] + 1) / G::BS, ob2 = D == 3 ? (o[2] + 1) / G::BS : 0;
+    // block coordinates of the item (sparse grids); a tile node lies in the
+    // blocks ob - 1 .. ob + 1
+    const int ob0 = SP ? (o[0] + 1) / G::BS : 0, ob1 = SP ? (o[1] + 1) / G::BS : 0,
+              ob2 = (SP && D == 3) ? (o[2] + 1) / G::BS : 0;
     if (SP) {
       if (tid < (D == 3 ? 27 : 9)) {
         const int e0 = D == 3 ? tid / 9 : tid / 3, e1 = D == 3 ? (tid / 3) % 3 : tid % 3, e2 = D == 3 ? tid % 3 : 1;
         const int b0 = ob0 + e0 - 1, b1 = ob1 + e1 - 1, b2 = ob2 + e2 - 1;
         int sl = -1;
         if (b0 >= 0 && b0 < K.nb[0] && b1 >= 0 && b1 < K.nb[1] && (D == 2 || (b2 >= 0 && b2 < K.nb[2])))
-          sl = A.bptr[D == 3 ? ((int64_t)b0 * K.nb[1] + b1) * K.nb[2] + b2 : (int64_t)b0 * K.nb[1] + b1];
+          sl = K.bptr[D == 3 ? ((int64_t)b0 * K.nb[1] + b1) * K.nb[2] + b2 : (int64_t)b0 * K.nb[1] + b1];
         sslot[tid] = sl;
       }
       __syncthreads();
     }
-    // pool slot of an in-grid tile node, from the item's table
-    auto tile_slot = [&](int g0, int g1, int g2) -> int {
-      const int a0 = g0 / G::BS - ob0 + 1, a1 = g1 / G::BS - ob1 + 1, a2 = D == 3 ? g2 / G::BS - ob2 + 1 : 0;
-      return sslot[D == 3 ? (a0 * 3 + a1) * 3 + a2 : a0 * 3 + a1];
-    };
     if (A.do_g2p) {  // stage the grid tile (m, v after grid_op)
       for (int j = tid; j < TNP; j += CH) {
         int l0, l1, l2 = 0;
@@ -550,7 +574,7 @@ __global__ void __launch_bounds__(CH, AQ_STEP_MIN_BLOCKS(R, LA)) k_step(const __
         R4 g = zero4;
         if (ok) {
           if (SP) {
-            const int sl = tile_slot(g0, g1, g2);
+            const int sl = tile_slot<D>(sslot, ob0, ob1, ob2, g0, g1, g2);
             if (sl >= 0) g = gin[node_in_slot<D>(sl, g0, g1, g2)];
           } else {
             g = gin[cell_index<D>(K.res, g0, g1, g2)];
@@ -647,7 +671,7 @@ __global__ void __launch_bounds__(CH, AQ_STEP_MIN_BLOCKS(R, LA)) k_step(const __
                 } else {
                   const int n0 = base[0] + a, n1 = base[1] + b, n2 = D == 3 ? base[2] + c : 0;
                   if (SP) {
-                    const int sl = A.bptr[block_of<D>(K.nb, n0, n1, n2)];
+                    const int sl = K.bptr[block_of<D>(K.nb, n0, n1, n2)];
                     g = sl >= 0 ? gin[node_in_slot<D>(sl, n0, n1, n2)] : zero4;
                   } else {
                     g = gin[cell_index<D>(K.res, n0, n1, n2)];
@@ -733,8 +757,8 @@ __global__ void __launch_bounds__(CH, AQ_STEP_MIN_BLOCKS(R, LA)) k_step(const __
             mn = fmin(mn, __shfl_xor_sync(0xffffffffu, mn, k));
           }
           if (lane == 0) {
-            atomic_max_d(A.rmax + s, mx);
-            atomic_min_d(A.rmin + s, mn);
+            atomicMax(&s_rmax[s], ord_key(mx));
+            atomicMin(&s_rmin[s], ord_key(mn));
           }
         }
       }
@@ -858,7 +882,7 @@ __global__ void __launch_bounds__(CH, AQ_STEP_MIN_BLOCKS(R, LA)) k_step(const __
                 int sl = -1;
                 if (c0 < K.nb[0] && c1 < K.nb[1] && (D == 2 || c2 < K.nb[2])) {
                   const int64_t bk = D == 3 ? ((int64_t)c0 * K.nb[1] + c1) * K.nb[2] + c2 : (int64_t)c0 * K.nb[1] + c1;
-                  sl = claim_slot(A.bptr, A.n_alloc, A.pool_blk, A.pool_cap, bk);
+                  sl = claim_slot(K.bptr, K.n_alloc, K.pool_blk, K.pool_cap, bk);
                   if (sl < 0) fl |= AQ_ST_POOL_FULL;
                 }
                 fsl[qb] = sl;
@@ -928,8 +952,8 @@ __global__ void __launch_bounds__(CH, AQ_STEP_MIN_BLOCKS(R, LA)) k_step(const __
         if (g0 < 0 || g0 >= K.res[0] || g1 < 0 || g1 >= K.res[1] || (D == 3 && (g2 < 0 || g2 >= K.res[2])))
           continue;
         if (SP) {
-          int sl = tile_slot(g0, g1, g2);
-          if (sl < 0) sl = claim_slot(A.bptr, A.n_alloc, A.pool_blk, A.pool_cap, block_of<D>(K.nb, g0, g1, g2));
+          int sl = tile_slot<D>(sslot, ob0, ob1, ob2, g0, g1, g2);
+          if (sl < 0) sl = claim_slot(K.bptr, K.n_alloc, K.pool_blk, K.pool_cap, block_of<D>(K.nb, g0, g1, g2));
           if (sl >= 0)
             red_add_node(gout + node_in_slot<D>(sl, g0, g1, g2), sum.x, sum.y, sum.z, sum.w);
           else
@@ -944,6 +968,10 @@ __global__ void __launch_bounds__(CH, AQ_STEP_MIN_BLOCKS(R, LA)) k_step(const __
   }
   if (fl) atomicOr(A.status, fl);
   if (nfall) atomicAdd(A.fallbacks, (unsigned long long)nfall);
+  if (A.ranges && A.do_g2p && tid < NS) {  // one merge per CTA and slot
+    if (s_rmax[tid] != 0ull) atomic_max_d(A.rmax + tid, ord_val(s_rmax[tid]));
+    if (s_rmin[tid] != ~0ull) atomic_min_d(A.rmin + tid, ord_val(s_rmin[tid]));
+  }
 }
 
 }  // namespace aq

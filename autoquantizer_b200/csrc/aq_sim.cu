@@ -268,14 +268,14 @@ __global__ void k_pool_clear(const int32_t* __restrict__ n_alloc, int cap, R4* _
     pool[i] = z;
 }
 
-// pool slots for the 3^D grid blocks around every occupied block
+// Pool slots for the 3^D grid blocks around every occupied block, in two
+// passes so that a block wanted by several occupied neighbours takes one
+// slot: pass 0 marks every wanted block (-2; all writers store the same
+// value), pass 1 lets the one thread whose compare-and-swap moves the mark
+// on (-2 -> -3) take a slot for it.
 template <int D>
-__global__ void k_activate(const int32_t* __restrict__ occ_blk, const int32_t* __restrict__ n_occ_p, int nb0, int nb1,
-                           int nb2, int32_t* __restrict__ bptr, int32_t* __restrict__ n_alloc,
-                           int32_t* __restrict__ pool_blk, int cap, unsigned* __restrict__ status) {
-  constexpr int NN = D == 3 ? 27 : 9;
-  const int64_t t = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
-  if (t >= (int64_t)*n_occ_p * NN) return;
+__device__ __forceinline__ int64_t around_block(const int32_t* occ_blk, int NN, int64_t t, int nb0, int nb1,
+                                                int nb2) {
   const int o = (int)(t / NN), e = (int)(t - (int64_t)o * NN);
   const int blk = occ_blk[o];
   int b0, b1, b2 = 0;
@@ -289,9 +289,32 @@ __global__ void k_activate(const int32_t* __restrict__ occ_blk, const int32_t* _
   }
   const int c0 = b0 + (D == 3 ? e / 9 : e / 3) - 1, c1 = b1 + (D == 3 ? (e / 3) % 3 : e % 3) - 1,
             c2 = D == 3 ? b2 + e % 3 - 1 : 0;
-  if (c0 < 0 || c0 >= nb0 || c1 < 0 || c1 >= nb1 || (D == 3 && (c2 < 0 || c2 >= nb2))) return;
-  const int64_t nbk = D == 3 ? ((int64_t)c0 * nb1 + c1) * nb2 + c2 : (int64_t)c0 * nb1 + c1;
-  if (claim_slot(bptr, n_alloc, pool_blk, cap, nbk) < 0) atomicOr(status, AQ_ST_POOL_FULL);
+  if (c0 < 0 || c0 >= nb0 || c1 < 0 || c1 >= nb1 || (D == 3 && (c2 < 0 || c2 >= nb2))) return -1;
+  return D == 3 ? ((int64_t)c0 * nb1 + c1) * nb2 + c2 : (int64_t)c0 * nb1 + c1;
+}
+
+template <int D>
+__global__ void k_activate(const int32_t* __restrict__ occ_blk, const int32_t* __restrict__ n_occ_p, int nb0, int nb1,
+                           int nb2, int32_t* __restrict__ bptr, int32_t* __restrict__ n_alloc,
+                           int32_t* __restrict__ pool_blk, int cap, unsigned* __restrict__ status, int pass) {
+  constexpr int NN = D == 3 ? 27 : 9;
+  const int64_t t = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (t >= (int64_t)*n_occ_p * NN) return;
+  const int64_t nbk = around_block<D>(occ_blk, NN, t, nb0, nb1, nb2);
+  if (nbk < 0) return;
+  if (pass == 0) {
+    bptr[nbk] = -2;
+    return;
+  }
+  if (atomicCAS(bptr + nbk, -2, -3) != -2) return;  // another thread takes this block
+  const int slot = atomicAdd(n_alloc, 1);
+  if (slot < cap) {
+    pool_blk[slot] = (int32_t)nbk;
+    bptr[nbk] = slot;
+  } else {
+    bptr[nbk] = -1;
+    atomicOr(status, AQ_ST_POOL_FULL);
+  }
 }
 
 // node masses of a sparse grid as a dense float array (zero where no block)
@@ -734,10 +757,13 @@ struct SimImpl final : SimBase {
     k_pool_reset<R4><<<num_sms() * 4, 256, 0, st>>>(S_->bptr, S_->pool_blk, S_->n_alloc, S_->pool_cap,
                                                     (R4*)S_->grid[0], (R4*)S_->grid[1]);
     AQ_CUDA_TRY(cudaMemsetAsync(S_->n_alloc, 0, sizeof(int32_t), st));
-    const int64_t need = std::min<int64_t>((int64_t)nn * n_occ, S_->nblk);
+    const int64_t need = std::min<int64_t>((int64_t)nn * n_occ, S_->nblk);  // activated blocks, at most
     if (need > S_->pool_cap) {
       AQ_CUDA_TRY(cudaStreamSynchronize(st));
-      const int64_t want = std::min<int64_t>(need + need / 4 + 256, std::min<int64_t>(S_->nblk, 0x7fffffff));
+      // slack beyond the block count: slots lost to write races during the
+      // interval (claim_slot) must not starve the blocks that need one
+      const int64_t want =
+          std::min<int64_t>(std::min<int64_t>(need + need / 4 + 256, (int64_t)S_->nblk + 256), 0x7fffffffLL);
       for (int k = 0; k < 2; ++k) {
         if (S_->grid[k]) cudaFree(S_->grid[k]);
         S_->grid[k] = nullptr;
@@ -757,9 +783,10 @@ struct SimImpl final : SimBase {
       AQ_CUDA_TRY(cudaMemsetAsync(S_->pool_blk, 0xff, sizeof(int32_t) * (size_t)want, st));
       S_->pool_cap = (int)want;
     }
-    k_activate<D><<<grid_for((int64_t)n_occ * nn, 256), 256, 0, st>>>(S_->occ_blk, S_->n_alloc + 1, K.nb[0], K.nb[1],
-                                                                       K.nb[2], S_->bptr, S_->n_alloc, S_->pool_blk,
-                                                                       S_->pool_cap, S_->status);
+    for (int pass = 0; pass < 2; ++pass)
+      k_activate<D><<<grid_for((int64_t)n_occ * nn, 256), 256, 0, st>>>(S_->occ_blk, S_->n_alloc + 1, K.nb[0],
+                                                                         K.nb[1], K.nb[2], S_->bptr, S_->n_alloc,
+                                                                         S_->pool_blk, S_->pool_cap, S_->status, pass);
     AQ_CUDA_TRY(cudaGetLastError());
     S_->cur = nxt;
     S_->launches += 10;
@@ -794,10 +821,10 @@ struct SimImpl final : SimBase {
     a.do_p2g = do_p2g;
     a.ranges = S_->ranges_on;
     a.raw_in = do_g2p;  // grid_in holds the previous P2G sums; grid_op runs as the tile is staged
-    a.bptr = S_->bptr;
-    a.n_alloc = S_->n_alloc;
-    a.pool_blk = S_->pool_blk;
-    a.pool_cap = S_->pool_cap;
+    K.bptr = S_->bptr;
+    K.n_alloc = S_->n_alloc;
+    K.pool_blk = S_->pool_blk;
+    K.pool_cap = S_->pool_cap;
     K.col_c = (R)cos(S_->col_theta);
     K.col_s = (R)sin(S_->col_theta);
     K.col_yshift = (int)(S_->col_height / S_->P.dx + 0.5);
@@ -1018,10 +1045,15 @@ int aq_sim_create(const aq_params* P, const aq_layout* L, aq_sim** out) {
     void** p;
     size_t off;
   };
-  Part parts[24];
+  Part parts[40];
   int nparts = 0;
   size_t total = 0;
+  bool too_many = false;
   auto alloc = [&](void** p, size_t bytes) {
+    if (nparts >= (int)(sizeof(parts) / sizeof(parts[0]))) {  // reported below
+      too_many = true;
+      return;
+    }
     parts[nparts++] = Part{p, total};
     total += (bytes + 255) & ~(size_t)255;
   };
@@ -1058,6 +1090,10 @@ int aq_sim_create(const aq_params* P, const aq_layout* L, aq_sim** out) {
   alloc((void**)&s->rmin, sizeof(double) * AQ_MAX_SLOTS);
   alloc((void**)&s->dloss, sizeof(double));
   alloc((void**)&s->dstats, sizeof(double) * 5 * AQ_MAX_SLOTS);
+  if (too_many) {  // a buffer was left out: the list above outgrew parts
+    free_sim(s);
+    return AQ_E_LIMIT;
+  }
   e = cudaMalloc(&s->slab, total);
   if (e == cudaSuccess)
     for (int k = 0; k < nparts; ++k) *parts[k].p = static_cast<char*>(s->slab) + parts[k].off;

@@ -23,8 +23,11 @@ Experiments:
   falling_block_3d  the 3D elastic block of the adjoint benchmark (262,144
               particles, 64^3, dt 5e-5, 257 timesteps, f32); scheme recipe of
               run_mpm_elastic_3d.py:331-341 (ranges doubled, CR, bits + 1).
-The reference's 3D letter/propeller experiments need mesh emitters and the
-SDF collider, which this package does not implement.
+  elastic_3d  run_mpm_elastic_3d.py — the letters mesh emitted frame by
+              frame (add_mesh over the mesh voxelizer), 3D reference law.
+  fluid_3d    run_mpm_fluid_3d.py — two fluid slabs stirred by the rotating
+              SDF propeller collider (init_sdf_value; the autodiff path's
+              collider schedule for -a and -r).
 
 Each forward run re-seeds the dithering generator (seed = run index), which
 plays the role of the reference's per-run random state.
@@ -214,8 +217,9 @@ class Letters3D(Experiment):
     the letters mesh inputs/auto_quant.ply (load_mesh with scale (0.1, 0.1,
     2), offset (0.02, 0.02, 0.5), :249), emitted by add_mesh at
     translation (0.90, 1.6, 0.1) and (2.2, 1.6, 0.1) (add_letters, :45-61).
-    The pipeline emits the first frame's letters only; the reference emits
-    again every emit_step frames."""
+    The range pass and the forward runs follow the driver's frame loop
+    (run_forward_only, :87-157): every emit_step frames, while the next batch
+    fits, two more sets of letters (emit / add_letters, :45-84)."""
 
     name = "elastic_3d"
     file_name = "elastic_3d.npy"
@@ -236,6 +240,7 @@ class Letters3D(Experiment):
             c.n_grid = 128
             c.n_timesteps = 1024 * 16 + 1
             self.sample_density = 1
+            self.emit_step = 5
             c.precision = "f64"
         else:  # high resolution (:272-280); detect_range keeps 500^3 particles, 16k substeps (:307-316)
             c.n_particles = int(3e8) if kind == "forward" else 500 ** 3
@@ -243,6 +248,7 @@ class Letters3D(Experiment):
             c.n_grid = 128 * 2
             c.n_timesteps = 1024 * 40 + 1 if kind == "forward" else 1024 * 16
             self.sample_density = 8
+            self.emit_step = 4
         c.steps = 128
         c.p_vol = (1 / c.n_grid * 0.5) ** c.dim
         c.quantized_properties = {"x": 1, "v": 1, "C": 1, "F": 1}
@@ -260,10 +266,48 @@ class Letters3D(Experiment):
         return load_mesh(os.path.join(self.inputs, "auto_quant.ply"), scale=(0.1, 0.1, 2), offset=(0.02, 0.02, 0.5))
 
     def init(self, mpm):
+        """initialize(); the letters come with the frames (emit)."""
         mpm.initialize()
-        tri = self.mesh()
-        for t in ((0.90, 1.6, 0.1), (2.2, 1.6, 0.1)):
-            mpm.add_mesh(tri, velocity=(0.0, -4.0, 0.0), translation=t, sample_density=self.sample_density)
+        self.num_emit = 0
+        self._tri = self.mesh()
+
+    def emit(self, frame, mpm):
+        """emit / add_letters (run_mpm_elastic_3d.py:45-84): at frames that are
+        multiples of emit_step, while the batch fits below n_particles, two
+        letter meshes at x 0.90 and 2.2, y 1.6, z 0.1 + 0.006 k (k = frame //
+        emit_step), falling at 4 m/s; a batch is twice the particle count of
+        one mesh and starts at particle k times that."""
+        if frame % self.emit_step:
+            return
+        k = frame // self.emit_step
+        z = 0.1 + 0.006 * k
+        if self.num_emit == 0:
+            self.num_emit = 2 * mpm.cnt_mesh_particles_num(self._tri, translation=(0.90, 1.6, z),
+                                                           sample_density=self.sample_density)
+        if k * self.num_emit + self.num_emit >= mpm.n_particles:
+            return
+        mpm.current_idx = k * self.num_emit
+        for x0 in (0.90, 2.2):
+            mpm.add_mesh(self._tri, velocity=(0.0, -4.0, 0.0), translation=(x0, 1.6, z),
+                         sample_density=self.sample_density)
+
+    def run_frames(self, mpm, detect=False):
+        """The driver's frame loop (run_forward_only, :87-157): int(n_timestep
+        / steps + 1) frames, each emit() then `steps` substeps; with detect,
+        the state at the end of every frame is folded into the ranges
+        (detect_bound_kernel, get_limits), which are returned."""
+        max_frame = int(mpm.n_timestep / mpm.steps + 1.0)
+        for frame in range(max_frame):
+            self.emit(frame, mpm)
+            if mpm.current_idx == 0:
+                continue
+            mpm.substeps(mpm.steps)
+            if detect:
+                mpm.detect_bound_kernel(0)
+        if detect:
+            mpm.detect_bound()
+            return mpm.get_limits()
+        return None
 
     def scheme(self, grads, ranges, mode, eps):
         if mode != CR:
@@ -305,7 +349,10 @@ class Propeller3D(Experiment):
             c.n_timesteps = 1024 * 8 + 1
             c.p_vol = (1 / c.n_grid) ** 3
             c.ub = [c.n_grid * 2 - 3, c.n_grid - 3, c.n_grid * 2 - 3]
-            c.grid_res = [2 * c.n_grid, c.n_grid, 2 * c.n_grid]
+            # the slabs reach x, z = 1.984 (node 128 in the stencil) and the
+            # reference's grid is a 4096^3 index space: nodes beyond the
+            # walls must exist here too
+            c.grid_res = [2 * c.n_grid + 4, c.n_grid + 4, 2 * c.n_grid + 4]
             c.precision = "f64" if kind == "ad" else "f32"
             self.kind = "ad"
         else:
@@ -401,7 +448,10 @@ def detect_range(exp, cfg, root):
     max/min, saved as ranges/<exp>/<file>."""
     cfg.use_quantaichi = False
     mpm = _solver(exp, cfg)
-    ranges = mpm.run_forward_detect_ranges()
+    if hasattr(exp, "run_frames"):  # experiments that emit particles frame by frame
+        ranges = exp.run_frames(mpm, detect=True)
+    else:
+        ranges = mpm.run_forward_detect_ranges()
     _, fn = _paths(exp, root)
     os.makedirs(os.path.dirname(fn), exist_ok=True)
     np.save(fn, ranges)
@@ -434,7 +484,11 @@ def run(exp, cfg, n_runs, quant=True):
     for i in range(n_runs):
         cfg.seed = i
         mpm = _solver(exp, cfg)
-        losses.append(float(mpm.run_forward_only()))
+        if hasattr(exp, "run_frames"):  # particles emitted frame by frame
+            exp.run_frames(mpm)
+            losses.append(float(mpm.compute_loss()))
+        else:
+            losses.append(float(mpm.run_forward_only()))
         if mpm.status()[0] != 0:
             raise RuntimeError("simulator status flags 0x%x in run %d" % (mpm.status()[0], i))
         mpm._drop_sim()

@@ -212,7 +212,18 @@ class MPMSolver:
         return self._host
 
     def _drop_sim(self):
-        self._rabs_host = None  # range detection restarts with a new simulator
+        # the running ranges outlive the simulator (the reference keeps its
+        # limit fields for the solver's lifetime, across emissions): fold the
+        # device's into the host-side maxima first
+        if self._sim is not None and getattr(self, "_ranges_on_device", False):
+            ns = self.n_slots()
+            mx = (C.c_double * ns)()
+            mn = (C.c_double * ns)()
+            if _lib.lib().aq_sim_ranges_get(self._sim, mx, mn, _lib.stream_ptr()) == 0:
+                cur = np.maximum(np.abs(np.array(mx[:])), np.abs(np.array(mn[:])))
+                cur[~np.isfinite(cur)] = 0.0
+                h = getattr(self, "_rabs_host", None)
+                self._rabs_host = cur if h is None else np.maximum(h, cur)
         self._ranges_on_device = False
         if self._sim is not None:
             if self._col is not None:  # carry the collider's angle and height over

@@ -3,7 +3,7 @@ reference checkout (read-only), given as the one argument:
 
     python tests/golden/make_golden.py <reference checkout>
 
-Writes reference_data.json:
+Writes reference_data.json and propeller_higher.npz:
   * the reference's shipped autodiff sensitivities and detected ranges
     (mpm_exps/grads/*/*.npy, mpm_exps/ranges/*/*.npy);
   * the scene constants and the f64 reference loss of the 2D elastic
@@ -109,6 +109,15 @@ def main(ref):
     with open(os.path.join(HERE, "reference_data.json"), "w") as f:
         json.dump(out, f, indent=1)
     print("wrote", os.path.join(HERE, "reference_data.json"))
+    # the propeller collider of the 3D fluid experiment's gradient and range
+    # passes (run_mpm_fluid_3d.py:101-146 with init_sdf_value,
+    # mpm_solver.py:284-318), as float32 volumes, the precision the
+    # simulator reads them in
+    inp = os.path.join(ref, "mpm_exps", "inputs")
+    sdf = np.load(os.path.join(inp, "propeller_higher.npz"))["sdf"].astype(np.float32)
+    nrm = np.load(os.path.join(inp, "propeller_higher_normal.npz"))["sdf"].astype(np.float32)
+    np.savez_compressed(os.path.join(HERE, "propeller_higher.npz"), sdf=sdf, normal=nrm)
+    print("wrote", os.path.join(HERE, "propeller_higher.npz"))
 
 
 if __name__ == "__main__":

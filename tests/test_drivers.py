@@ -175,12 +175,20 @@ def test_fluid_3d_scheme_reproduces_the_drivers_recorded_bits():
 
 
 class _Recorder(_FakeSolver):
+    PER_MESH = 100  # particles a stand-in mesh seeds
+
     def __init__(self, cfg):
         super().__init__(cfg)
         self.calls = []
+        self.current_idx = 0
+        self.n_particles = cfg.n_particles
 
     def add_mesh(self, tri, **kw):
-        self.calls.append(("add_mesh", tri.shape, kw))
+        self.calls.append(("add_mesh", tri.shape, kw, self.current_idx))
+        self.current_idx += self.PER_MESH
+
+    def cnt_mesh_particles_num(self, tri, **kw):
+        return self.PER_MESH
 
     def init_sdf_value(self, sdf, normal, **kw):
         self.calls.append(("init_sdf_value", sdf.shape, normal.shape, kw))
@@ -211,14 +219,24 @@ def test_3d_experiment_setups(tmp_path):
     assert (cfg.n_particles, cfg.n_grid, cfg.dt, cfg.E, cfg.la, cfg.nu) == (int(3e8), 256, 7.5e-5, 5e5, 5e4, 0.2)
     m = _Recorder(cfg)
     le.init(m)
-    assert [c[2]["translation"] for c in m.calls] == [(0.90, 1.6, 0.1), (2.2, 1.6, 0.1)]
+    assert m.calls == []  # the letters come with the frames
+    for frame in range(9):
+        le.emit(frame, m)
+    # frames 0, 4, 8 (emit_step 4): two meshes each, z 0.1 + 0.006 k, each
+    # batch starting at k * (2 x the particles of one mesh)
+    zs = [0.1, 0.1 + 0.006, 0.1 + 0.012]
+    assert [c[2]["translation"] for c in m.calls] == [(x, 1.6, z) for z in zs for x in (0.90, 2.2)]
+    assert [c[3] for c in m.calls] == [0, 100, 200, 300, 400, 500]
     assert all(c[2]["sample_density"] == 8 and c[2]["velocity"] == (0.0, -4.0, 0.0) for c in m.calls)
+    m.n_particles = 700  # the next batch would not fit: no more letters
+    le.emit(12, m)
+    assert len(m.calls) == 6
 
     pr = D.Propeller3D()
     pr.inputs = str(inp)
     cfg = pr.config("ad")
     assert (cfg.n_particles, cfg.n_grid, cfg.dt, cfg.la) == (100 ** 3, 64, 4e-4, 5e5)
-    assert cfg.ub == [125, 61, 125] and cfg.grid_res == [128, 64, 128]
+    assert cfg.ub == [125, 61, 125] and cfg.grid_res == [132, 68, 132]
     m = _Recorder(cfg)
     pr.init(m)
     assert m.calls[0][0] == "init_sdf_value" and m.calls[0][3]["height_rate"] == 0.15

@@ -121,3 +121,27 @@ def test_detect_bound_kernel_folds_only_the_states_it_is_called_on():
     np.testing.assert_allclose(lim[d:], expect, rtol=1e-12, atol=0)
     c = s.state_values()
     assert np.any(np.abs(c).max(0)[d:] > expect)  # the later state would have widened them
+
+
+def test_fluid_3d_ranges_match_reference_statistically(tmp_path):
+    """The -r pass of the 3D fluid experiment (run_mpm_fluid_3d.py:101-146:
+    1e6 particles in two slabs, 64 grid over 2 x 1 x 2, 8192 substeps of
+    4e-4, the propeller collider on the autodiff schedule), against the
+    reference's shipped ranges/fluid_3d/fluid_3d.npy.  add_cube seeds with
+    random positions (ti.random in the reference), so the extremes agree as
+    statistics: positions exactly 2, every v and C range within a factor of
+    2, max |J| within 0.1 (J near 1)."""
+    z = np.load(os.path.join(os.path.dirname(__file__), "golden", "propeller_higher.npz"))
+    np.savez(tmp_path / "propeller_higher.npz", sdf=z["sdf"])
+    np.savez(tmp_path / "propeller_higher_normal.npz", sdf=z["normal"])
+    exp = D.Propeller3D()
+    exp.inputs = str(tmp_path)
+    out = D.detect_range(exp, exp.config("ranges"), str(tmp_path))
+    ours = np.array(out["ranges"])
+    ref = np.array(GOLD["ranges"]["fluid_3d/fluid_3d.npy"])
+    print("fluid_3d ranges ours/reference:", np.array2string(ours / ref, precision=3))
+    assert ours.shape == ref.shape == (16,)
+    assert np.array_equal(ours[:3], [2.0, 2.0, 2.0])
+    ratio = ours[3:15] / ref[3:15]
+    assert np.all((ratio > 0.5) & (ratio < 2.0)), ratio
+    assert abs(ours[15] - ref[15]) < 0.1, (ours[15], ref[15])

@@ -89,16 +89,19 @@ def test_sparse_grid_mass_matches_dense():
 def test_sparse_1024_index_space_matches_dense():
     """500,000 particles in a block of 40 cells a side inside a 1024^3 grid:
     occupied blocks are about 0.1 % of the 256^3 blocks.  The dense run
-    (33 GB of grids) and the sparse one agree to the parity tolerance."""
+    (69 GB of f64 grids) and the sparse one agree to 1e-8 relative (in f32
+    the stiff block amplifies the different summation orders of the two
+    into differences of C far above rounding, as any two runs would)."""
     from autoquantizer_b200.mpm_solver import MPMSolver
 
     def run(sparse):
         cfg, vals = scenes.falling_block_3d(n=500000, n_grid=1024)
         cfg.dt = 5e-6
+        cfg.precision = "f64"
         cfg.sparse_grid = sparse
         s = MPMSolver(cfg)
         s.set_particles(vals)
-        s.substeps(20)
+        s.substeps(10)
         fl, _ = s.status()
         assert fl == 0
         return s.state_values(), (s.sparse_blocks() if sparse else None)
@@ -108,4 +111,4 @@ def test_sparse_1024_index_space_matches_dense():
     assert 0 < occupied <= slots < 0.1 * 256 ** 3
     for k in range(dense.shape[1]):
         scale = max(1.0, float(np.abs(dense[:, k]).max()))
-        assert np.max(np.abs(sparse[:, k] - dense[:, k])) <= 2e-5 * scale, k
+        assert np.max(np.abs(sparse[:, k] - dense[:, k])) <= 1e-8 * scale, k
