@@ -233,12 +233,51 @@ __device__ __forceinline__ void offs(int o, int* off) {
 
 // ------------------------------------------------------------- forward
 
+// Runs of equal keys over consecutive lanes of a warp.  The state is sorted
+// by base cell, so a run holds the warp's particles of one cell, which add
+// into the same 3^D nodes: run_sum adds a value over the lane's run in
+// log2(longest run) shuffle steps, and the run's first lane makes the one
+// global atomic for the whole run instead of one per particle.
+struct WarpRuns {
+  int lane, end, steps;  // end: last lane of this lane's run
+  bool head;             // this lane starts its run
+};
+
+__device__ __forceinline__ WarpRuns warp_runs(long long key) {
+  WarpRuns r;
+  r.lane = threadIdx.x & 31;
+  const long long prev = __shfl_up_sync(0xffffffffu, key, 1);
+  r.head = r.lane == 0 || prev != key;
+  const unsigned starts = __ballot_sync(0xffffffffu, r.head);
+  const unsigned later = r.lane == 31 ? 0u : (starts & (0xffffffffu << (r.lane + 1)));
+  r.end = later ? __ffs(later) - 2 : 31;
+  const int len = r.head ? r.end - r.lane + 1 : 1;
+  const int maxlen = (int)__reduce_max_sync(0xffffffffu, (unsigned)len);
+  int steps = 0;
+  while ((1 << steps) < maxlen) ++steps;
+  r.steps = steps;
+  return r;
+}
+
+// After the call the run's first lane holds the sum of v over the run.
+template <class R>
+__device__ __forceinline__ R run_sum(R v, const WarpRuns& r) {
+  for (int k = 0; k < r.steps; ++k) {
+    const int d = 1 << k;
+    const R o = __shfl_down_sync(0xffffffffu, v, d);
+    if (r.lane + d <= r.end) v += o;
+  }
+  return v;
+}
+
 template <int D, bool HF, class R>
 __global__ void __launch_bounds__(128) k_ad_p2g(const AdK<R> K, const R* __restrict__ st, int64_t n,
                                                 R* __restrict__ grid) {
   typedef Sch<D, HF, false> S;
-  const int64_t p = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
-  if (p >= n) return;
+  const int64_t p0 = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  const bool active = p0 < n;
+  if (__all_sync(0xffffffffu, !active)) return;
+  const int64_t p = active ? p0 : n - 1;  // lanes past the end take part in the shuffles only
   const R* s = st + p * K.NS;
   int base[3];
   R fx[3], w[3][3], dw[3][3];
@@ -247,24 +286,31 @@ __global__ void __launch_bounds__(128) k_ad_p2g(const AdK<R> K, const R* __restr
   ad_sigma<D, HF, R>(K, s, sig);
 #pragma unroll
   for (int k = 0; k < D * D; ++k) A[k] = K.kst * sig[k] + K.p_mass * s[S::C + k];
+  const WarpRuns runs = warp_runs(active ? (long long)ad_cell<D>(K.res, base) : -1 - (long long)(threadIdx.x & 31));
+  const R on = active ? (R)1 : (R)0;
   for (int o = 0; o < (D == 3 ? 27 : 9); ++o) {
     int off[3], I[3];
     offs<D>(o, off);
-    R wt = 1, dpos[3];
+    R wt = on, dpos[3];
 #pragma unroll
     for (int d = 0; d < D; ++d) {
       wt *= w[off[d]][d];
       dpos[d] = ((R)off[d] - fx[d]) * K.dx;
       I[d] = base[d] + off[d];
     }
-    R* g = grid + 4 * ad_cell<D>(K.res, I);
-    atomicAdd(g, wt * K.p_mass);
+    R val[4];
+    val[0] = run_sum(wt * K.p_mass, runs);
 #pragma unroll
     for (int d = 0; d < D; ++d) {
       R a = K.p_mass * s[S::V + d];
 #pragma unroll
       for (int e = 0; e < D; ++e) a += A[d * D + e] * dpos[e];
-      atomicAdd(g + 1 + d, wt * a);
+      val[1 + d] = run_sum(wt * a, runs);
+    }
+    if (active && runs.head) {
+      R* g = grid + 4 * ad_cell<D>(K.res, I);
+#pragma unroll
+      for (int k = 0; k < 1 + D; ++k) atomicAdd(g + k, val[k]);
     }
   }
 }
@@ -369,14 +415,17 @@ __global__ void __launch_bounds__(128) k_ad_g2p_bwd(const AdK<R> K, const R* __r
                                                     const R* __restrict__ gv, const R* __restrict__ ab_out,
                                                     R* __restrict__ ab_in, R* __restrict__ gvb, int64_t n) {
   typedef Sch<D, HF, false> S;
-  const int64_t p = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
-  if (p >= n) return;
+  const int64_t p0 = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  const bool active = p0 < n;
+  if (__all_sync(0xffffffffu, !active)) return;
+  const int64_t p = active ? p0 : n - 1;  // lanes past the end take part in the shuffles only
   const R* s = st + p * K.NS;
   const R* bo = ab_out + p * K.NS;
   R* bi = ab_in + p * K.NS;
   int base[3];
   R fx[3], w[3][3], dw[3][3];
   ad_weights<D, R>(s + S::X, K, base, fx, w, dw);
+  const WarpRuns runs = warp_runs(active ? (long long)ad_cell<D>(K.res, base) : -1 - (long long)(threadIdx.x & 31));
   // recompute new C (needed for F' = (I + dt C') F)
   R nC[9] = {0, 0, 0, 0, 0, 0, 0, 0, 0};
   for (int o = 0; o < (D == 3 ? 27 : 9); ++o) {
@@ -446,8 +495,8 @@ __global__ void __launch_bounds__(128) k_ad_g2p_bwd(const AdK<R> K, const R* __r
       R cd = 0;  // (C'bar dpos)_d
 #pragma unroll
       for (int e = 0; e < D; ++e) cd += Cpb[d * D + e] * dpos[e];
-      const R vb = wt * (vpb[d] + K.four_inv_dx2 * cd);
-      atomicAdd(gvb + 4 * cell + d, vb);
+      const R vb = run_sum(active ? wt * (vpb[d] + K.four_inv_dx2 * cd) : (R)0, runs);
+      if (active && runs.head) atomicAdd(gvb + 4 * cell + d, vb);
       wb += g[d] * (vpb[d] + K.four_inv_dx2 * cd);
     }
     // through dpos = x_i - x_p: xbar -= 4/dx^2 w C'bar^T v_i
@@ -468,6 +517,7 @@ __global__ void __launch_bounds__(128) k_ad_g2p_bwd(const AdK<R> K, const R* __r
       xb[d] += wb * gw;
     }
   }
+  if (!active) return;
   for (int k = 0; k < K.NS; ++k) bi[k] = 0;
 #pragma unroll
   for (int d = 0; d < D; ++d) bi[S::X + d] = xb[d];

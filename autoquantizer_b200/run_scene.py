@@ -1,6 +1,6 @@
 """Run one of the seeded scenes for a number of substeps and print timing.
 
-    python -m autoquantizer_b200.run_scene --scene mixed_boxes_3d --substeps 8 [--fp32] [--n N] [--grid G]
+    python -m autoquantizer_b200.run_scene --scene mixed_boxes_3d --substeps 8 [--fp32] [--sparse] [--n N] [--grid G]
     python -m autoquantizer_b200.run_scene --device-gen --n 300000000 --grid 640 --substeps 50
 
 A small fixed workload for profiler captures of single kernel launches.
@@ -22,6 +22,7 @@ def main():
     ap.add_argument("--sort-interval", type=int, default=None)
     ap.add_argument("--device-gen", action="store_true",
                     help="mixed_boxes_3d generated on the GPU (large particle counts)")
+    ap.add_argument("--sparse", action="store_true", help="sparse grid (block table and node pools)")
     args = ap.parse_args()
 
     import torch
@@ -44,6 +45,7 @@ def main():
         cfg, vals = getattr(scenes, args.scene)(**kw)
     if args.sort_interval:
         cfg.sort_interval = args.sort_interval
+    cfg.sparse_grid = bool(args.sparse)
     s = MPMSolver(cfg)
     s.set_particles(vals)
     s.substeps(args.warmup)
@@ -57,7 +59,8 @@ def main():
                       "ms_per_substep": 1e3 * dt / args.substeps,
                       "particle_substeps_per_s": cfg.n_particles * args.substeps / dt,
                       "bytes_per_particle": s.bytes_per_particle(),
-                      "status": fl, "tile_fallbacks": fb}))
+                      "status": fl, "tile_fallbacks": fb,
+                      "sparse_blocks": s.sparse_blocks() if args.sparse else None}))
 
 
 if __name__ == "__main__":

@@ -406,7 +406,15 @@ def main():
     ap.add_argument("--out", default=None)
     ap.add_argument("--save-data", default=None, help="write the generated datasets to this .npz")
     ap.add_argument("--load-data", default=None, help="read datasets written by --save-data instead")
+    ap.add_argument("--fit-only", type=int, default=0, metavar="STEPS",
+                    help="only train STEPS steps at batch 512 on random data (a small workload for profilers)")
     args = ap.parse_args()
+    if args.fit_only:
+        rng = np.random.default_rng(0)
+        X, Y = rng.normal(size=(512, N_IN)), rng.normal(size=(512, N_OUT))
+        hist = MLP(seed=0).fit(X, Y, np.ones_like(Y), steps=args.fit_only, batch=512)
+        print(json.dumps({"fit_only_steps": args.fit_only, "loss": hist[-1][1]}))
+        return
     t0 = time.perf_counter()
     if args.load_data:
         z = np.load(args.load_data, allow_pickle=False)
