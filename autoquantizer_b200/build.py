@@ -48,6 +48,7 @@ def stale():
 # the names are the include strings the sources use
 JIT_HEADERS = [("aq_kernels.cuh", os.path.join(CSRC, "aq_kernels.cuh")),
                ("aq_codec.cuh", os.path.join(CSRC, "aq_codec.cuh")),
+               ("aq_step_config.h", os.path.join(CSRC, "aq_step_config.h")),
                ("../../include/aq.h", os.path.join(ROOT, "include", "aq.h"))]
 
 

@@ -199,6 +199,7 @@ void* jit_k_step(int D, bool HF, bool HM, bool f64, bool col, bool sparse, const
     }
   }
   if (from_dir) extra.push_back(std::string("-I") + sdir);
+  extra.push_back("-DAQ_CH=" + std::to_string(AQ_CH));  // the launch's CTA size
   std::vector<const char*> opts = {"--gpu-architecture=sm_100a", "-std=c++17", "-lineinfo", "-DAQ_JIT=1"};
   for (const std::string& x : extra) opts.push_back(x.c_str());
   const nvrtcResult rc = g_nv.compile(prog, (int)opts.size(), opts.data());

@@ -6,6 +6,7 @@
 #include <string>
 
 #include "../../include/aq.h"
+#include "aq_step_config.h"
 
 namespace aq {
 
@@ -19,9 +20,9 @@ std::string jit_layout_source(const aq_layout& L);
 // registers (short records) rather than in a shared-memory slot per thread.
 constexpr int kJitRegRecordMaxWords = 8;
 inline bool jit_reg_record(const aq_layout& L) { return L.n_words <= kJitRegRecordMaxWords; }
-// CTAs per SM k_step's registers are budgeted for (128-thread CTAs): 6
-// (80 registers) with register records, 4 (128) with shared-memory slots
-constexpr int kJitRegRecordMinBlocks = 6, kJitSlotMinBlocks = 4;
+// CTAs per SM k_step's registers are budgeted for: 80 registers a thread
+// with register records, 128 with shared-memory slots
+constexpr int kJitRegRecordMinBlocks = 768 / AQ_CH, kJitSlotMinBlocks = 512 / AQ_CH;
 int jit_set_smem(void* fn, int bytes);
 int jit_occupancy(void* fn, int block, size_t smem, int* out);
 int jit_launch(void* fn, unsigned grid, unsigned block, size_t smem, cudaStream_t st, void** args);

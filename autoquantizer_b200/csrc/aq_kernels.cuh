@@ -21,12 +21,12 @@
 //   binning  : per-cell counts/offsets, per-particle key and rank, and one
 //              work item per occupied block (block, first record, count).
 //
-// k_step, persistent CTAs of CH = 128 threads claiming work items (whole
-// cell blocks, the fullest first) from a counter:
+// k_step, persistent CTAs of CH = 64 threads (two warps) claiming work items
+// (whole cell blocks, the fullest first) from a counter:
 //   1. stage the block's grid tile (7^3 nodes in 3D: the block, the cell
 //      below it and the stencil) in shared memory, applying grid_op (and
 //      the SDF collider when compiled in) to every node (G2P source);
-//   2. the 4 warps take the block's records 32 at a time (units), without
+//   2. the warps take the block's records 32 at a time (units), without
 //      CTA barriers between units; per unit each lane loads its record into
 //      registers (layout-specialized build, short records) or its shared
 //      slot, and
@@ -43,6 +43,7 @@
 #pragma once
 
 #include "aq_codec.cuh"
+#include "aq_step_config.h"
 
 #ifdef __CUDACC_RTC__
 #define AQ_POS_INF __int_as_float(0x7f800000)
@@ -53,15 +54,19 @@
 
 namespace aq {
 
-#ifndef AQ_CH
-#define AQ_CH 128
-#endif
-constexpr int CH = AQ_CH;  // particles per work item = threads per CTA
+// Threads per CTA.  Two warps per work item: the warps of an item wait for
+// each other only at its staging and flush barriers, and the fewer warps an
+// item has, the less time they spend waiting there and the fewer private
+// tiles its flush sums (at the same 24 resident warps per SM, 64-thread CTAs
+// measured 2.7 % faster than 128-thread CTAs on the 3D mixed scene, 96
+// 2.4 %, 32 4.5 % slower: shared memory then holds 17 CTAs only).
+constexpr int CH = AQ_CH;  // AQ_CH: aq_step_config.h
 constexpr int NWARP = CH / 32;
 // CTAs per SM the register allocation of k_step must allow: the layout's
-// choice (LA::kMinBlocks) for float, 4 (128 registers) for double.  Short
-// records kept in registers run best at 6 CTAs (80 registers: more
-// resident warps beat the extra spills); records in shared-memory slots at 4.
+// choice (LA::kMinBlocks) for float, 512 / CH (128 registers) for double.
+// Short records kept in registers run best at 768 / CH CTAs (80 registers:
+// more resident warps beat the extra spills); records in shared-memory
+// slots at 512 / CH.
 #ifndef AQ_STEP_MIN_BLOCKS
 #define AQ_STEP_MIN_BLOCKS(R, LA) (sizeof(R) == 8 ? 512 / AQ_CH : LA::kMinBlocks)
 #endif

@@ -54,28 +54,47 @@ __device__ __forceinline__ float ld_f<__nv_bfloat16>(const __nv_bfloat16* p, int
   return __bfloat162float(p[i]);
 }
 
-// Stage rows [r0, r0 + GT) x k [k0, k0 + GK) of an operand into s[GT][GKP]
-// (zeros outside [R, K)).  kmajor: element (r, k) at src[r * ld + k], else
-// at src[k * ld + r].
+// A chunk of an operand (rows [r0, r0 + GT) x k [k0, k0 + GK)) is moved in
+// two steps: stage_load reads the thread's GPT element pairs into registers
+// (all loads issued together, zeros outside [R, K)), stage_store writes them
+// to s[GT][GKP] as bf16.  The next chunk's loads are issued before the
+// current chunk's products, so their latency overlaps the tensor-core work.
+// kmajor: element (r, k) at src[r * ld + k], else at src[k * ld + r].
+constexpr int GTHREADS = 128;                   // threads per GEMM CTA
+constexpr int GPT = GT * GK / 2 / GTHREADS;     // element pairs per thread and operand
+
+__device__ __forceinline__ void pair_pos(int i, bool kmajor, int& r, int& kk) {
+  if (kmajor) {  // consecutive threads along k
+    r = i / (GK / 2);
+    kk = 2 * (i - r * (GK / 2));
+  } else {  // consecutive threads along r
+    kk = 2 * (i / GT);
+    r = i - (kk / 2) * GT;
+  }
+}
+
 template <class T>
-__device__ __forceinline__ void stage(__nv_bfloat16 (*s)[GKP], const T* src, int64_t ld, bool kmajor, int r0, int R,
-                                      int k0, int K) {
-  for (int i = threadIdx.x; i < GT * GK / 2; i += blockDim.x) {
+__device__ __forceinline__ void stage_load(float (&v)[GPT][2], const T* src, int64_t ld, bool kmajor, int r0, int R,
+                                           int k0, int K) {
+#pragma unroll
+  for (int q = 0; q < GPT; ++q) {
     int r, kk;
-    if (kmajor) {  // consecutive threads along k
-      r = i / (GK / 2);
-      kk = 2 * (i - r * (GK / 2));
-    } else {  // consecutive threads along r
-      kk = 2 * (i / GT);
-      r = i - (kk / 2) * GT;
-    }
+    pair_pos(threadIdx.x + q * GTHREADS, kmajor, r, kk);
     const int gr = r0 + r, gk = k0 + kk;
-    float v0 = 0.f, v1 = 0.f;
+    v[q][0] = v[q][1] = 0.f;
     if (gr < R) {
-      if (gk < K) v0 = ld_f(src, kmajor ? (int64_t)gr * ld + gk : (int64_t)gk * ld + gr);
-      if (gk + 1 < K) v1 = ld_f(src, kmajor ? (int64_t)gr * ld + gk + 1 : (int64_t)(gk + 1) * ld + gr);
+      if (gk < K) v[q][0] = ld_f(src, kmajor ? (int64_t)gr * ld + gk : (int64_t)gk * ld + gr);
+      if (gk + 1 < K) v[q][1] = ld_f(src, kmajor ? (int64_t)gr * ld + gk + 1 : (int64_t)(gk + 1) * ld + gr);
     }
-    *reinterpret_cast<__nv_bfloat162*>(&s[r][kk]) = __floats2bfloat162_rn(v0, v1);
+  }
+}
+
+__device__ __forceinline__ void stage_store(__nv_bfloat16 (*s)[GKP], const float (&v)[GPT][2], bool kmajor) {
+#pragma unroll
+  for (int q = 0; q < GPT; ++q) {
+    int r, kk;
+    pair_pos(threadIdx.x + q * GTHREADS, kmajor, r, kk);
+    *reinterpret_cast<__nv_bfloat162*>(&s[r][kk]) = __floats2bfloat162_rn(v[q][0], v[q][1]);
   }
 }
 
@@ -92,7 +111,7 @@ __device__ __forceinline__ void mma_bf16(float (&d)[4], uint32_t a0, uint32_t a1
 //      EPI_XGRAD out = act ? acc * gelu'(aux[m][n]) : acc
 //      EPI_STORE out = acc
 template <class TA, class TB, int EPI>
-__global__ void __launch_bounds__(128) k_gemm_bf16(const TA* __restrict__ A, int64_t lda, int a_kmajor,
+__global__ void __launch_bounds__(GTHREADS) k_gemm_bf16(const TA* __restrict__ A, int64_t lda, int a_kmajor,
                                                    const TB* __restrict__ B, int64_t ldb, int b_kmajor, int M, int N,
                                                    int K, const float* __restrict__ bias, const float* __restrict__ aux,
                                                    float* __restrict__ Z, float* __restrict__ out, int act) {
@@ -109,10 +128,17 @@ __global__ void __launch_bounds__(128) k_gemm_bf16(const TA* __restrict__ A, int
     for (int j = 0; j < 4; ++j)
 #pragma unroll
       for (int e = 0; e < 4; ++e) acc[i][j][e] = 0.f;
+  float va[GPT][2], vb[GPT][2];
+  stage_load(va, A, lda, a_kmajor != 0, m0, M, 0, K);
+  stage_load(vb, B, ldb, b_kmajor != 0, n0, N, 0, K);
   for (int k0 = 0; k0 < K; k0 += GK) {
-    stage(sA, A, lda, a_kmajor != 0, m0, M, k0, K);
-    stage(sB, B, ldb, b_kmajor != 0, n0, N, k0, K);
+    stage_store(sA, va, a_kmajor != 0);
+    stage_store(sB, vb, b_kmajor != 0);
     __syncthreads();
+    if (k0 + GK < K) {  // next chunk in flight during this chunk's products
+      stage_load(va, A, lda, a_kmajor != 0, m0, M, k0 + GK, K);
+      stage_load(vb, B, ldb, b_kmajor != 0, n0, N, k0 + GK, K);
+    }
 #pragma unroll
     for (int kk = 0; kk < GK; kk += 16) {
       uint32_t af[2][4], bf[4][2];
@@ -259,11 +285,11 @@ int aq_mlp_forward(int32_t in, int32_t h, int32_t out, const float* d_params, co
     a1 = tmp;
     a2 = tmp + (size_t)B * h;
   }
-  k_gemm_bf16<float, __nv_bfloat16, EPI_FWD><<<gemm_grid(B, h), 128, 0, st>>>(
+  k_gemm_bf16<float, __nv_bfloat16, EPI_FWD><<<gemm_grid(B, h), GTHREADS, 0, st>>>(
       d_x, in, 1, wb + o.w1, in, 1, B, h, in, d_params + o.b1, nullptr, z1, a1, 1);
-  k_gemm_bf16<float, __nv_bfloat16, EPI_FWD><<<gemm_grid(B, h), 128, 0, st>>>(
+  k_gemm_bf16<float, __nv_bfloat16, EPI_FWD><<<gemm_grid(B, h), GTHREADS, 0, st>>>(
       a1, h, 1, wb + o.w2, h, 1, B, h, h, d_params + o.b2, nullptr, z2, a2, 1);
-  k_gemm_bf16<float, __nv_bfloat16, EPI_FWD><<<gemm_grid(B, out), 128, 0, st>>>(
+  k_gemm_bf16<float, __nv_bfloat16, EPI_FWD><<<gemm_grid(B, out), GTHREADS, 0, st>>>(
       a2, h, 1, wb + o.w3, h, 1, B, out, h, d_params + o.b3, nullptr, nullptr, d_y, 0);
   AQ_CUDA_TRY(cudaGetLastError());
   if (tmp) AQ_CUDA_TRY(cudaFreeAsync(tmp, st));
@@ -285,19 +311,19 @@ int aq_mlp_backward(int32_t in, int32_t h, int32_t out, const uint16_t* d_params
   float* dz2 = dz;
   float* dz1 = dz + (size_t)B * h;
   // layer 3: dW3 = dy^T a2, db3, dz2 = (dy W3) * gelu'(z2)
-  k_gemm_bf16<float, float, EPI_STORE><<<gemm_grid(out, h), 128, 0, st>>>(
+  k_gemm_bf16<float, float, EPI_STORE><<<gemm_grid(out, h), GTHREADS, 0, st>>>(
       d_dy, out, 0, a2, h, 0, out, h, B, nullptr, nullptr, nullptr, d_grad + o.w3, 0);
   k_colsum<<<grid_for(out, 128), 128, 0, st>>>(d_dy, B, out, d_grad + o.b3);
-  k_gemm_bf16<float, __nv_bfloat16, EPI_XGRAD><<<gemm_grid(B, h), 128, 0, st>>>(
+  k_gemm_bf16<float, __nv_bfloat16, EPI_XGRAD><<<gemm_grid(B, h), GTHREADS, 0, st>>>(
       d_dy, out, 1, wb + o.w3, h, 0, B, h, out, nullptr, z2, nullptr, dz2, 1);
   // layer 2
-  k_gemm_bf16<float, float, EPI_STORE><<<gemm_grid(h, h), 128, 0, st>>>(
+  k_gemm_bf16<float, float, EPI_STORE><<<gemm_grid(h, h), GTHREADS, 0, st>>>(
       dz2, h, 0, a1, h, 0, h, h, B, nullptr, nullptr, nullptr, d_grad + o.w2, 0);
   k_colsum<<<grid_for(h, 128), 128, 0, st>>>(dz2, B, h, d_grad + o.b2);
-  k_gemm_bf16<float, __nv_bfloat16, EPI_XGRAD><<<gemm_grid(B, h), 128, 0, st>>>(
+  k_gemm_bf16<float, __nv_bfloat16, EPI_XGRAD><<<gemm_grid(B, h), GTHREADS, 0, st>>>(
       dz2, h, 1, wb + o.w2, h, 0, B, h, h, nullptr, z1, nullptr, dz1, 1);
   // layer 1
-  k_gemm_bf16<float, float, EPI_STORE><<<gemm_grid(h, in), 128, 0, st>>>(
+  k_gemm_bf16<float, float, EPI_STORE><<<gemm_grid(h, in), GTHREADS, 0, st>>>(
       dz1, h, 0, d_x, in, 0, h, in, B, nullptr, nullptr, nullptr, d_grad + o.w1, 0);
   k_colsum<<<grid_for(h, 128), 128, 0, st>>>(dz1, B, h, d_grad + o.b1);
   AQ_CUDA_TRY(cudaGetLastError());

@@ -100,3 +100,16 @@ def test_surrogate_beats_the_method_without_it():
     sur, bl = SG.evaluate(mlp, Xte, Yte, Mte, mte, baseline=base)
     assert sur["log_err"] < 0.7 * bl["log_err"], (sur, bl)
     assert sur["within_1_bit"] >= bl["within_1_bit"], (sur, bl)
+
+
+def test_ensemble_predicts_the_members_mean():
+    """The ensemble's on-device mean equals the mean of its members' own
+    predictions; the members start from different weights and batch orders."""
+    rng = np.random.default_rng(2)
+    X = rng.normal(size=(64, SG.N_IN))
+    Y = rng.normal(size=(64, SG.N_OUT))
+    e = SG.Ensemble(3, seed=5)
+    e.fit(X, Y, np.ones_like(Y), steps=20, batch=32)
+    each = [m.predict(X) for m in e.members]
+    assert not np.allclose(each[0], each[1])
+    assert e.predict(X) == pytest.approx(np.mean(each, axis=0), rel=1e-5, abs=1e-6)

@@ -71,7 +71,16 @@ def test_targets_and_scheme():
     for gi in range(3, 12):
         if groups[gi]:
             assert r[gi] == pytest.approx(2 * stats[groups[gi], 3].max())
-    bits = S.scheme_bits(y, m, r, loss=123.0, tol_rel=1e-3)
     idx = np.where(m > 0)[0]
     want, _ = solvers.LagrangianEB(10.0 ** y[idx] * r[idx] ** 2, ref=123.0, tol_rel=1e-3)
-    assert bits[idx].tolist() == (want + 1).tolist() and np.all(bits[m == 0] == 0)
+    raw = S.scheme_bits(y, m, r, loss=123.0, tol_rel=1e-3, storable=False)
+    assert raw[idx].tolist() == (want + 1).tolist() and np.all(raw[m == 0] == 0)
+    bits = S.scheme_bits(y, m, r, loss=123.0, tol_rel=1e-3)
+    assert bits[idx].tolist() == np.maximum(want + 1, S.MIN_WIDTH).tolist() and np.all(bits[m == 0] == 0)
+    # a group whose error hardly matters gets a solver width below the
+    # layout's minimum; the storable scheme clamps it, the solver's keeps it
+    y2 = y.copy()
+    y2[idx[0]] -= 12.0
+    raw2 = S.scheme_bits(y2, m, r, loss=123.0, tol_rel=1e-3, storable=False)
+    assert raw2[idx[0]] < S.MIN_WIDTH
+    assert S.scheme_bits(y2, m, r, loss=123.0, tol_rel=1e-3)[idx[0]] == S.MIN_WIDTH
