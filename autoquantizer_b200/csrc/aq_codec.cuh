@@ -84,7 +84,9 @@ __device__ __forceinline__ double uniform_f64(uint64_t pk, int s) {
 
 // ------------------------------------------------------------ bit access
 
-__device__ __forceinline__ uint64_t get_bits(const uint64_t* w, int off, int nb) {
+// w: the record's words, a pointer or a view with operator[] (GRec)
+template <class WP>
+__device__ __forceinline__ uint64_t get_bits(const WP& w, int off, int nb) {
   const int wi = off >> 6, sh = off & 63;
   uint64_t v = w[wi] >> sh;
   if (sh + nb > 64) v |= w[wi + 1] << (64 - sh);
@@ -222,12 +224,66 @@ __device__ __forceinline__ float dequant_shared(const aq_slot& S, uint32_t d_in,
   return __uint_as_float(fb | sign);
 }
 
+// ------------------------------------------------ record storage in HBM
+// The simulator keeps its records in groups of 32 (records 32 g .. 32 g + 31,
+// in the simulator's order): a group stores its words as pairs, pair j
+// (words 2j and 2j+1) of all 32 records side by side, 16 bytes per record,
+// then, for an odd word count, the last word of all 32 records, 8 bytes
+// each.  Group g starts at word 32 g W, so every pair is 16-byte aligned,
+// and a warp that reads 32 consecutive records loads each pair with one
+// coalesced access of 16-byte vectors (512 contiguous bytes, or two runs
+// when the records straddle a group boundary).  Buffers hold whole groups.
+// aq_encode, aq_decode and the words exchanged through the C ABI keep each
+// record's words contiguous, as the reference's bit_pack does.
+__host__ __device__ __forceinline__ int64_t grec_word(int64_t r, int k, int W) {
+  const int64_t base = (r >> 5) * 32 * (int64_t)W;
+  const int l = (int)(r & 31), W2 = W & ~1;
+  return k < W2 ? base + (int64_t)(k >> 1) * 64 + 2 * l + (k & 1) : base + (int64_t)W2 * 32 + l;
+}
+
+// words a grouped buffer of n records occupies
+__host__ __device__ __forceinline__ int64_t grouped_words(int64_t n, int W) { return ((n + 31) >> 5) * 32 * (int64_t)W; }
+
+// read view of record r of a grouped buffer (word index -> word)
+struct GRec {
+  const uint64_t* w;
+  int64_t r;
+  int W;
+  __device__ __forceinline__ uint64_t operator[](int k) const { return w[grec_word(r, k, W)]; }
+};
+
+// Record r's W words into rec[0, W) / from rec: the pairs as 16-byte
+// vectors.  WC: the word count when it is a compile-time constant, else 0.
+template <int WC>
+__device__ __forceinline__ void load_grec(const uint64_t* __restrict__ words, int64_t r, int W, uint64_t* rec) {
+  const int Wn = WC ? WC : W, W2 = Wn & ~1;
+  const uint64_t* g = words + (r >> 5) * 32 * (int64_t)Wn;
+  const int l = (int)(r & 31);
+#pragma unroll
+  for (int k = 0; k < W2; k += 2) {
+    const ulonglong2 v = __ldg(reinterpret_cast<const ulonglong2*>(g + (k >> 1) * 64 + 2 * l));
+    rec[k] = v.x;
+    rec[k + 1] = v.y;
+  }
+  if (Wn & 1) rec[W2] = __ldg(g + W2 * 32 + l);
+}
+
+template <int WC>
+__device__ __forceinline__ void store_grec(uint64_t* __restrict__ words, int64_t r, int W, const uint64_t* rec) {
+  const int Wn = WC ? WC : W, W2 = Wn & ~1;
+  uint64_t* g = words + (r >> 5) * 32 * (int64_t)Wn;
+  const int l = (int)(r & 31);
+#pragma unroll
+  for (int k = 0; k < W2; k += 2) *reinterpret_cast<ulonglong2*>(g + (k >> 1) * 64 + 2 * l) = make_ulonglong2(rec[k], rec[k + 1]);
+  if (Wn & 1) g[W2 * 32 + l] = rec[W2];
+}
+
 // --------------------------------------------------------------- records
 
 // Decode slots [0, NS) (predicated on n_slots) from record w; slots whose
 // bit is clear in MASK are left untouched.
-template <int NS, class R, unsigned MASK = 0xffffffffu>
-__device__ __forceinline__ void decode_record(const aq_layout& L, const uint64_t* w, R (&vals)[NS]) {
+template <int NS, class R, unsigned MASK = 0xffffffffu, class WP>
+__device__ __forceinline__ void decode_record(const aq_layout& L, const WP& w, R (&vals)[NS]) {
   const bool f64 = L.compute_f64 != 0;
 #pragma unroll
   for (int s = 0; s < NS; ++s) {
@@ -261,8 +317,8 @@ __device__ __forceinline__ void decode_record(const aq_layout& L, const uint64_t
 }
 
 // Decode one slot (runtime index).
-template <class R>
-__device__ __forceinline__ R decode_slot(const aq_layout& L, int s, const uint64_t* w) {
+template <class R, class WP>
+__device__ __forceinline__ R decode_slot(const aq_layout& L, int s, const WP& w) {
   const aq_slot& S = L.slot[s];
   const uint64_t code = get_bits(w, S.bit_offset, S.bits);
   switch (S.kind) {

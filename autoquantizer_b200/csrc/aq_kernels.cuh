@@ -12,8 +12,11 @@
 //              cell block; inside a block slot-major (the first record of
 //              every cell in cell order, then the second of every cell, ...),
 //              so that 32 consecutive records lie in 32 different cells
-//              except where a slot has fewer than 32 cells.  A particle-id
-//              array moves with the records.
+//              except where a slot has fewer than 32 cells.  Stored in
+//              groups of 32 records with their words interleaved in pairs
+//              (grec_word, aq_codec.cuh): a warp's record loads and stores
+//              are coalesced 16-byte vectors.  A particle-id array moves
+//              with the records.
 //   grids    : two dense grids of R4 nodes (m, m v), row-major: one holds
 //              the P2G sums of substep k (grid_op is applied as tiles are
 //              staged from it), the other receives the P2G of substep k+1
@@ -151,8 +154,8 @@ struct StepArgs {
 
 // Layout from the kernel parameter (nvcc build).
 struct RtLayout {
-  static constexpr bool kRegRecord = false;  // records pass through shared memory (runtime word count)
-  static constexpr int kWords = 1;
+  static constexpr bool kRegRecord = false;  // records pass through shared memory
+  static constexpr int kWords = 0;            // runtime word count
   static constexpr int kMinBlocks = 512 / AQ_CH;
   static __device__ __forceinline__ const aq_layout& get(const aq_layout& p) { return p; }
 };
@@ -595,10 +598,8 @@ __global__ void __launch_bounds__(CH, AQ_STEP_MIN_BLOCKS(R, LA)) k_step(const __
       const int64_t rec = first + 32 * u + lane;
       const bool active = 32 * u + lane < cnt;
       int32_t pid = 0;
-      if (active) {
-        const uint64_t* src = A.words + rec * W;
-#pragma unroll
-        for (int k = 0; k < W; ++k) myrec[k] = __ldg(src + k);
+      if (active) {  // grouped storage: the warp's 16-byte pair loads coalesce
+        load_grec<LA::kWords>(A.words, rec, W, myrec);
         pid = __ldg(A.pid + rec);
       }
       R vals[NS];
@@ -745,9 +746,7 @@ __global__ void __launch_bounds__(CH, AQ_STEP_MIN_BLOCKS(R, LA)) k_step(const __
         // bit_pack_assign of the new state; vals become the values a later
         // read of the record returns (input of the next P2G)
         encode_record<NS, R>(L, vals, myrec, particle_key(A.sk, pid), (const float*)0, (const double*)0);
-        uint64_t* dst = A.words + rec * W;
-#pragma unroll
-        for (int k = 0; k < W; ++k) dst[k] = myrec[k];
+        store_grec<LA::kWords>(A.words, rec, W, myrec);
       }
 
       // -------------------------------------------- range detection (opt)

@@ -35,7 +35,7 @@ __global__ void __launch_bounds__(256) k_bin(const __grid_constant__ aq_layout L
                                              int32_t* __restrict__ cell_count, unsigned* __restrict__ status) {
   const int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
   if (i >= n) return;
-  const uint64_t* w = words + i * K.W;
+  const GRec w{words, i, K.W};
   unsigned fl = 0;
   int b[3] = {0, 0, 0};
 #pragma unroll
@@ -62,10 +62,9 @@ __global__ void __launch_bounds__(256) k_bin(const __grid_constant__ aq_layout L
 // the block (in cell order), then the second record of every cell, and so
 // on.  k_step's warps take this sequence 32 records at a time, so the lanes
 // of a warp are in different cells except where a slot holds fewer than 32
-// cells.  A warp moves 32 consecutive records: it reads their words
-// (contiguous) with coalesced loads into shared memory, computes each
-// record's destination, then writes the words record by record from
-// consecutive lanes, so both sides move whole sectors.
+// cells.  A warp moves one group of 32 records (grouped storage,
+// grec_word): it reads the group's word pairs with coalesced 16-byte loads
+// and writes each record's pairs to its destination as 16-byte vectors.
 constexpr int SCATTER_T = 128;
 
 __global__ void __launch_bounds__(SCATTER_T) k_scatter(const uint64_t* __restrict__ win,
@@ -73,53 +72,43 @@ __global__ void __launch_bounds__(SCATTER_T) k_scatter(const uint64_t* __restric
                                                        int32_t* __restrict__ pout, const int32_t* __restrict__ keys,
                                                        const int32_t* __restrict__ ranks,
                                                        const int32_t* __restrict__ start, int64_t n, int W) {
-  extern __shared__ uint64_t sh_rec[];  // (SCATTER_T / 32) warps x 32 records x W words
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
-  const int64_t i0 = (int64_t)blockIdx.x * SCATTER_T + warp * 32;
-  if (i0 >= n) return;
-  const int cnt = (int)(n - i0 < 32 ? n - i0 : 32);
-  const int nw = cnt * W;
-  uint64_t* ws = sh_rec + (size_t)warp * 32 * W;
-  const uint64_t* src = win + i0 * W;
-  for (int k = lane; k < nw; k += 32) ws[k] = __ldg(src + k);
-  int64_t dst = 0;
-  int32_t p = 0;
-  if (lane < cnt) {
-    const int64_t i = i0 + lane;
-    p = __ldg(pin + i);
-    const int key = keys[i];
-    const int rk = ranks[i];  // rank of the record in its cell
-    const int64_t c0 = (int64_t)(key >> 6) * 64;
-    const int myc = key & 63;
-    // records before this one: min(count, rk) of every cell, plus one more
-    // for every earlier cell that has an rk-th record.  The block's 65
-    // offsets are read as int4 vectors (start is 256-byte aligned, c0 a
-    // multiple of 64).
-    const int4* st4 = reinterpret_cast<const int4*>(start + c0);
-    int4 v = __ldg(st4);
-    const int64_t b0 = v.x;
-    int t = 0;
+  const int64_t i0 = (int64_t)blockIdx.x * SCATTER_T + warp * 32;  // first record of a group
+  const int64_t i = i0 + lane;
+  if (i >= n) return;
+  const int32_t p = __ldg(pin + i);
+  const int key = keys[i];
+  const int rk = ranks[i];  // rank of the record in its cell
+  const int64_t c0 = (int64_t)(key >> 6) * 64;
+  const int myc = key & 63;
+  // records before this one: min(count, rk) of every cell, plus one more
+  // for every earlier cell that has an rk-th record.  The block's 65
+  // offsets are read as int4 vectors (start is 256-byte aligned, c0 a
+  // multiple of 64).
+  const int4* st4 = reinterpret_cast<const int4*>(start + c0);
+  int4 v = __ldg(st4);
+  const int64_t b0 = v.x;
+  int t = 0;
 #pragma unroll 4
-    for (int q = 0; q < 16; ++q) {
-      const int4 nv = q < 15 ? __ldg(st4 + q + 1) : make_int4(__ldg(start + c0 + 64), 0, 0, 0);
-      const int ss[5] = {v.x, v.y, v.z, v.w, nv.x};
+  for (int q = 0; q < 16; ++q) {
+    const int4 nv = q < 15 ? __ldg(st4 + q + 1) : make_int4(__ldg(start + c0 + 64), 0, 0, 0);
+    const int ss[5] = {v.x, v.y, v.z, v.w, nv.x};
 #pragma unroll
-      for (int j = 0; j < 4; ++j) {
-        const int k = 4 * q + j, nk = ss[j + 1] - ss[j];
-        t += min(nk, rk) + ((k < myc && nk > rk) ? 1 : 0);
-      }
-      v = nv;
+    for (int j = 0; j < 4; ++j) {
+      const int k = 4 * q + j, nk = ss[j + 1] - ss[j];
+      t += min(nk, rk) + ((k < myc && nk > rk) ? 1 : 0);
     }
-    dst = b0 + t;
+    v = nv;
   }
-  __syncwarp();
-  for (int b = 0; b < nw; b += 32) {  // uniform trip count: the shuffle needs every lane
-    const int k = b + lane;
-    const int r = min(k / W, 31);
-    const int64_t d = __shfl_sync(0xffffffffu, dst, r);
-    if (k < nw) wout[d * W + (k - r * W)] = ws[k];
-  }
-  if (lane < cnt) pout[dst] = p;
+  const int64_t dst = b0 + t;
+  const uint64_t* g = win + i0 * W;  // the group's words (i0 is a multiple of 32)
+  uint64_t* go = wout + (dst >> 5) * 32 * (int64_t)W;
+  const int lo = (int)(dst & 31), W2 = W & ~1;
+  for (int k = 0; k < W2; k += 2)
+    *reinterpret_cast<ulonglong2*>(go + (k >> 1) * 64 + 2 * lo) =
+        __ldg(reinterpret_cast<const ulonglong2*>(g + (k >> 1) * 64 + 2 * lane));
+  if (W & 1) go[W2 * 32 + lo] = __ldg(g + W2 * 32 + lane);
+  pout[dst] = p;
 }
 
 // One work item per occupied cell block: (block, first record, count),
@@ -180,7 +169,7 @@ __global__ void __launch_bounds__(256) k_sbin(const __grid_constant__ aq_layout 
                                               int32_t* __restrict__ iota, unsigned* __restrict__ status) {
   const int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
   if (i >= n) return;
-  const uint64_t* w = words + i * K.W;
+  const GRec w{words, i, K.W};
   unsigned fl = 0;
   int b[3] = {0, 0, 0};
 #pragma unroll
@@ -425,18 +414,26 @@ __global__ void __launch_bounds__(128) k_get_state(const __grid_constant__ aq_la
   const int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
   if (i >= n) return;
   const int ns = L.n_slots;
-  const uint64_t* w = words + i * L.n_words;
+  const GRec w{words, i, L.n_words};
   const int64_t dst = pid[i];
   for (int s = 0; s < ns; ++s) out[dst * ns + s] = (T)decode_slot<double>(L, s, w);
 }
 
-__global__ void k_words_permute(const uint64_t* __restrict__ in, const int32_t* __restrict__ pid,
-                                uint64_t* __restrict__ out, int64_t n, int W, int to_particle_order) {
+// Records from the simulator's grouped storage to contiguous records in
+// particle order (record i goes to out[pid[i]]).
+__global__ void k_words_ungroup(const uint64_t* __restrict__ in, const int32_t* __restrict__ pid,
+                                uint64_t* __restrict__ out, int64_t n, int W) {
   const int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
   if (i >= n) return;
-  const int64_t a = to_particle_order ? (int64_t)pid[i] : i;
-  const int64_t b = to_particle_order ? i : (int64_t)pid[i];
-  for (int j = 0; j < W; ++j) out[a * W + j] = in[b * W + j];
+  const int64_t a = pid[i];
+  for (int j = 0; j < W; ++j) out[a * W + j] = in[grec_word(i, j, W)];
+}
+
+// Contiguous records (record i at in[i W]) into grouped storage, same order.
+__global__ void k_words_group(const uint64_t* __restrict__ in, uint64_t* __restrict__ out, int64_t n, int W) {
+  const int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  for (int j = 0; j < W; ++j) out[grec_word(i, j, W)] = in[i * W + j];
 }
 
 __global__ void k_iota(int32_t* p, int64_t n) {
@@ -457,7 +454,7 @@ __global__ void __launch_bounds__(256) k_loss(const __grid_constant__ aq_layout 
   __shared__ double sh[8];
   double acc = 0;
   for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x) {
-    const uint64_t* w = words + i * K.W;
+    const GRec w{words, i, K.W};
     double vv = 0;
 #pragma unroll
     for (int d = 0; d < D; ++d) {
@@ -494,7 +491,7 @@ __global__ void __launch_bounds__(256) k_field_stats(const __grid_constant__ aq_
   const int s = blockIdx.y, ns = L.n_slots;
   double a[5] = {0, 0, 0, 0, 0};
   for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x) {
-    const double v = decode_slot<double>(L, s, words + i * L.n_words);
+    const double v = decode_slot<double>(L, s, GRec{words, i, L.n_words});
     const double av = fabs(v);
     a[0] += av;
     a[1] += v;
@@ -680,7 +677,7 @@ struct SimImpl final : SimBase {
     k_scan_top<<<1, SCAN_T, 0, st>>>(S_->scan_sums, nt, S_->cell_start, S_->nkeys);
     k_scan_apply<<<nt, SCAN_T, 0, st>>>(S_->cell_count, S_->nkeys, S_->scan_sums, S_->cell_start);
     const int nxt = 1 - S_->cur;
-    k_scatter<<<grid_for(n, SCATTER_T), SCATTER_T, sizeof(uint64_t) * SCATTER_T * S_->W, st>>>(S_->words[S_->cur], S_->pid[S_->cur], S_->words[nxt], S_->pid[nxt],
+    k_scatter<<<grid_for(n, SCATTER_T), SCATTER_T, 0, st>>>(S_->words[S_->cur], S_->pid[S_->cur], S_->words[nxt], S_->pid[nxt],
                                                 S_->keys, S_->ranks, S_->cell_start, n, S_->W);
     k_items_count<<<grid_for(S_->nblk, 256), 256, 0, st>>>(S_->cell_start, S_->nblk, S_->n_items);
     k_items<<<grid_for(S_->nblk, 256), 256, 0, st>>>(S_->cell_start, S_->nblk, S_->items, S_->n_items, nullptr);
@@ -744,7 +741,7 @@ struct SimImpl final : SimBase {
     k_cstart<<<grid_for(((int64_t)n_occ + 1) * 32, 256), 256, 0, st>>>(S_->ccount, S_->occ_first, S_->n_alloc + 1, n,
                                                                        S_->cstart);
     const int nxt = 1 - S_->cur;
-    k_scatter<<<grid_for(n, SCATTER_T), SCATTER_T, sizeof(uint64_t) * SCATTER_T * S_->W, st>>>(
+    k_scatter<<<grid_for(n, SCATTER_T), SCATTER_T, 0, st>>>(
         S_->words[S_->cur], S_->pid[S_->cur], S_->words[nxt], S_->pid[nxt], S_->keys, S_->ranks, S_->cstart, n, S_->W);
     AQ_CUDA_TRY(cudaMemsetAsync(S_->n_items, 0, sizeof(int32_t) * (1 + 2 * IB), st));
     k_items_count<<<grid_for(n_occ, 256), 256, 0, st>>>(S_->cstart, n_occ, S_->n_items);
@@ -1057,8 +1054,8 @@ int aq_sim_create(const aq_params* P, const aq_layout* L, aq_sim** out) {
     parts[nparts++] = Part{p, total};
     total += (bytes + 255) & ~(size_t)255;
   };
-  alloc((void**)&s->words[0], sizeof(uint64_t) * (n * s->W + 2));
-  alloc((void**)&s->words[1], sizeof(uint64_t) * (n * s->W + 2));
+  alloc((void**)&s->words[0], sizeof(uint64_t) * (grouped_words(n, s->W) + 2));
+  alloc((void**)&s->words[1], sizeof(uint64_t) * (grouped_words(n, s->W) + 2));
   alloc((void**)&s->pid[0], sizeof(int32_t) * n);
   alloc((void**)&s->pid[1], sizeof(int32_t) * n);
   alloc((void**)&s->keys, sizeof(int32_t) * n);
@@ -1122,7 +1119,7 @@ int aq_sim_create(const aq_params* P, const aq_layout* L, aq_sim** out) {
     e = cudaMemset(s->grid[0], 0, rsz * 4 * s->ncell);
     if (e == cudaSuccess) e = cudaMemset(s->grid[1], 0, rsz * 4 * s->ncell);
   }
-  if (e == cudaSuccess) e = cudaMemset(s->words[0], 0, sizeof(uint64_t) * (n * s->W + 2));
+  if (e == cudaSuccess) e = cudaMemset(s->words[0], 0, sizeof(uint64_t) * (grouped_words(n, s->W) + 2));
   if (e == cudaSuccess) e = cudaMemset(s->status, 0, sizeof(unsigned));
   if (e == cudaSuccess) e = cudaMemset(s->fallbacks, 0, sizeof(unsigned long long));
   if (e == cudaSuccess) e = cudaMemset(s->item_ctr, 0, 2 * sizeof(int32_t));
@@ -1164,10 +1161,15 @@ int aq_sim_set_state(aq_sim* s, const void* values, int32_t values_f64, void* st
   cudaStream_t st = as_stream(stream);
   k_iota<<<grid_for(s->n, 256), 256, 0, st>>>(s->pid[s->cur], s->n);
   AQ_CUDA_TRY(cudaGetLastError());
-  int rc = aq_encode(&s->L, values, values_f64, s->words[s->cur], s->n, nullptr, s->P.seed, -1, nullptr, stream);
+  // contiguous records into the other buffer, then grouped into the current
+  uint64_t* tmp = s->words[1 - s->cur];
+  int rc = aq_encode(&s->L, values, values_f64, tmp, s->n, nullptr, s->P.seed, -1, nullptr, stream);
+  if (rc != AQ_OK) return rc;
+  k_words_group<<<grid_for(s->n, 256), 256, 0, st>>>(tmp, s->words[s->cur], s->n, s->W);
+  AQ_CUDA_TRY(cudaGetLastError());
   s->sorted = false;
-  s->launches += 2;
-  return rc;
+  s->launches += 3;
+  return AQ_OK;
 }
 
 int aq_sim_get_state(aq_sim* s, void* values, int32_t values_f64, void* stream) {
@@ -1269,16 +1271,17 @@ int aq_sim_set_words(aq_sim* s, const uint64_t* words, void* stream) {
   if (!s || !words) return AQ_E_ARG;
   cudaStream_t st = as_stream(stream);
   k_iota<<<grid_for(s->n, 256), 256, 0, st>>>(s->pid[s->cur], s->n);
-  AQ_CUDA_TRY(cudaMemcpyAsync(s->words[s->cur], words, sizeof(uint64_t) * s->n * s->W, cudaMemcpyDeviceToDevice, st));
+  k_words_group<<<grid_for(s->n, 256), 256, 0, st>>>(words, s->words[s->cur], s->n, s->W);
+  AQ_CUDA_TRY(cudaGetLastError());
   s->sorted = false;
-  s->launches += 1;
+  s->launches += 2;
   return AQ_OK;
 }
 
 int aq_sim_get_words(aq_sim* s, uint64_t* words, void* stream) {
   if (!s || !words) return AQ_E_ARG;
   cudaStream_t st = as_stream(stream);
-  k_words_permute<<<grid_for(s->n, 256), 256, 0, st>>>(s->words[s->cur], s->pid[s->cur], words, s->n, s->W, 1);
+  k_words_ungroup<<<grid_for(s->n, 256), 256, 0, st>>>(s->words[s->cur], s->pid[s->cur], words, s->n, s->W);
   AQ_CUDA_TRY(cudaGetLastError());
   s->launches += 1;
   return AQ_OK;
