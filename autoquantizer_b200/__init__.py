@@ -5,7 +5,7 @@ simulator / config / quantization-scheme API on top.
 """
 from . import _lib, quant, solvers  # noqa: F401
 from .mpm_config import MPMConfig  # noqa: F401
-from .solvers import LagrangianCR, LagrangianEB  # noqa: F401
+from .solvers import LagrangianCR, LagrangianEB, ScipySolver, ScipySolverMemMode  # noqa: F401
 
 
 def MPMSolver(*args, **kwargs):
@@ -14,4 +14,5 @@ def MPMSolver(*args, **kwargs):
     return _S(*args, **kwargs)
 
 
-__all__ = ["MPMConfig", "MPMSolver", "LagrangianCR", "LagrangianEB", "quant", "solvers"]
+__all__ = ["MPMConfig", "MPMSolver", "LagrangianCR", "LagrangianEB", "ScipySolver", "ScipySolverMemMode",
+           "quant", "solvers"]

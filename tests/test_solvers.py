@@ -41,3 +41,39 @@ def test_error_model_step_gradient():
     sens = np.array([4.0, 9.0])
     g = step_gradient(sens, bits=[9, 5], ranges=[2.0, 1.0])
     assert g == pytest.approx([4.0 * (2.0 / 256) / 6, 9.0 * (1.0 / 16) / 6])
+
+
+SCIPY_GOLD = json.load(open(os.path.join(os.path.dirname(__file__), "golden", "scipy_solver.json")))
+
+
+@pytest.mark.parametrize("case", SCIPY_GOLD["cases"],
+                         ids=lambda c: "%s-%s-%g" % (c["key"].split("/")[0], c["form"], c["eps"]))
+def test_slsqp_solvers_match_reference(case):
+    """The SLSQP solvers give the reference's bit widths (and stop where it
+    stops) on the reference's shipped sensitivities and ranges."""
+    g = np.array(case["grad"])
+    n = len(g)
+    if case["form"] == "mem":
+        s = solvers.ScipySolverMemMode(n, a=[1], eps=case["eps"], grad=g)
+    else:
+        s = solvers.ScipySolver(n, a=np.ones(n), eps=case["eps"], grad=g)
+    s.set_range(case["ranges"])
+    res = s.run()
+    assert int(res.status) == case["status"]
+    assert [int(b) for b in s.get_bits()] == case["bits"]
+
+
+def test_slsqp_memory_form_meets_its_budget():
+    """Where SLSQP converges, the memory form's widths stay within the
+    budget it was given (sum of -log2(sqrt(3) x / R) <= 32 eps n, up to the
+    rounding up of each width) and spend more bits on more sensitive scalars."""
+    case = [c for c in SCIPY_GOLD["cases"] if c["form"] == "mem" and c["status"] == 0][0]
+    g = np.array(case["grad"])
+    n = len(g)
+    s = solvers.ScipySolverMemMode(n, a=[1], eps=case["eps"], grad=g)
+    s.set_range(case["ranges"])
+    assert s.run().status == 0
+    bits = np.array(s.get_bits())
+    assert bits.sum() <= 32 * case["eps"] * n + n
+    cont = -np.log2(np.sqrt(3.0) * np.abs(s.sol) / np.array(case["ranges"]))
+    assert cont.sum() == pytest.approx(32 * case["eps"] * n, rel=1e-6)
