@@ -28,6 +28,10 @@ Experiments:
   fluid_3d    run_mpm_fluid_3d.py — two fluid slabs stirred by the rotating
               SDF propeller collider (init_sdf_value; the autodiff path's
               collider schedule for -a and -r).
+  fluid_3d_scaling  run_mpm_fluid_3d_scaling.py — a fluid block (or, for
+              configurations 5 and 6, two water jets) in a walled box, from
+              one of the reference's JSON configurations (-c); scheme from
+              the SLSQP memory-budget solver.
 
 Each forward run re-seeds the dithering generator (seed = run index), which
 plays the role of the reference's per-run random state.
@@ -40,7 +44,7 @@ import sys
 import numpy as np
 
 from .mpm_config import MPMConfig
-from .solvers import LagrangianCR, LagrangianEB
+from .solvers import LagrangianCR, LagrangianEB, ScipySolverMemMode
 
 CR, EB = 0, 1
 
@@ -413,7 +417,139 @@ class Propeller3D(Experiment):
         return bits + 1, r
 
 
-EXPERIMENTS = {e.name: e for e in (Elastic2D, Fluid2D, FallingBlock3D, Letters3D, Propeller3D)}
+class Fluid3DScaling(Experiment):
+    """The 3D fluid scaling and initial-condition experiments
+    (run_mpm_fluid_3d_scaling.py): a weakly compressible fluid block (bulk
+    modulus 5e5, 2e6 for configurations 4 and 7; rho 1000) in a walled box,
+    set up from one of the reference's JSON configurations (parse_json,
+    :60-73: particle count, dt, timesteps = steps * 1024 + 1, grid, walls
+    lb / ub, id, frame length steps // 16 * 128, task 0 scaling or 1 initial
+    condition; --config), the initial blocks of init() (:222-275) and, for
+    configurations 5 and 6, two water jets emitted every 30 substeps
+    (emit_water, :126-131).  solve() (:324-346) reads the gradients of the
+    reference's 200,000-particle run and the ranges of its 5,000,000-particle
+    run and derives the scheme with the SLSQP memory-budget solver for
+    configurations 0-5, the compression-rate closed form (bits + 1) for 6
+    and 7; compression-rate mode only."""
+
+    name = "fluid_3d_scaling"
+    file_name = "fluid_3d_t16385_dt0.0002_p200000_g64.npy"
+    solve_range_file = "fluid_3d_t65537_dt5e-05_p5000000_g256.npy"
+    f64_data = 0.06709209246760206
+    modes = (CR,)
+    config_file = None
+    emit_step = 30
+    SCALING, INIT_CONDITION = 0, 1
+
+    def config(self, kind="forward"):
+        c = MPMConfig()
+        c.dim = 3
+        c.bound = [3, 3, 3]
+        c.lb = [15, 3, 3]
+        c.ub = [48, 60, 60]
+        c.use_friction = False
+        c.use_fluid = True
+        if self.config_file is not None:
+            with open(self.config_file) as f:
+                data = json.load(f)
+            c.n_particles = data["n_particles"]
+            c.dt = data["dt"]
+            c.n_timesteps = data["steps"] * 1024 + 1
+            c.n_grid = data["grids"]
+            c.lb = data["lb"]
+            c.ub = data["ub"]
+            c.id = data["id"]
+            c.steps = data["steps"] // 16 * 128
+            c.task = data.get("task", self.SCALING)
+        c.la = 2e6 if c.id in (4, 7) else 5e5
+        c.E = 5e4
+        c.p_rho = 1000.0
+        c.p_vol = (1 / c.n_grid * 0.5) ** c.dim
+        c.size = 1.0
+        c.g = 9.8
+        c.quantized_properties = {"x": 1, "v": 1, "C": 1, "J": 1}
+        c.quant_bits = np.array([32] * 16)
+        c.quant_ranges = np.array([2.0] * 16)
+        c.precision = "f64"  # ti.init(default_fp=ti.float64)
+        self.cid, self.task = c.id, c.task
+        return c
+
+    def init(self, mpm):
+        """init() (:222-275): blocks at the walls lb, sized from lb / ub."""
+        mpm.initialize()
+        c = mpm.param
+        dx = 1 / c.n_grid
+        lb, ub, n = c.lb, c.ub, c.n_particles
+        low = ((lb[0] + 0.5) * dx, (lb[1] + 0.5) * dx, (lb[2] + 0.5) * dx)
+        full = ((ub[0] - lb[0] + 1) * dx, 0.2, 0.3)
+        if self.task == self.SCALING:
+            mpm.add_cube(low, full, n)
+        elif self.task == self.INIT_CONDITION:
+            if self.cid == 0:
+                mpm.add_cube(low, ((ub[0] - lb[0] + 1) * 0.5 * dx, 0.2, 0.3), n)
+            elif self.cid == 1:
+                mpm.add_cube((((lb[0] + ub[0]) * 0.5) * dx, low[1], low[2]),
+                             ((ub[0] - lb[0] + 1) * 0.5 * dx, 0.2, 0.3), n)
+            elif self.cid == 2:
+                mpm.add_cube(low, ((ub[0] - lb[0] + 1) * dx, 0.3, 0.3), n)
+            elif self.cid == 3:
+                mpm.add_cube(low, full, n // 2)
+                mpm.add_cube((low[0], low[1], (ub[2] - 0.3 * c.n_grid - 0.5) * dx), full, n // 2)
+            elif self.cid in (4, 7):
+                mpm.add_cube(low, full, n)
+            elif self.cid not in (5, 6):  # 5 and 6 start empty: the jets fill them
+                raise ValueError("no initial condition %d" % self.cid)
+        else:
+            raise ValueError("task %r is neither scaling (0) nor initial condition (1)" % (self.task,))
+
+    def emit(self, s, mpm):
+        """The jets of configurations 5 and 6 (:126-131), at substeps that are
+        multiples of emit_step."""
+        if s % self.emit_step:
+            return
+        if self.cid == 5:
+            mpm.emit_water([0.5, 0.3, 0.2], 0.04, [0.0, 0.0, 2.0], 1000)
+            mpm.emit_water([0.5, 0.3, 0.8], 0.04, [0.0, 0.0, -2.0], 1000)
+        elif self.cid == 6:
+            mpm.emit_water([0.5, 0.3, 0.3], 0.04, [0.0, 0.0, 3.0], 1000)
+            mpm.emit_water([0.5, 0.3, 0.7], 0.04, [0.0, 0.0, -3.0], 1000)
+
+    def run_frames(self, mpm, detect=False):
+        """run_forward_only (:77-152): n_timestep - 1 substeps, the jets
+        emitted on their substeps; with detect, the range pass of
+        run_forward_detect_ranges (:292-302), which emits nothing."""
+        if detect:
+            return mpm.run_forward_detect_ranges()
+        total = mpm.n_timestep - 1
+        s = 0
+        while s < total:
+            nxt = total
+            if self.cid in (5, 6):
+                self.emit(s, mpm)
+                nxt = min(total, (s // self.emit_step + 1) * self.emit_step)
+            if mpm.current_idx > 0:
+                mpm.substeps(nxt - s)
+            s = nxt
+        return None
+
+    def scheme(self, grads, ranges, mode, eps):
+        if mode != CR:
+            raise ValueError("fluid_3d_scaling runs the compression-rate mode only")
+        ranges = np.array(ranges, dtype=np.float64)
+        ranges[:3] = 1.0
+        ranges[3:] *= 2.0
+        grads = np.asarray(grads, dtype=np.float64)
+        if self.cid < 6:
+            s = ScipySolverMemMode(len(grads), a=[1], eps=eps, grad=grads / grads.min())
+            s.set_range(ranges)
+            s.run()
+            return np.array(s.get_bits()).astype(np.int32), ranges
+        bits, _ = LagrangianCR(grads=grads * ranges ** 2, r=eps)
+        return bits + 1, ranges
+
+
+EXPERIMENTS = {e.name: e for e in (Elastic2D, Fluid2D, FallingBlock3D, Letters3D, Propeller3D,
+                                    Fluid3DScaling)}
 
 
 def _paths(exp, root):
@@ -462,6 +598,8 @@ def solve(exp, cfg, root, mode, eps):
     """The drivers' solve(): bits and ranges from the saved gradients and
     ranges, written into the config."""
     gfn, rfn = _paths(exp, root)
+    if getattr(exp, "solve_range_file", None):  # a range file of another run (fluid_3d_scaling)
+        rfn = os.path.join(os.path.dirname(rfn), exp.solve_range_file)
     grads, ranges = np.load(gfn), np.load(rfn)
     bits, ranges = exp.scheme(grads, ranges, mode, eps)
     if np.any(np.asarray(bits) < 1) or np.any(np.asarray(bits) > 32):
@@ -506,12 +644,15 @@ def main(argv=None):
     ap.add_argument("-N", "--runs", type=int, default=20)
     ap.add_argument("--root", default=".")
     ap.add_argument("--inputs", default="inputs", help="folder of the 3D experiments' meshes and collider volumes")
+    ap.add_argument("-c", "--config", default=None,
+                    help="fluid_3d_scaling: one of the reference's JSON configurations (mpm_exps/configs/...)")
     ap.add_argument("--timesteps", type=int, default=None)
     ap.add_argument("--json", action="store_true")
     args = ap.parse_args(argv)
 
     exp = EXPERIMENTS[args.experiment]()
     exp.inputs = args.inputs
+    exp.config_file = args.config
     cfg = exp.config("ad" if args.ad else "ranges" if args.ranges else "forward")
     if args.timesteps:
         cfg.n_timesteps = args.timesteps

@@ -307,3 +307,68 @@ def test_driver_loop_helpers_on_the_host():
               "theta": 0.0, "height": 0.0, "omega": 5.0, "rate": 0.1}
     s.step_collider_difftaichi(10)
     assert s.collider_state() == (pytest.approx(5.0 * cfg.dt * 10), pytest.approx(0.15 * cfg.dt * 10))
+
+
+SCIPY_GOLD = json.load(open(os.path.join(os.path.dirname(__file__), "golden", "scipy_solver.json")))
+FS = "fluid_3d_scaling/fluid_3d_t16385_dt0.0002_p200000_g64.npy"
+FS_R = "fluid_3d_scaling/fluid_3d_t65537_dt5e-05_p5000000_g256.npy"
+
+
+def _scaling_config(tmp_path, **kw):
+    data = {"id": 0, "n_particles": 200000, "dt": 2e-4, "steps": 16, "grids": 64, "lb": [15, 3, 3], "ub": [48, 60, 60]}
+    data.update(kw)
+    fn = tmp_path / "config.json"
+    fn.write_text(json.dumps(data))
+    exp = D.Fluid3DScaling()
+    exp.config_file = str(fn)
+    return exp, exp.config()
+
+
+def test_fluid_3d_scaling_reads_the_reference_config_format(tmp_path):
+    """parse_json (run_mpm_fluid_3d_scaling.py:60-73) and the driver's fixed
+    settings (:362-401)."""
+    exp, c = _scaling_config(tmp_path, id=4, task=1, steps=32, grids=128, dt=1e-4, lb=[30, 3, 3], ub=[97, 124, 124])
+    assert (c.n_timesteps, c.steps, c.n_grid, c.dt) == (32 * 1024 + 1, 32 // 16 * 128, 128, 1e-4)
+    assert c.lb == [30, 3, 3] and c.ub == [97, 124, 124]
+    assert (c.la, c.E, c.p_rho, c.size) == (2e6, 5e4, 1000.0, 1.0)
+    assert c.p_vol == pytest.approx((0.5 / 128) ** 3)
+    assert exp.task == 1 and exp.cid == 4
+    _, c0 = _scaling_config(tmp_path)
+    assert c0.la == 5e5 and c0.task == D.Fluid3DScaling.SCALING
+
+
+def test_fluid_3d_scaling_solve_matches_the_reference_slsqp_solver(tmp_path):
+    """solve() for configurations 0-5: the SLSQP memory-budget solver on the
+    shipped gradients (divided by their minimum) and ranges (positions 1,
+    the rest doubled); its widths are the reference solver's."""
+    exp, _ = _scaling_config(tmp_path)
+    g, r = np.array(GOLD["grads"][FS]), np.array(GOLD["ranges"][FS_R])
+    cases = [c for c in SCIPY_GOLD["cases"] if c["key"] == FS and c["form"] == "mem"]
+    assert cases
+    for case in cases:
+        bits, ranges = exp.scheme(g, r, D.CR, case["eps"])
+        assert bits.tolist() == case["bits"]
+        assert ranges.tolist() == case["ranges"]
+
+
+def test_fluid_3d_scaling_solve_uses_the_closed_form_for_configs_6_and_7(tmp_path):
+    exp, _ = _scaling_config(tmp_path, id=7, task=1)
+    g, r = np.array(GOLD["grads"][FS]), np.array(GOLD["ranges"][FS_R])
+    bits, ranges = exp.scheme(g, r, D.CR, 0.3)
+    ref, _ = D.LagrangianCR(g * ranges ** 2, r=0.3)
+    assert bits.tolist() == (ref + 1).tolist()
+    with pytest.raises(ValueError):
+        exp.scheme(g, r, D.EB, 0.3)
+
+
+def test_fluid_3d_scaling_solve_reads_the_fixed_range_file(tmp_path):
+    """The scaling driver's solve() reads the ranges of the 5M-particle run,
+    not those of the run the gradients come from."""
+    exp, c = _scaling_config(tmp_path)
+    os.makedirs(tmp_path / "grads" / "fluid_3d_scaling")
+    os.makedirs(tmp_path / "ranges" / "fluid_3d_scaling")
+    np.save(tmp_path / "grads" / FS, np.array(GOLD["grads"][FS]))
+    np.save(tmp_path / "ranges" / FS_R, np.array(GOLD["ranges"][FS_R]))
+    out = D.solve(exp, c, str(tmp_path), D.CR, 0.5)
+    case = [k for k in SCIPY_GOLD["cases"] if k["key"] == FS and k["form"] == "mem" and k["eps"] == 0.5][0]
+    assert out["bits"] == case["bits"]

@@ -153,3 +153,58 @@ def test_fluid_3d_ranges_match_reference_statistically(tmp_path):
     assert np.all((ratio[keep] > 0.5) & (ratio[keep] < 2.0)), ratio
     assert 1.0 < ours[4] < ref[4], (ours[4], ref[4])
     assert abs(ours[15] - ref[15]) < 0.1, (ours[15], ref[15])
+
+
+def _scaling(tmp_path, **kw):
+    data = {"id": 0, "n_particles": 20000, "dt": 2e-4, "steps": 1, "grids": 64, "lb": [15, 3, 3], "ub": [48, 60, 60]}
+    data.update(kw)
+    fn = tmp_path / ("config%d.json" % data["id"])
+    fn.write_text(json.dumps(data))
+    exp = D.Fluid3DScaling()
+    exp.config_file = str(fn)
+    return exp
+
+
+def test_fluid_3d_scaling_pipeline(tmp_path):
+    """The scaling experiment's -r and -f passes on a small configuration of
+    the reference's format (20,000 particles, 64 grid, 1025 substeps):
+    ranges of the fluid block, then the SLSQP scheme from the shipped
+    sensitivities and ranges and one quantized forward run with a clean
+    status."""
+    exp = _scaling(tmp_path)
+    out = D.detect_range(exp, exp.config("ranges"), str(tmp_path))
+    r = np.array(out["ranges"])
+    assert r.shape == (16,) and np.all(np.isfinite(r))
+    assert np.all(r[:3] == 2.0)
+    assert 0.0 < r[4] < 10.0  # max |v_y|: a 0.2-high block falls well below 10 m/s
+    assert 0.9 < r[15] < 1.5  # max |J| of a weakly compressible fluid
+    os.makedirs(tmp_path / "grads" / "fluid_3d_scaling", exist_ok=True)
+    np.save(tmp_path / "grads" / "fluid_3d_scaling" / exp.file_name,
+            np.array(GOLD["grads"]["fluid_3d_scaling/" + exp.file_name]))
+    np.save(tmp_path / "ranges" / "fluid_3d_scaling" / exp.solve_range_file,
+            np.array(GOLD["ranges"]["fluid_3d_scaling/" + exp.solve_range_file]))
+    cfg = exp.config()
+    sol = D.solve(exp, cfg, str(tmp_path), D.CR, 0.5)
+    assert 0.45 < sol["compression_rate"] < 0.55
+    loss = D.run(exp, cfg, 1)
+    assert np.all(np.isfinite(loss)) and loss[0] > 0
+
+
+def test_fluid_3d_scaling_jets_fill_the_box(tmp_path):
+    """Configurations 5 and 6 start empty and emit two jets of 1000
+    particles every 30 substeps while they fit (emit_water only adds while
+    current_idx + num < n_particles)."""
+    from autoquantizer_b200.mpm_solver import MPMSolver
+
+    exp = _scaling(tmp_path, id=6, task=1)
+    cfg = exp.config()
+    cfg.n_timesteps = 301
+    mpm = MPMSolver(cfg)
+    exp.init(mpm)
+    assert mpm.current_idx == 0
+    exp.run_frames(mpm)
+    # 9 pairs of jets, then at substep 270 one more jet: a second would reach n_particles
+    assert mpm.current_idx == 19000
+    assert mpm.status()[0] == 0
+    x = mpm.state_values()[: mpm.current_idx, :3]
+    assert np.all((x > 0) & (x < 1))
