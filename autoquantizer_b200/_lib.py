@@ -32,7 +32,8 @@ EXPORTS = [
     "aq_state_error", "aq_error_string", "aq_abi_version", "aq_sim_profile_enable", "aq_sim_profile_get",
     "aq_sim_kernel_is_jit", "aq_adjoint_create", "aq_adjoint_destroy", "aq_adjoint_forward", "aq_adjoint_backward",
     "aq_mlp_param_count", "aq_mlp_to_bf16", "aq_mlp_forward", "aq_mlp_backward", "aq_mlp_mse_grad", "aq_mlp_adam",
-    "aq_state_error_noalloc",
+    "aq_state_error_noalloc", "aq_sim_create_streamed", "aq_sim_stream_set_words", "aq_sim_stream_get_words",
+    "aq_sim_stream_chunks",
 ]
 
 
@@ -93,6 +94,10 @@ def lib():
         "aq_encode": ([C.POINTER(Layout), vp, i32, vp, i64, vp, u64, i64, vp, vp], C.c_int),
         "aq_decode": ([C.POINTER(Layout), vp, vp, i32, i64, vp], C.c_int),
         "aq_sim_create": ([C.POINTER(Params), C.POINTER(Layout), C.POINTER(vp)], C.c_int),
+        "aq_sim_create_streamed": ([C.POINTER(Params), C.POINTER(Layout), i64, C.POINTER(vp)], C.c_int),
+        "aq_sim_stream_set_words": ([vp, vp, vp], C.c_int),
+        "aq_sim_stream_get_words": ([vp, vp, vp], C.c_int),
+        "aq_sim_stream_chunks": ([vp, C.POINTER(i64), C.POINTER(i64)], C.c_int),
         "aq_sim_destroy": ([vp], C.c_int),
         "aq_sim_set_state": ([vp, vp, i32, vp], C.c_int),
         "aq_sim_get_state": ([vp, vp, i32, vp], C.c_int),

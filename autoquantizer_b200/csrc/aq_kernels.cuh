@@ -661,43 +661,57 @@ __global__ void __launch_bounds__(CH, AQ_STEP_MIN_BLOCKS(R, LA)) k_step(const __
                 Sm[d][2] += wab * Q[d];
               }
             }
-        } else {
-          if (!in_tile) ++nfall;
+        } else if (D == 2 && in_tile) {
 #pragma unroll
           for (int a = 0; a < 3; ++a)
 #pragma unroll
             for (int b = 0; b < 3; ++b) {
-              const R wab = w[a][0] * w[b][1];
+              const R weight = w[a][0] * w[b][1];
+              const R4 g = gtile[lb + a * T + b];
+              const R gv[3] = {g.y, g.z, g.w};
+              const int off[3] = {a, b, 0};
 #pragma unroll
-              for (int c = 0; c < (D == 3 ? 3 : 1); ++c) {
-                const R weight = D == 3 ? wab * w[c][2] : wab;
-                R4 g;
-                if (in_tile) {
-                  g = gtile[lb + (D == 3 ? a * G::XS + b * T + c : a * T + b)];
-                } else {
-                  const int n0 = base[0] + a, n1 = base[1] + b, n2 = D == 3 ? base[2] + c : 0;
-                  if (SP) {
-                    const int sl = K.bptr[block_of<D>(K.nb, n0, n1, n2)];
-                    g = sl >= 0 ? gin[node_in_slot<D>(sl, n0, n1, n2)] : zero4;
-                  } else {
-                    g = gin[cell_index<D>(K.res, n0, n1, n2)];
-                  }
-                  if (A.raw_in) g = grid_op_node<D, R, COL>(K, g, n0, n1, n2);
-                }
-                const R gv[3] = {g.y, g.z, g.w};
-                const int off[3] = {a, b, c};
+              for (int d = 0; d < D; ++d) {
+                const R wg = weight * gv[d];
+                nv[d] += wg;
 #pragma unroll
-                for (int d = 0; d < D; ++d) {
-                  const R wg = weight * gv[d];
-                  nv[d] += wg;
-#pragma unroll
-                  for (int e = 0; e < D; ++e) {
-                    if (off[e] == 1) Sm[d][e] += wg;
-                    if (off[e] == 2) Sm[d][e] += (R)2 * wg;
-                  }
+                for (int e = 0; e < D; ++e) {
+                  if (off[e] == 1) Sm[d][e] += wg;
+                  if (off[e] == 2) Sm[d][e] += (R)2 * wg;
                 }
               }
             }
+        } else {
+          // outside the tile (rare): the global grid, one node per iteration
+          // (a rolled loop keeps this cold path out of the instruction cache)
+          ++nfall;
+#pragma unroll 1
+          for (int k = 0; k < (D == 3 ? 27 : 9); ++k) {
+            const int a = D == 3 ? k / 9 : k / 3, b = D == 3 ? (k / 3) % 3 : k % 3, c = D == 3 ? k % 3 : 0;
+            const R wa = a == 0 ? w[0][0] : (a == 1 ? w[1][0] : w[2][0]);
+            const R wb = b == 0 ? w[0][1] : (b == 1 ? w[1][1] : w[2][1]);
+            const R wc = c == 0 ? w[0][2] : (c == 1 ? w[1][2] : w[2][2]);
+            const R wab = wa * wb;
+            const R weight = D == 3 ? wab * wc : wab;
+            const int n0 = base[0] + a, n1 = base[1] + b, n2 = D == 3 ? base[2] + c : 0;
+            R4 g;
+            if (SP) {
+              const int sl = K.bptr[block_of<D>(K.nb, n0, n1, n2)];
+              g = sl >= 0 ? gin[node_in_slot<D>(sl, n0, n1, n2)] : zero4;
+            } else {
+              g = gin[cell_index<D>(K.res, n0, n1, n2)];
+            }
+            if (A.raw_in) g = grid_op_node<D, R, COL>(K, g, n0, n1, n2);
+            const R gv[3] = {g.y, g.z, g.w};
+            const R offr[3] = {(R)a, (R)b, (R)c};
+#pragma unroll
+            for (int d = 0; d < D; ++d) {
+              const R wg = weight * gv[d];
+              nv[d] += wg;
+#pragma unroll
+              for (int e = 0; e < D; ++e) Sm[d][e] += offr[e] * wg;
+            }
+          }
         }
         // new_C = 4 inv_dx sum w g_v (off - fx)^T;  new_x = x + dt new_v
         R nC[D * D];
@@ -892,36 +906,35 @@ __global__ void __launch_bounds__(CH, AQ_STEP_MIN_BLOCKS(R, LA)) k_step(const __
                 fsl[qb] = sl;
               }
             }
+            // one node per iteration: a rolled loop keeps this cold path
+            // out of the instruction cache
+#pragma unroll 1
+            for (int k = 0; k < (D == 3 ? 27 : 9); ++k) {
+              const int a = D == 3 ? k / 9 : k / 3, b = D == 3 ? (k / 3) % 3 : k % 3, c = D == 3 ? k % 3 : 0;
+              const R wa = a == 0 ? w[0][0] : (a == 1 ? w[1][0] : w[2][0]);
+              const R wb = b == 0 ? w[0][1] : (b == 1 ? w[1][1] : w[2][1]);
+              const R wc = c == 0 ? w[0][2] : (c == 1 ? w[1][2] : w[2][2]);
+              const R weight = D == 3 ? wa * wb * wc : wa * wb;
+              R mv[3] = {0, 0, 0};
 #pragma unroll
-            for (int a = 0; a < 3; ++a)
-#pragma unroll
-              for (int b = 0; b < 3; ++b)
-#pragma unroll
-                for (int c = 0; c < (D == 3 ? 3 : 1); ++c) {
-                  const R weight = D == 3 ? w[a][0] * w[b][1] * w[c][2] : w[a][0] * w[b][1];
-                  R mv[3] = {0, 0, 0};
-#pragma unroll
-                  for (int d = 0; d < D; ++d) {
-                    R s = q[d];
-                    if (a == 1) s += Aff[d * D + 0];
-                    if (a == 2) s += (R)2 * Aff[d * D + 0];
-                    if (b == 1) s += Aff[d * D + 1];
-                    if (b == 2) s += (R)2 * Aff[d * D + 1];
-                    if (D == 3 && c == 1) s += Aff[d * D + 2];
-                    if (D == 3 && c == 2) s += (R)2 * Aff[d * D + 2];
-                    mv[d] = weight * s;
-                  }
-                  const int n0 = base[0] + a, n1 = base[1] + b, n2 = D == 3 ? base[2] + c : 0;
-                  if (SP) {
-                    const int qb = D == 3 ? ((n0 / G::BS - fb0) << 2) | ((n1 / G::BS - fb1) << 1) | (n2 / G::BS - fb2)
-                                          : ((n0 / G::BS - fb0) << 1) | (n1 / G::BS - fb1);
-                    const int sl = fsl[qb];
-                    if (sl >= 0)
-                      red_add_node(gout + node_in_slot<D>(sl, n0, n1, n2), weight * K.p_mass, mv[0], mv[1], mv[2]);
-                  } else {
-                    red_add_node(gout + cell_index<D>(K.res, n0, n1, n2), weight * K.p_mass, mv[0], mv[1], mv[2]);
-                  }
-                }
+              for (int d = 0; d < D; ++d) {
+                R s = q[d];
+                s += (R)a * Aff[d * D + 0];
+                s += (R)b * Aff[d * D + 1];
+                if (D == 3) s += (R)c * Aff[d * D + 2];
+                mv[d] = weight * s;
+              }
+              const int n0 = base[0] + a, n1 = base[1] + b, n2 = D == 3 ? base[2] + c : 0;
+              if (SP) {
+                const int qb = D == 3 ? ((n0 / G::BS - fb0) << 2) | ((n1 / G::BS - fb1) << 1) | (n2 / G::BS - fb2)
+                                      : ((n0 / G::BS - fb0) << 1) | (n1 / G::BS - fb1);
+                const int sl = fsl[qb];
+                if (sl >= 0)
+                  red_add_node(gout + node_in_slot<D>(sl, n0, n1, n2), weight * K.p_mass, mv[0], mv[1], mv[2]);
+              } else {
+                red_add_node(gout + cell_index<D>(K.res, n0, n1, n2), weight * K.p_mass, mv[0], mv[1], mv[2]);
+              }
+            }
           }
           __syncwarp();
         }

@@ -421,11 +421,12 @@ __global__ void __launch_bounds__(128) k_get_state(const __grid_constant__ aq_la
 
 // Records from the simulator's grouped storage to contiguous records in
 // particle order (record i goes to out[pid[i]]).
+// base: the id of out's first record (a streamed chunk's first particle).
 __global__ void k_words_ungroup(const uint64_t* __restrict__ in, const int32_t* __restrict__ pid,
-                                uint64_t* __restrict__ out, int64_t n, int W) {
+                                uint64_t* __restrict__ out, int64_t n, int W, int64_t base = 0) {
   const int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
   if (i >= n) return;
-  const int64_t a = pid[i];
+  const int64_t a = pid[i] - base;
   for (int j = 0; j < W; ++j) out[a * W + j] = in[grec_word(i, j, W)];
 }
 
@@ -581,6 +582,19 @@ struct aq_sim {
   int blk_bits = 1;  // bits of a grid block index (radix sort)
   void* slab = nullptr;      // the one device allocation all buffers above live in
   int ranges_on = 0;
+  // streamed (out-of-core) mode, aq_sim_create_streamed: the records of all
+  // n_total particles live in pinned host memory, chunk by chunk in the
+  // device's grouped layout (chunk c: particles c * chunk onward, its words
+  // from h_words + c * grouped_words(chunk, W), its ids from h_pid + c *
+  // chunk); every pass over the particles moves each chunk through the
+  // device buffers, where n is then that chunk's count.  chunk 0: in-core.
+  int64_t chunk = 0;
+  int64_t n_total = 0;
+  uint64_t* h_words = nullptr;
+  int32_t* h_pid = nullptr;
+  // uploads and downloads run on their own streams beside the kernels
+  cudaStream_t up_st = nullptr, down_st = nullptr;
+  cudaEvent_t ev_start = nullptr, ev_up = nullptr, ev_sorted = nullptr, ev_stepped = nullptr, ev_down = nullptr;
   int64_t step = 0;
   int last_grid = 0;  // grid[] holding the P2G sums of the latest substep
   int since_sort = 0;
@@ -792,9 +806,11 @@ struct SimImpl final : SimBase {
     return AQ_OK;
   }
 
-  int launch_step(int do_g2p, int do_p2g, void* gin, void* gout, cudaStream_t st) {
+  // clear = false: gout already holds this pass's sums of earlier chunks
+  // (streamed mode clears it once per pass)
+  int launch_step(int do_g2p, int do_p2g, void* gin, void* gout, cudaStream_t st, bool clear = true) {
     // the P2G target starts at zero (profiled as the grid pass)
-    if (do_p2g && (rc_ = clear_grid(gout, st))) return rc_;
+    if (do_p2g && clear && (rc_ = clear_grid(gout, st))) return rc_;
     aq_sim* S_ = s;
     StepArgs a;
     memset(&a, 0, sizeof(a));
@@ -860,8 +876,92 @@ struct SimImpl final : SimBase {
     return AQ_OK;
   }
 
+  // ------------------------------------------------ streamed (out-of-core)
+  int64_t n_chunks() const { return (s->n_total + s->chunk - 1) / s->chunk; }
+  int64_t chunk_count(int64_t c) const { return std::min(s->chunk, s->n_total - c * s->chunk); }
+  uint64_t* chunk_words(int64_t c) const { return s->h_words + c * grouped_words(s->chunk, s->W); }
+
+  // chunk c from host memory into the current device buffers (loss)
+  int load_chunk(int64_t c, cudaStream_t st) {
+    s->n = chunk_count(c);
+    AQ_CUDA_TRY(cudaMemcpyAsync(s->words[s->cur], chunk_words(c), sizeof(uint64_t) * grouped_words(s->n, s->W),
+                                cudaMemcpyHostToDevice, st));
+    AQ_CUDA_TRY(cudaMemcpyAsync(s->pid[s->cur], s->h_pid + c * s->chunk, sizeof(int32_t) * s->n,
+                                cudaMemcpyHostToDevice, st));
+    return AQ_OK;
+  }
+
+  // One pass of k_step over every chunk: upload, bin (the chunk's own
+  // items), step, download.  The P2G target is cleared once for the pass;
+  // all chunks add into it and read the same complete G2P source.  Kernels
+  // run on st, uploads on up_st, downloads on down_st: chunk c + 1 goes up
+  // into the buffer chunk c's binning read (free once that binning is done)
+  // while chunk c steps and comes down from the other buffer, which chunk
+  // c + 1's binning then overwrites (after that download).
+  int stream_pass(int do_g2p, int do_p2g, void* gin, void* gout, cudaStream_t st) {
+    aq_sim* S_ = s;
+    int rc;
+    if (do_p2g && (rc = clear_grid(gout, st))) return rc;
+    AQ_CUDA_TRY(cudaEventRecord(S_->ev_start, st));
+    AQ_CUDA_TRY(cudaStreamWaitEvent(S_->up_st, S_->ev_start, 0));
+    AQ_CUDA_TRY(cudaStreamWaitEvent(S_->down_st, S_->ev_start, 0));
+    const int64_t nc = n_chunks();
+    for (int64_t c = 0; c < nc; ++c) {
+      const int up = 1 - S_->cur;  // the buffer the last binning read
+      const int64_t m = chunk_count(c);
+      // (chunk 0: ev_start covers the previous pass, downloads included)
+      if (c > 0) AQ_CUDA_TRY(cudaStreamWaitEvent(S_->up_st, S_->ev_sorted, 0));
+      AQ_CUDA_TRY(cudaMemcpyAsync(S_->words[up], chunk_words(c), sizeof(uint64_t) * grouped_words(m, S_->W),
+                                  cudaMemcpyHostToDevice, S_->up_st));
+      AQ_CUDA_TRY(cudaMemcpyAsync(S_->pid[up], S_->h_pid + c * S_->chunk, sizeof(int32_t) * m,
+                                  cudaMemcpyHostToDevice, S_->up_st));
+      AQ_CUDA_TRY(cudaEventRecord(S_->ev_up, S_->up_st));
+      AQ_CUDA_TRY(cudaStreamWaitEvent(st, S_->ev_up, 0));
+      if (c > 0) AQ_CUDA_TRY(cudaStreamWaitEvent(st, S_->ev_down, 0));  // the binning's target is going down
+      S_->cur = up;
+      S_->n = m;
+      if ((rc = sort(st))) return rc;  // words[up] -> words[1 - up], cur = 1 - up
+      AQ_CUDA_TRY(cudaEventRecord(S_->ev_sorted, st));
+      if ((rc = launch_step(do_g2p, do_p2g, gin, gout, st, false))) return rc;
+      AQ_CUDA_TRY(cudaEventRecord(S_->ev_stepped, st));
+      AQ_CUDA_TRY(cudaStreamWaitEvent(S_->down_st, S_->ev_stepped, 0));
+      AQ_CUDA_TRY(cudaMemcpyAsync(chunk_words(c), S_->words[S_->cur], sizeof(uint64_t) * grouped_words(m, S_->W),
+                                  cudaMemcpyDeviceToHost, S_->down_st));
+      AQ_CUDA_TRY(cudaMemcpyAsync(S_->h_pid + c * S_->chunk, S_->pid[S_->cur], sizeof(int32_t) * m,
+                                  cudaMemcpyDeviceToHost, S_->down_st));
+      AQ_CUDA_TRY(cudaEventRecord(S_->ev_down, S_->down_st));
+    }
+    AQ_CUDA_TRY(cudaStreamWaitEvent(st, S_->ev_down, 0));  // the host store is complete when st gets here
+    return AQ_OK;
+  }
+
+  // The fused chain of substeps() over streamed chunks: a P2G pass, one
+  // fused pass per substep, a final G2P pass (n + 1 passes for n substeps);
+  // each chunk is re-binned on every pass, which costs little beside the
+  // host transfers that bound this mode.
+  int stream_substeps(int n, cudaStream_t st) {
+    aq_sim* S_ = s;
+    int rc, a = 0;
+    if ((rc = stream_pass(0, 1, nullptr, S_->grid[a], st))) return rc;
+    for (int k = 0; k < n; ++k) {
+      const int b = 1 - a;
+      if (k + 1 < n) {
+        if ((rc = stream_pass(1, 1, S_->grid[a], S_->grid[b], st))) return rc;
+        a = b;
+      } else {
+        if ((rc = stream_pass(1, 0, S_->grid[a], nullptr, st))) return rc;
+        S_->last_grid = a;
+      }
+      ++S_->step;
+      S_->col_theta += S_->col_omega * S_->P.dt;
+      S_->col_height += S_->col_rate * S_->P.dt;
+    }
+    return AQ_OK;
+  }
+
   int substeps(int n, cudaStream_t st) override {
     aq_sim* S_ = s;
+    if (S_->chunk) return stream_substeps(n, st);
     const int interval = S_->P.sort_interval < 1 ? 1 : S_->P.sort_interval;
     int rc;
     while (n > 0) {
@@ -897,8 +997,17 @@ struct SimImpl final : SimBase {
 
   int loss(double* h, cudaStream_t st) override {
     AQ_CUDA_TRY(cudaMemsetAsync(s->dloss, 0, sizeof(double), st));
-    k_loss<D, R><<<num_sms() * 4, 256, 0, st>>>(s->L, K, s->words[s->cur], s->n, s->dloss);
-    AQ_CUDA_TRY(cudaGetLastError());
+    if (s->chunk) {  // streamed: the sum over every chunk
+      for (int64_t c = 0; c < n_chunks(); ++c) {
+        int rc;
+        if ((rc = load_chunk(c, st))) return rc;
+        k_loss<D, R><<<num_sms() * 4, 256, 0, st>>>(s->L, K, s->words[s->cur], s->n, s->dloss);
+        AQ_CUDA_TRY(cudaGetLastError());
+      }
+    } else {
+      k_loss<D, R><<<num_sms() * 4, 256, 0, st>>>(s->L, K, s->words[s->cur], s->n, s->dloss);
+      AQ_CUDA_TRY(cudaGetLastError());
+    }
     AQ_CUDA_TRY(cudaMemcpyAsync(h, s->dloss, sizeof(double), cudaMemcpyDeviceToHost, st));
     AQ_CUDA_TRY(cudaStreamSynchronize(st));
     return AQ_OK;
@@ -976,6 +1085,12 @@ static void free_sim(aq_sim* s) {
     if (s->cub_tmp) cudaFree(s->cub_tmp);
   }
   if (s->slab) cudaFree(s->slab);
+  if (s->h_words) cudaFreeHost(s->h_words);
+  if (s->h_pid) cudaFreeHost(s->h_pid);
+  for (cudaEvent_t ev : {s->ev_start, s->ev_up, s->ev_sorted, s->ev_stepped, s->ev_down})
+    if (ev) cudaEventDestroy(ev);
+  if (s->up_st) cudaStreamDestroy(s->up_st);
+  if (s->down_st) cudaStreamDestroy(s->down_st);
   delete s;
 }
 
@@ -1149,6 +1264,93 @@ int aq_sim_create(const aq_params* P, const aq_layout* L, aq_sim** out) {
   return AQ_OK;
 }
 
+int aq_sim_create_streamed(const aq_params* P, const aq_layout* L, int64_t chunk, aq_sim** out) {
+  if (!P || !L || !out || chunk < 1) return AQ_E_ARG;
+  *out = nullptr;
+  if (P->sparse) return AQ_E_ARG;  // streamed chunks bin on a dense grid
+  const int64_t n_total = P->n_particles;
+  if (n_total < 1 || n_total > 0x7fffffffLL) return AQ_E_ARG;
+  if (chunk > n_total) chunk = n_total;
+  aq_params Q = *P;
+  Q.n_particles = chunk;  // the device buffers hold one chunk
+  aq_sim* s = nullptr;
+  int rc = aq_sim_create(&Q, L, &s);
+  if (rc != AQ_OK) return rc;
+  const int64_t nc = (n_total + chunk - 1) / chunk;
+  const size_t wbytes = sizeof(uint64_t) * (size_t)(nc * grouped_words(chunk, s->W));
+  cudaError_t e = cudaMallocHost((void**)&s->h_words, wbytes);
+  if (e == cudaSuccess) e = cudaMallocHost((void**)&s->h_pid, sizeof(int32_t) * (size_t)(nc * chunk));
+  if (e != cudaSuccess) {
+    set_last_cuda_error(e, "cudaMallocHost");
+    free_sim(s);
+    return AQ_E_NOMEM;
+  }
+  e = cudaStreamCreateWithFlags(&s->up_st, cudaStreamNonBlocking);
+  if (e == cudaSuccess) e = cudaStreamCreateWithFlags(&s->down_st, cudaStreamNonBlocking);
+  for (cudaEvent_t* ev : {&s->ev_start, &s->ev_up, &s->ev_sorted, &s->ev_stepped, &s->ev_down})
+    if (e == cudaSuccess) e = cudaEventCreateWithFlags(ev, cudaEventDisableTiming);
+  if (e != cudaSuccess) {
+    set_last_cuda_error(e, "cudaStreamCreate/cudaEventCreate");
+    free_sim(s);
+    return AQ_E_CUDA;
+  }
+  memset(s->h_words, 0, wbytes);
+  for (int64_t i = 0; i < n_total; ++i) s->h_pid[i] = (int32_t)i;
+  s->chunk = chunk;
+  s->n_total = n_total;
+  *out = s;
+  return AQ_OK;
+}
+
+int aq_sim_stream_set_words(aq_sim* s, const uint64_t* h_words, void* stream) {
+  if (!s || !h_words) return AQ_E_ARG;
+  if (!s->chunk) return AQ_E_STATE;
+  cudaStream_t st = as_stream(stream);
+  AQ_CUDA_TRY(cudaStreamSynchronize(st));  // no pass still reads or writes the host store
+  const int64_t nc = (s->n_total + s->chunk - 1) / s->chunk;
+  uint64_t* tmp = s->words[1 - s->cur];
+  for (int64_t c = 0; c < nc; ++c) {
+    const int64_t base = c * s->chunk, m = std::min(s->chunk, s->n_total - base);
+    AQ_CUDA_TRY(cudaMemcpyAsync(tmp, h_words + base * s->W, sizeof(uint64_t) * m * s->W, cudaMemcpyHostToDevice, st));
+    k_words_group<<<grid_for(m, 256), 256, 0, st>>>(tmp, s->words[s->cur], m, s->W);
+    AQ_CUDA_TRY(cudaGetLastError());
+    AQ_CUDA_TRY(cudaMemcpyAsync(s->h_words + c * grouped_words(s->chunk, s->W), s->words[s->cur],
+                                sizeof(uint64_t) * grouped_words(m, s->W), cudaMemcpyDeviceToHost, st));
+    for (int64_t j = 0; j < m; ++j) s->h_pid[base + j] = (int32_t)(base + j);
+    s->launches += 1;
+  }
+  AQ_CUDA_TRY(cudaStreamSynchronize(st));
+  s->sorted = false;
+  return AQ_OK;
+}
+
+int aq_sim_stream_get_words(aq_sim* s, uint64_t* h_words, void* stream) {
+  if (!s || !h_words) return AQ_E_ARG;
+  if (!s->chunk) return AQ_E_STATE;
+  cudaStream_t st = as_stream(stream);
+  const int64_t nc = (s->n_total + s->chunk - 1) / s->chunk;
+  uint64_t* tmp = s->words[1 - s->cur];
+  for (int64_t c = 0; c < nc; ++c) {
+    const int64_t base = c * s->chunk, m = std::min(s->chunk, s->n_total - base);
+    AQ_CUDA_TRY(cudaMemcpyAsync(s->words[s->cur], s->h_words + c * grouped_words(s->chunk, s->W),
+                                sizeof(uint64_t) * grouped_words(m, s->W), cudaMemcpyHostToDevice, st));
+    AQ_CUDA_TRY(cudaMemcpyAsync(s->pid[s->cur], s->h_pid + base, sizeof(int32_t) * m, cudaMemcpyHostToDevice, st));
+    k_words_ungroup<<<grid_for(m, 256), 256, 0, st>>>(s->words[s->cur], s->pid[s->cur], tmp, m, s->W, base);
+    AQ_CUDA_TRY(cudaGetLastError());
+    AQ_CUDA_TRY(cudaMemcpyAsync(h_words + base * s->W, tmp, sizeof(uint64_t) * m * s->W, cudaMemcpyDeviceToHost, st));
+    s->launches += 1;
+  }
+  AQ_CUDA_TRY(cudaStreamSynchronize(st));
+  return AQ_OK;
+}
+
+int aq_sim_stream_chunks(const aq_sim* s, int64_t* h_chunk, int64_t* h_n_total) {
+  if (!s || !h_chunk || !h_n_total) return AQ_E_ARG;
+  *h_chunk = s->chunk;
+  *h_n_total = s->chunk ? s->n_total : s->n;
+  return AQ_OK;
+}
+
 int aq_sim_destroy(aq_sim* s) {
   if (!s) return AQ_E_ARG;
   cudaDeviceSynchronize();
@@ -1158,6 +1360,7 @@ int aq_sim_destroy(aq_sim* s) {
 
 int aq_sim_set_state(aq_sim* s, const void* values, int32_t values_f64, void* stream) {
   if (!s || !values) return AQ_E_ARG;
+  if (s->chunk) return AQ_E_STATE;  // streamed: the state is in host memory
   cudaStream_t st = as_stream(stream);
   k_iota<<<grid_for(s->n, 256), 256, 0, st>>>(s->pid[s->cur], s->n);
   AQ_CUDA_TRY(cudaGetLastError());
@@ -1174,6 +1377,7 @@ int aq_sim_set_state(aq_sim* s, const void* values, int32_t values_f64, void* st
 
 int aq_sim_get_state(aq_sim* s, void* values, int32_t values_f64, void* stream) {
   if (!s || !values) return AQ_E_ARG;
+  if (s->chunk) return AQ_E_STATE;  // streamed: the state is in host memory
   cudaStream_t st = as_stream(stream);
   if (values_f64)
     k_get_state<double><<<grid_for(s->n, 128), 128, 0, st>>>(s->L, s->words[s->cur], s->pid[s->cur], (double*)values,
@@ -1250,6 +1454,7 @@ int aq_sim_collider_get(aq_sim* s, double* h_theta, double* h_height) {
 
 int aq_sim_field_stats(aq_sim* s, const void* ref, int32_t ref_f64, double* h_out, void* stream) {
   if (!s || !h_out) return AQ_E_ARG;
+  if (s->chunk) return AQ_E_STATE;  // streamed: the state is in host memory
   cudaStream_t st = as_stream(stream);
   AQ_CUDA_TRY(cudaMemsetAsync(s->dstats, 0, sizeof(double) * 5 * AQ_MAX_SLOTS, st));
   const unsigned nb = (unsigned)std::min<int64_t>(grid_for(s->n, 256), (int64_t)num_sms() * 4);
@@ -1269,6 +1474,7 @@ int aq_sim_field_stats(aq_sim* s, const void* ref, int32_t ref_f64, double* h_ou
 
 int aq_sim_set_words(aq_sim* s, const uint64_t* words, void* stream) {
   if (!s || !words) return AQ_E_ARG;
+  if (s->chunk) return AQ_E_STATE;  // streamed: the state is in host memory
   cudaStream_t st = as_stream(stream);
   k_iota<<<grid_for(s->n, 256), 256, 0, st>>>(s->pid[s->cur], s->n);
   k_words_group<<<grid_for(s->n, 256), 256, 0, st>>>(words, s->words[s->cur], s->n, s->W);
@@ -1280,6 +1486,7 @@ int aq_sim_set_words(aq_sim* s, const uint64_t* words, void* stream) {
 
 int aq_sim_get_words(aq_sim* s, uint64_t* words, void* stream) {
   if (!s || !words) return AQ_E_ARG;
+  if (s->chunk) return AQ_E_STATE;  // streamed: the state is in host memory
   cudaStream_t st = as_stream(stream);
   k_words_ungroup<<<grid_for(s->n, 256), 256, 0, st>>>(s->words[s->cur], s->pid[s->cur], words, s->n, s->W);
   AQ_CUDA_TRY(cudaGetLastError());

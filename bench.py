@@ -405,6 +405,13 @@ def run_ours(args, ws, rank, local):
     e2e_main = e2e(args.frame, max(1, args.e2e_steps))
     e2e_one = e2e(1, max(3, args.e2e_steps * 4))
 
+    # ---- streamed (out-of-core) mode: the records in pinned host memory,
+    # passed through the device in chunks every substep; the host link bounds
+    # it, so the record's bytes set the speed
+    streamed = None
+    if args.stream_steps > 0:
+        streamed = streamed_run(q, cfg32, vals, n, args.stream_steps, args.stream_parts, ws)
+
     # ---- CPU baseline (rank 0, N=1 only)
     cpu = None
     if rank == 0 and ws == 1 and not args.no_cpu:
@@ -445,12 +452,49 @@ def run_ours(args, ws, rank, local):
             "cpu_baseline": cpu,
             "e2e": e2e_main,
             "e2e_frame1": e2e_one,
+            "streamed": streamed,
             "gpu_launches": int(launches),
             "kernel_jit": q.kernel_is_jit(),
             "status": {"flags": flags, "tile_fallbacks": fallbacks},
             "clocks": ck,
         }
         print(json.dumps(line), flush=True)
+
+
+def streamed_run(q, cfg32, vals, n, steps, parts, ws):
+    """Particle-substeps/s of the streamed mode (aq_sim_create_streamed:
+    records in pinned host memory, `parts` chunks through the device per
+    pass) for the quantized record (from the quantized run's current
+    state) and the FP32-state record (the scene's initial values), timed
+    with CUDA events over `steps` substeps after two untimed ones."""
+    import torch
+
+    from autoquantizer_b200.mpm_solver import MPMSolver
+    from autoquantizer_b200.streamed import StreamedSolver
+
+    out = {"mode": "records in pinned host memory, %d chunks through the device per pass "
+                   "(aq_sim_create_streamed); every pass uploads and downloads every record and its id" % parts,
+           "chunk": n // parts, "steps": steps}
+    f = MPMSolver(cfg32)
+    f.set_particles(vals)
+    for name, sol in (("quantized", q), ("fp32_state", f)):
+        st = StreamedSolver(sol, chunk=n // parts)
+        st.substeps(2)
+        barrier(ws)
+        torch.cuda.synchronize()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record()
+        st.substeps(steps)
+        e1.record()
+        torch.cuda.synchronize()
+        v, ms_ = job_rate(n * steps, e0.elapsed_time(e1), ws)
+        rb = sol.bytes_per_particle()
+        out[name] = {"value": v, "unit": UNIT, "ms_per_step": ms_ / steps, "record_bytes": rb,
+                     "host_bytes_per_substep": 2 * (rb + 4) * n, "status_flags": st.status()[0]}
+        st.close()
+    del f
+    out["quantized_speedup"] = out["quantized"]["value"] / out["fp32_state"]["value"]
+    return out
 
 
 def cr_half_run(args, rank, vals, ref, loss64, total, K, W, ws):
@@ -556,6 +600,9 @@ def main():
     ap.add_argument("--cpu-seconds", type=float, default=15.0)
     ap.add_argument("--no-cpu", action="store_true")
     ap.add_argument("--no-cr", action="store_true", help="skip the compression-rate-0.5 scheme run")
+    ap.add_argument("--stream-steps", type=int, default=8,
+                    help="substeps timed in the streamed (out-of-core) mode; 0 skips it")
+    ap.add_argument("--stream-parts", type=int, default=4, help="chunks per pass in the streamed mode")
     ap.add_argument("--x-bound", type=float, default=1e-4, help="requested position RMS error bound")
     ap.add_argument("--loss-eps", type=float, default=1e-3, help="eps of the |loss - loss_f64| < 3 eps test")
     args = ap.parse_args()

@@ -198,6 +198,28 @@ int aq_sim_get_words(aq_sim* sim, uint64_t* d_words, void* stream);
  * P2G of substep k+1 run in one kernel. */
 int aq_sim_substeps(aq_sim* sim, int32_t n, void* stream);
 
+/* Streamed (out-of-core) simulator: the packed records of all
+ * h_params->n_particles particles live in pinned host memory that the
+ * library allocates, and every pass over the particles (aq_sim_substeps,
+ * aq_sim_loss) moves them through the device in chunks of at most `chunk`
+ * records (upload, binning of the chunk, the substep kernel, download); the
+ * grids stay on the device and collect every chunk.  For scenes whose
+ * records do not fit in device memory: device memory then holds two chunk
+ * buffers and the grids, and the host link bounds the speed, in proportion
+ * to the record bytes.  Dense grids only (sparse = 0).  Records enter and
+ * leave through aq_sim_stream_set_words / aq_sim_stream_get_words (host
+ * pointers, particle order, n x n_words); aq_sim_set_state, get_state,
+ * set_words, get_words and field_stats return AQ_E_STATE on a streamed
+ * simulator.  Results equal the in-core simulator's up to the order in which
+ * grid sums are added.  No counterpart in the reference, whose particle
+ * state is device-resident (mpm_solver.py:190-207). */
+int aq_sim_create_streamed(const aq_params* h_params, const aq_layout* h_layout, int64_t chunk, aq_sim** out);
+/* Synchronize `stream` (host copies complete on return). */
+int aq_sim_stream_set_words(aq_sim* sim, const uint64_t* h_words, void* stream);
+int aq_sim_stream_get_words(aq_sim* sim, uint64_t* h_words, void* stream);
+/* The chunk size (0: in-core) and the particle count of a simulator. */
+int aq_sim_stream_chunks(const aq_sim* sim, int64_t* h_chunk, int64_t* h_n_total);
+
 /* Mesh voxelizer of the emitters (add_mesh: voxelizer.py:53-119): voxel
  * counts of n_tris triangles (d_tris: n_tris x 9 doubles, corners a, b, c)
  * on a res[0] x res[1] x res[2] voxel grid of spacing dx into d_voxels

@@ -227,3 +227,51 @@ def test_run_forward_with_ad_nlogn_bisection_matches_segments():
         out.append((loss, np.asarray(s.get_gradients(), dtype=np.float64).ravel()))
     assert out[0][0] == pytest.approx(out[1][0], rel=1e-12)
     np.testing.assert_allclose(out[1][1], out[0][1], rtol=1e-9)
+
+
+def test_fp32_adjoint_matches_fp64_on_every_slot():
+    """The FP32 adjoint against the FP64 adjoint, which the difference tests
+    above pin, on the 3D falling block (32,768 particles, 32^3, 64 substeps,
+    checkpoints every 16), for every slot, v and C included (FP32 central
+    differences cannot resolve those).  The slots' sensitivities span 19
+    decades (x_y 3e-3, v_y 1e-8, F 1e-12..1e-14, x_x and v_x 1e-17, C
+    1e-21), and FP32 resolves the small ones only relative to the large
+    ones: the dominant slots (x, v_y) agree to 1e-2 relative, the others
+    to a factor of 4.  What the solver takes from them is a width,
+    log2(S R^2) / 2 up to constants: the error-bound scheme from the FP32
+    sensitivities is the FP64 one's within one bit in every slot."""
+    import copy
+
+    import torch
+
+    cfg, vals = scenes.falling_block_3d(n=32768, n_grid=32)
+    cfg.use_quantaichi = False
+    cfg.materials = None
+    out = {}
+    for prec in ("f32", "f64"):
+        c = copy.deepcopy(cfg)
+        c.precision = prec
+        s = MPMSolver(c)
+        ns = s.n_slots()
+        s.set_particles(vals[:, :ns])
+        adj = Adjoint(s._params())
+        s0 = torch.from_numpy(np.ascontiguousarray(vals[:, :ns])).cuda()
+        sT = adj.forward(s0, 64, 16)
+        _, sens = adj.backward(ek_seed(sT, 3, s.p_mass, s.g))
+        out[prec] = np.asarray(sens, dtype=np.float64)
+        adj.close()
+    s32, s64 = out["f32"], out["f64"]
+    print("sensitivities f64:", np.array2string(s64, precision=3))
+    print("sensitivities f32/f64:", np.array2string(s32 / s64, precision=4))
+    assert s32.shape == s64.shape == (24,)
+    assert np.all(s64 > 0) and np.all(s32 > 0)
+    dominant = [0, 1, 2, 4]
+    np.testing.assert_allclose(s32[dominant], s64[dominant], rtol=1e-2)
+    assert np.all(np.abs(np.log2(s32 / s64)) < 2.0)
+    from autoquantizer_b200.solvers import LagrangianEB
+
+    ranges = np.array([1.0] * 3 + [2.0] * 3 + [64.0] * 9 + [2.0] * 9)
+    b32, _ = LagrangianEB(s32 * ranges ** 2, ref=1.0, tol_rel=1e-3)
+    b64, _ = LagrangianEB(s64 * ranges ** 2, ref=1.0, tol_rel=1e-3)
+    print("error-bound widths f64:", b64.tolist(), "f32:", b32.tolist())
+    assert np.all(np.abs(b32 - b64) <= 1), (b32, b64)
