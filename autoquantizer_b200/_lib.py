@@ -33,7 +33,7 @@ EXPORTS = [
     "aq_sim_kernel_is_jit", "aq_adjoint_create", "aq_adjoint_destroy", "aq_adjoint_forward", "aq_adjoint_backward",
     "aq_mlp_param_count", "aq_mlp_to_bf16", "aq_mlp_forward", "aq_mlp_backward", "aq_mlp_mse_grad", "aq_mlp_adam",
     "aq_state_error_noalloc", "aq_sim_create_streamed", "aq_sim_stream_set_words", "aq_sim_stream_get_words",
-    "aq_sim_stream_chunks",
+    "aq_sim_stream_chunks", "aq_sim_set_count", "aq_sim_append", "aq_sim_count",
 ]
 
 
@@ -98,6 +98,9 @@ def lib():
         "aq_sim_stream_set_words": ([vp, vp, vp], C.c_int),
         "aq_sim_stream_get_words": ([vp, vp, vp], C.c_int),
         "aq_sim_stream_chunks": ([vp, C.POINTER(i64), C.POINTER(i64)], C.c_int),
+        "aq_sim_set_count": ([vp, i64], C.c_int),
+        "aq_sim_append": ([vp, vp, i32, i64, vp], C.c_int),
+        "aq_sim_count": ([vp, C.POINTER(i64), C.POINTER(i64)], C.c_int),
         "aq_sim_destroy": ([vp], C.c_int),
         "aq_sim_set_state": ([vp, vp, i32, vp], C.c_int),
         "aq_sim_get_state": ([vp, vp, i32, vp], C.c_int),

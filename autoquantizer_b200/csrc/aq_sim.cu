@@ -430,16 +430,19 @@ __global__ void k_words_ungroup(const uint64_t* __restrict__ in, const int32_t* 
   for (int j = 0; j < W; ++j) out[a * W + j] = in[grec_word(i, j, W)];
 }
 
-// Contiguous records (record i at in[i W]) into grouped storage, same order.
-__global__ void k_words_group(const uint64_t* __restrict__ in, uint64_t* __restrict__ out, int64_t n, int W) {
+// Contiguous records (record i at in[i W]) into grouped storage, same order,
+// from grouped position base on (appended records: base = records already
+// stored; the words of records below base are not touched).
+__global__ void k_words_group(const uint64_t* __restrict__ in, uint64_t* __restrict__ out, int64_t n, int W,
+                              int64_t base = 0) {
   const int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
   if (i >= n) return;
-  for (int j = 0; j < W; ++j) out[grec_word(i, j, W)] = in[i * W + j];
+  for (int j = 0; j < W; ++j) out[grec_word(base + i, j, W)] = in[i * W + j];
 }
 
-__global__ void k_iota(int32_t* p, int64_t n) {
+__global__ void k_iota(int32_t* p, int64_t n, int64_t base = 0) {
   const int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
-  if (i < n) p[i] = (int32_t)i;
+  if (i < n) p[i] = (int32_t)(base + i);
 }
 
 // Node masses (component 0 of the row-major m, m v grid) as float.
@@ -541,7 +544,8 @@ struct aq_sim {
   aq_params P;
   aq_layout L;
   int W = 0, WS = 0, NS = 0, D = 0;
-  int64_t n = 0;
+  int64_t n = 0;    // active records
+  int64_t cap = 0;  // records the device buffers hold (n_particles at creation)
   uint64_t* words[2] = {nullptr, nullptr};
   int32_t* pid[2] = {nullptr, nullptr};
   int cur = 0;
@@ -1128,6 +1132,7 @@ int aq_sim_create(const aq_params* P, const aq_layout* L, aq_sim** out) {
   s->WS = L->n_words | 1;  // odd shared-memory stride: conflict-free 8-byte accesses
   s->NS = ns;
   s->n = P->n_particles;
+  s->cap = P->n_particles;
   int nb[3] = {1, 1, 1};
   const int BS = D == 3 ? 4 : 8;
   s->ncell = 1;
@@ -1341,6 +1346,44 @@ int aq_sim_stream_get_words(aq_sim* s, uint64_t* h_words, void* stream) {
     s->launches += 1;
   }
   AQ_CUDA_TRY(cudaStreamSynchronize(st));
+  return AQ_OK;
+}
+
+int aq_sim_set_count(aq_sim* s, int64_t n) {
+  if (!s) return AQ_E_ARG;
+  if (s->chunk) return AQ_E_STATE;
+  if (n < 1 || n > s->cap) return AQ_E_ARG;
+  s->n = n;
+  s->sorted = false;
+  return AQ_OK;
+}
+
+int aq_sim_append(aq_sim* s, const void* values, int32_t values_f64, int64_t count, void* stream) {
+  if (!s || !values || count < 1) return AQ_E_ARG;
+  if (s->chunk) return AQ_E_STATE;
+  if (count > s->cap - s->n) return AQ_E_LIMIT;
+  cudaStream_t st = as_stream(stream);
+  const int64_t base = s->n;
+  int32_t* ids = s->pid[s->cur] + base;
+  k_iota<<<grid_for(count, 256), 256, 0, st>>>(ids, count, base);
+  AQ_CUDA_TRY(cudaGetLastError());
+  // contiguous records into the other buffer (scratch between binnings),
+  // then grouped behind the stored ones
+  uint64_t* tmp = s->words[1 - s->cur];
+  int rc = aq_encode(&s->L, values, values_f64, tmp, count, ids, s->P.seed, -1, nullptr, stream);
+  if (rc != AQ_OK) return rc;
+  k_words_group<<<grid_for(count, 256), 256, 0, st>>>(tmp, s->words[s->cur], count, s->W, base);
+  AQ_CUDA_TRY(cudaGetLastError());
+  s->n = base + count;
+  s->sorted = false;
+  s->launches += 3;
+  return AQ_OK;
+}
+
+int aq_sim_count(const aq_sim* s, int64_t* h_n, int64_t* h_cap) {
+  if (!s || !h_n || !h_cap) return AQ_E_ARG;
+  *h_n = s->chunk ? s->n_total : s->n;
+  *h_cap = s->chunk ? s->n_total : s->cap;
   return AQ_OK;
 }
 

@@ -245,24 +245,40 @@ class MPMSolver:
 
     def _append(self, x, v=None, material=0, what="add"):
         """New particles at current_idx: positions x (cnt x dim), velocity v
-        (a dim vector or cnt x dim, default 0), F = I or J = 1, C = 0."""
+        (a dim vector or cnt x dim, default 0), F = I or J = 1, C = 0.  With
+        a simulator running, they are encoded on the device behind the
+        stored records (aq_sim_append), which stay as they are, as the
+        reference's emitters write only the new particles; otherwise they
+        go into the host staging array the next simulator starts from."""
         x = np.asarray(x, dtype=np.float64).reshape(-1, self.dim)
         st, cnt = self.current_idx, len(x)
         if st + cnt > self.n_particles:
             raise ValueError("%s: %d particles exceed n_particles=%d" % (what, st + cnt, self.n_particles))
+        rows = np.zeros((cnt, self.n_slots()), dtype=np.float64)
+        a, b = self.slot_range("x")
+        rows[:, a:b] = x
+        va, vb = self.slot_range("v")
+        if v is not None:
+            rows[:, va:vb] = np.broadcast_to(np.asarray(v, dtype=np.float64), (cnt, self.dim))
+        fa, fb = self.slot_range("F" if self.has_F else "J")
+        rows[:, fa:fb] = np.eye(self.dim).ravel() if self.has_F else 1.0
+        if self.has_mat:
+            rows[:, self.slot_range("mat")[0]] = material
+        if cnt == 0:
+            return 0
+        if self._sim is not None and not self._dirty:
+            import torch
+
+            t = torch.from_numpy(rows).cuda()
+            _lib.check(_lib.lib().aq_sim_append(self._sim, C.c_void_p(t.data_ptr()), 1, cnt, _lib.stream_ptr()),
+                       "aq_sim_append")
+            torch.cuda.current_stream().synchronize()
+            self.current_idx = st + cnt
+            return cnt
         self._pull()
         h = self._staging()
         self._dev = None
-        a, b = self.slot_range("x")
-        h[st:st + cnt, a:b] = x
-        va, vb = self.slot_range("v")
-        h[st:st + cnt, va:vb] = 0.0 if v is None else np.broadcast_to(np.asarray(v, dtype=np.float64), (cnt, self.dim))
-        ca, cb = self.slot_range("C")
-        h[st:st + cnt, ca:cb] = 0.0
-        fa, fb = self.slot_range("F" if self.has_F else "J")
-        h[st:st + cnt, fa:fb] = np.eye(self.dim).ravel() if self.has_F else 1.0
-        if self.has_mat:
-            h[st:st + cnt, self.slot_range("mat")[0]] = material
+        h[st:st + cnt] = rows
         self.current_idx = st + cnt
         self._drop_sim()
         return cnt
@@ -430,10 +446,15 @@ class MPMSolver:
         if self._sim is not None and not self._dirty:
             return
         if self._sim is None:
+            # room for n_particles records (the emitters append on the
+            # device), current_idx of them active
+            P = self._params()
+            P.n_particles = max(int(self.n_particles), int(self.current_idx))
             sim = C.c_void_p()
-            _lib.check(_lib.lib().aq_sim_create(C.byref(self._params()), C.byref(self.layout()), C.byref(sim)),
-                       "aq_sim_create")
+            _lib.check(_lib.lib().aq_sim_create(C.byref(P), C.byref(self.layout()), C.byref(sim)), "aq_sim_create")
             self._sim = sim
+            if self.current_idx < P.n_particles:
+                _lib.check(_lib.lib().aq_sim_set_count(self._sim, int(self.current_idx)), "aq_sim_set_count")
             if self._col is not None:
                 self._apply_collider()
         if self._dev is not None and self._host is None:

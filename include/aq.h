@@ -198,6 +198,21 @@ int aq_sim_get_words(aq_sim* sim, uint64_t* d_words, void* stream);
  * P2G of substep k+1 run in one kernel. */
 int aq_sim_substeps(aq_sim* sim, int32_t n, void* stream);
 
+/* Particles added to a running simulator (the emitters: add_cube, add_ball,
+ * emit_water, add_mesh, the letters; mpm_solver.py:1334-1440,1562-1632, which
+ * write only the new particles' fields).  A simulator holds up to
+ * h_params->n_particles records (its capacity); aq_sim_set_count sets how
+ * many of them are active (1..capacity; records beyond are ignored), and
+ * aq_sim_append encodes `count` more particles from d_values (count x
+ * n_slots, particle ids n, n + 1, ...; dithering keyed on those ids at the
+ * initial-state step, as aq_sim_set_state draws) behind the active ones,
+ * leaving every stored record as it is.  AQ_E_LIMIT past the capacity;
+ * AQ_E_STATE on a streamed simulator.  aq_sim_count reports the active
+ * count and the capacity. */
+int aq_sim_set_count(aq_sim* sim, int64_t n);
+int aq_sim_append(aq_sim* sim, const void* d_values, int32_t values_f64, int64_t count, void* stream);
+int aq_sim_count(const aq_sim* sim, int64_t* h_n, int64_t* h_capacity);
+
 /* Streamed (out-of-core) simulator: the packed records of all
  * h_params->n_particles particles live in pinned host memory that the
  * library allocates, and every pass over the particles (aq_sim_substeps,

@@ -151,3 +151,55 @@ def test_reference_letters_on_the_gpu():
     got = np.zeros_like(mask)
     got[idx[:, 0], idx[:, 1], idx[:, 2]] = True
     assert np.array_equal(got, mask)
+
+
+def test_emission_into_a_running_simulator_leaves_stored_records_alone():
+    """Particles emitted while a simulator runs are encoded on the device
+    behind the stored records (aq_sim_append), as the reference's emitters
+    write only the new particles' fields: the stored records keep their
+    bits (re-encoding them, with dithering on, could move codes), the
+    simulator is not rebuilt, and the new particles hold the emitted values
+    to within a quantization step."""
+    cfg, vals = scenes.dam_break_2d(n=8192, n_grid=128)
+    cfg.n_particles = 12000
+    s = MPMSolver(cfg)
+    s.set_particles(vals)
+    s.substeps(5)
+    sim = s._sim.value
+    before = s.words()
+    assert s.emit_water([0.5, 0.5], 0.04, [0.0, -1.0], 1000) == 1000
+    s.add_cube((0.6, 0.6), (0.1, 0.1), 1500)
+    assert s.current_idx == 8192 + 2500
+    assert s._sim.value == sim
+    after = s.words()
+    assert after.shape == (10692, before.shape[1])
+    assert np.array_equal(after[:8192], before)
+    new = s.state_values()[8192:]
+    q = np.nan_to_num(quant_steps(s))
+    assert np.all(np.abs(new[:1000, 2:4] - [0.0, -1.0]) <= q[2:4] * 2 + 1e-6 * 2 ** 12)
+    d = np.hypot(new[:1000, 0] - 0.5, new[:1000, 1] - 0.5)
+    assert np.all(d <= 0.04 + q[0])
+    assert np.all((new[1000:, 0] >= 0.6 - q[0]) & (new[1000:, 0] <= 0.7 + q[0]))
+    s.substeps(5)
+    assert s.status()[0] == 0
+
+
+def test_appended_particles_run_like_particles_set_at_once():
+    """A run whose second half of particles was appended to the running
+    simulator matches, over 4 substeps, a run that set all of them at once
+    (f64 compute, FP32-state layout: the only difference is the order of the
+    grid sums)."""
+    cfg, vals = scenes.mixed_boxes_3d(n=20000, n_grid=32, quantized=False, precision="f64")
+    a = MPMSolver(cfg)
+    a.set_particles(vals)
+    a.substeps(4)
+    b = MPMSolver(cfg)
+    b.set_particles(vals[:12000])
+    b.substeps(0)  # starts the simulator
+    sim = b._sim.value
+    b._append(vals[12000:, :3], v=vals[12000:, 3:6], material=vals[12000:, -1])
+    b.substeps(4)
+    assert b._sim.value == sim
+    x, y = a.state_values(), b.state_values()
+    assert x.shape == y.shape == (20000, 25)
+    np.testing.assert_allclose(y, x, rtol=0, atol=1e-9 * max(1.0, np.abs(x).max()))
