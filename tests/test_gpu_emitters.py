@@ -168,11 +168,12 @@ def test_emission_into_a_running_simulator_leaves_stored_records_alone():
     sim = s._sim.value
     before = s.words()
     assert s.emit_water([0.5, 0.5], 0.04, [0.0, -1.0], 1000) == 1000
-    s.add_cube((0.6, 0.6), (0.1, 0.1), 1500)
-    assert s.current_idx == 8192 + 2500
+    s.add_cube((0.6, 0.6), (0.1, 0.1), 1500)  # 2D: a 38 x 38 lattice
+    m = s.current_idx - 8192 - 1000
+    assert m == 38 * 38
     assert s._sim.value == sim
     after = s.words()
-    assert after.shape == (10692, before.shape[1])
+    assert after.shape == (8192 + 1000 + m, before.shape[1])
     assert np.array_equal(after[:8192], before)
     new = s.state_values()[8192:]
     q = np.nan_to_num(quant_steps(s))
