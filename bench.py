@@ -366,9 +366,9 @@ def run_ours(args, ws, rank, local):
     del f
 
     # ---- a scheme derived by the analytical solver at compression rate 0.5
-    cr = None
+    cr, cfg_cr = None, None
     if not args.no_cr:
-        cr = cr_half_run(args, rank, vals, ref, loss64, total, K, W, ws)
+        cr, cfg_cr = cr_half_run(args, rank, vals, ref, loss64, total, K, W, ws)
     del d, ref
 
     # ---- end to end through the public API with host buffers: per step the
@@ -410,7 +410,7 @@ def run_ours(args, ws, rank, local):
     # it, so the record's bytes set the speed
     streamed = None
     if args.stream_steps > 0:
-        streamed = streamed_run(q, cfg32, vals, n, args.stream_steps, args.stream_parts, ws)
+        streamed = streamed_run(q, cfg32, vals, n, args.stream_steps, args.stream_parts, ws, cfg_cr)
 
     # ---- CPU baseline (rank 0, N=1 only)
     cpu = None
@@ -461,12 +461,13 @@ def run_ours(args, ws, rank, local):
         print(json.dumps(line), flush=True)
 
 
-def streamed_run(q, cfg32, vals, n, steps, parts, ws):
+def streamed_run(q, cfg32, vals, n, steps, parts, ws, cfg_cr=None):
     """Particle-substeps/s of the streamed mode (aq_sim_create_streamed:
     records in pinned host memory, `parts` chunks through the device per
     pass) for the quantized record (from the quantized run's current
-    state) and the FP32-state record (the scene's initial values), timed
-    with CUDA events over `steps` substeps after two untimed ones."""
+    state), the FP32-state record and, when given, the compression-rate-0.5
+    scheme's record (both from the scene's initial values), timed with CUDA
+    events over `steps` substeps after two untimed ones."""
     import torch
 
     from autoquantizer_b200.mpm_solver import MPMSolver
@@ -477,7 +478,12 @@ def streamed_run(q, cfg32, vals, n, steps, parts, ws):
            "chunk": n // parts, "steps": steps}
     f = MPMSolver(cfg32)
     f.set_particles(vals)
-    for name, sol in (("quantized", q), ("fp32_state", f)):
+    runs = [("quantized", q), ("fp32_state", f)]
+    if cfg_cr is not None:
+        c = MPMSolver(cfg_cr)
+        c.set_particles(vals)
+        runs.append(("cr_half_scheme", c))
+    for name, sol in runs:
         st = StreamedSolver(sol, chunk=n // parts)
         st.substeps(2)
         barrier(ws)
@@ -494,6 +500,8 @@ def streamed_run(q, cfg32, vals, n, steps, parts, ws):
         st.close()
     del f
     out["quantized_speedup"] = out["quantized"]["value"] / out["fp32_state"]["value"]
+    if cfg_cr is not None:
+        out["cr_half_speedup"] = out["cr_half_scheme"]["value"] / out["fp32_state"]["value"]
     return out
 
 
@@ -509,7 +517,7 @@ def cr_half_run(args, rank, vals, ref, loss64, total, K, W, ws):
     all elastic with the reference's 3D law at the geometric-mean E and mean
     nu of the scene's two elastic boxes.  Ranges: the FP32-state run's range
     detection over the same substeps.  Returns its throughput, compression
-    and errors against the FP64 run."""
+    and errors against the FP64 run, with the scheme's config (None if no rate fits)."""
     import torch
 
     from autoquantizer_b200 import _lib, scenes
@@ -556,7 +564,7 @@ def cr_half_run(args, rank, vals, ref, loss64, total, K, W, ws):
             chosen = (rate, bits, ranges)
             break
     if chosen is None:
-        return {"error": "no rate in [0.3, 0.5] fits six words", "bits_at_0.5": [int(b) for b in raw]}
+        return {"error": "no rate in [0.3, 0.5] fits six words", "bits_at_0.5": [int(b) for b in raw]}, None
     rate, bits, ranges = chosen
     cq, _ = scenes.mixed_boxes_3d(seed=rank)
     cq.quant_bits = np.asarray(bits)
@@ -586,7 +594,7 @@ def cr_half_run(args, rank, vals, ref, loss64, total, K, W, ws):
             "within_bound": bool(fe["x"]["rms"] <= args.x_bound and rel <= 3 * args.loss_eps),
             "status_flags": flags, "adjoint_s": t_adj,
             "sensitivities": "adjoint on a single-material stand-in (reference 3D elastic law, E %.4g, nu %.3f)"
-                             % (stand.E, stand.nu)}
+                             % (stand.E, stand.nu)}, cq
 
 
 def main():
