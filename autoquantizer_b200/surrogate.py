@@ -7,8 +7,11 @@ produces (mpm_solver.py:1093-1302), then calls the analytical solver
 weights, fp32 accumulation; libaq aq_mlp_* kernels for inference, backward
 and Adam) predicts the log10 sensitivities of 12 field groups from cheap
 statistics of a 16-substep forward window, so a scheme can be derived without
-a backward run; the adjoint (adjoint.py) produces the training labels and
-remains the fallback and the yardstick for the surrogate's error.
+a backward run; the adjoint (adjoint.py) produces the training labels,
+judges the surrogate's error, and is the fallback: derive_scheme takes the
+adjoint's sensitivities for a scene whose ensemble members disagree by more
+than a threshold (evaluate_fallback reports the trade of fallback share,
+agreement and speed-up per threshold).
 
 Field groups: x_0..2, v_0..2, rows 0..2 of C, rows 0..2 of F (J in row 0 for
 fluids); 2D scenes leave the third entries empty (masked).
@@ -357,6 +360,20 @@ class Ensemble:
         y = torch.stack([m.forward_raw(x) for m in self.members]).mean(0).cpu().numpy()
         return y * m0.y_std + m0.y_mean
 
+    def predict_spread(self, X):
+        """The members' mean and their standard deviation per group (log10
+        sensitivity units): where the networks disagree, the data did not
+        pin the prediction down, and the adjoint is the safer source."""
+        import torch
+
+        m0 = self.members[0]
+        X = np.asarray(X, dtype=np.float64)
+        x = torch.from_numpy(((X - m0.x_mean) / m0.x_std).astype(np.float32)).cuda()
+        ys = torch.stack([m.forward_raw(x) for m in self.members]).double()
+        mean = ys.mean(0).cpu().numpy() * m0.y_std + m0.y_mean
+        spread = ys.std(0, unbiased=False).cpu().numpy() * m0.y_std
+        return mean, spread
+
 
 # ----------------------------------------------------------------- schemes
 
@@ -418,6 +435,57 @@ def evaluate(mlp, X, Y, M, meta, tol_rel=1e-3, baseline=None):
     if bl:
         bl["unclamped"] = summ(base_u)
     return sur, bl
+
+
+FALLBACK_THRESHOLDS = (0.05, 0.1, 0.15, 0.2, 0.3, 0.5)
+
+
+def evaluate_fallback(pred, spread, Y, M, meta, thresholds=FALLBACK_THRESHOLDS, t_sur=None, t_adj=None,
+                      tol_rel=1e-3):
+    """The surrogate with the adjoint as fallback, on held-out scenes: a
+    scene whose ensemble spread exceeds the threshold in any present group
+    takes the adjoint's sensitivities (its widths are then the adjoint's),
+    the others the ensemble's mean.  Per threshold: the share of scenes
+    that fall back, the share of fields and of scenes within one bit of the
+    adjoint-derived storable widths and, given the two derivation times,
+    the expected speed-up over always running the adjoint,
+    t_adj / (t_sur + share * t_adj)."""
+    out = []
+    for th in thresholds:
+        fb, fields, scenes = [], [], []
+        for i in range(len(Y)):
+            m = M[i] > 0
+            back = bool(np.max(np.where(m, spread[i], 0.0)) > th)
+            b_adj = scheme_bits(Y[i], M[i], meta[i]["ranges"], meta[i]["loss"], tol_rel)
+            b = b_adj if back else scheme_bits(pred[i], M[i], meta[i]["ranges"], meta[i]["loss"], tol_rel)
+            d = np.abs(b - b_adj)[m]
+            fb.append(back)
+            fields.append(float(np.mean(d <= 1)))
+            scenes.append(float(np.all(d <= 1)))
+        row = {"threshold": th, "fallback_share": float(np.mean(fb)), "within_1_bit": float(np.mean(fields)),
+               "scenes_all_within_1_bit": float(np.mean(scenes))}
+        if t_sur is not None and t_adj is not None:
+            row["speedup_vs_adjoint"] = float(t_adj / (t_sur + row["fallback_share"] * t_adj))
+        out.append(row)
+    return out
+
+
+def derive_scheme(cfg, s0, ensemble, threshold=0.2, tol_rel=1e-3):
+    """A bit-width scheme (bits incl. sign per field group, present
+    groups) for the scene cfg with initial values s0 on the device: from the
+    ensemble's predicted sensitivities when its members agree within
+    `threshold` (log10 units) in every present group, else from the
+    adjoint's.  Returns (bits, mask, "surrogate" or "adjoint")."""
+    n = s0.shape[0]
+    st = window_stats(cfg, s0)
+    mean, spread = ensemble.predict_spread(features(cfg, st, n)[None])
+    _, mask = group_sensitivities(cfg, np.ones(st.shape[0]))
+    ranges = group_ranges(cfg, st)
+    if np.max(np.where(mask > 0, spread[0], 0.0)) <= threshold:
+        return scheme_bits(mean[0], mask, ranges, window_loss(cfg, st), tol_rel), mask, "surrogate"
+    sens, loss = adjoint_sensitivities(cfg, s0)
+    ys, mask = group_sensitivities(cfg, sens)
+    return scheme_bits(ys, mask, ranges, loss, tol_rel), mask, "adjoint"
 
 
 def timing_comparison(cfg, vals, mlp, reps=5):
@@ -490,10 +558,15 @@ def main():
     cfg, vals = random_scene(rng, args.n_max // 2, args.n_max, horizon=args.horizon)
     timing_comparison(cfg, vals, mlp, reps=1)  # warm-up (kernel compilation, allocator)
     t_sur, t_adj, b_sur, b_adj = timing_comparison(cfg, vals, mlp)
+    fallback = None
+    if isinstance(mlp, Ensemble):
+        pred, spread = mlp.predict_spread(Xte)
+        fallback = evaluate_fallback(pred, spread, Yte, Mte, mte, t_sur=t_sur, t_adj=t_adj)
     rep = {"train_scenes": args.train, "test_scenes": args.test, "horizon": args.horizon, "window": WINDOW,
            "ensemble": args.ensemble, "steps": args.steps, "min_width": MIN_WIDTH,
            "dataset_seconds": t_data, "fit_seconds": t_fit, "loss_history": hist, "surrogate": sur,
-           "baseline_mean_predictor": bl, "scheme_seconds": {"surrogate": t_sur, "adjoint": t_adj,
+           "baseline_mean_predictor": bl, "with_adjoint_fallback": fallback,
+           "scheme_seconds": {"surrogate": t_sur, "adjoint": t_adj,
                                                             "speedup": t_adj / t_sur},
            "timing_scene": {"dim": cfg.dim, "fluid": bool(cfg.use_fluid), "n": int(vals.shape[0]),
                             "bits_surrogate": b_sur.tolist(), "bits_adjoint": b_adj.tolist()}}

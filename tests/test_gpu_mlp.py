@@ -113,3 +113,30 @@ def test_ensemble_predicts_the_members_mean():
     each = [m.predict(X) for m in e.members]
     assert not np.allclose(each[0], each[1])
     assert e.predict(X) == pytest.approx(np.mean(each, axis=0), rel=1e-5, abs=1e-6)
+    mean, spread = e.predict_spread(X)
+    assert mean == pytest.approx(np.mean(each, axis=0), rel=1e-5, abs=1e-6)
+    assert spread == pytest.approx(np.std(each, axis=0), rel=1e-4, abs=1e-6)
+
+
+def test_derive_scheme_falls_back_to_the_adjoint():
+    """derive_scheme takes the ensemble's prediction when its members agree
+    within the threshold and the adjoint's sensitivities otherwise; the
+    fallback's widths are the adjoint-derived scheme's (to a bit: two
+    adjoint runs add their atomic sums in different orders)."""
+    import torch
+
+    Xtr, Ytr, Mtr, _ = SG.make_dataset(24, 11, n_min=10_000, n_max=20_000, horizon=32)
+    e = SG.Ensemble(2, seed=1)
+    e.fit(Xtr, Ytr, Mtr, steps=200, batch=16)
+    rng = np.random.default_rng(7)
+    cfg, vals = SG.random_scene(rng, 10_000, 20_000, horizon=32)
+    s0 = torch.from_numpy(vals).to("cuda", torch.float32)
+    b_fb, mask, how = SG.derive_scheme(cfg, s0, e, threshold=-1.0)
+    assert how == "adjoint"
+    sens, loss = SG.adjoint_sensitivities(cfg, s0)
+    ys, m2 = SG.group_sensitivities(cfg, sens)
+    st = SG.window_stats(cfg, s0)
+    assert np.abs(b_fb - SG.scheme_bits(ys, m2, SG.group_ranges(cfg, st), loss)).max() <= 1
+    b_sur, _, how = SG.derive_scheme(cfg, s0, e, threshold=1e9)
+    assert how == "surrogate"
+    assert b_sur.shape == b_fb.shape and np.all(b_sur[mask > 0] >= SG.MIN_WIDTH)
