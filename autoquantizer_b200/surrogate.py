@@ -9,9 +9,10 @@ and Adam) predicts the log10 sensitivities of 12 field groups from cheap
 statistics of a 16-substep forward window, so a scheme can be derived without
 a backward run; the adjoint (adjoint.py) produces the training labels,
 judges the surrogate's error, and is the fallback: derive_scheme takes the
-adjoint's sensitivities for a scene whose ensemble members disagree by more
-than a threshold (evaluate_fallback reports the trade of fallback share,
-agreement and speed-up per threshold).
+adjoint's sensitivities for a scene whose ensemble members derive widths
+that differ by more than a bit (evaluate_fallback reports the trade of
+fallback share, agreement and speed-up for that rule and for thresholds on
+the members' spread).
 
 Field groups: x_0..2, v_0..2, rows 0..2 of C, rows 0..2 of F (J in row 0 for
 fluids); 2D scenes leave the third entries empty (masked).
@@ -360,19 +361,22 @@ class Ensemble:
         y = torch.stack([m.forward_raw(x) for m in self.members]).mean(0).cpu().numpy()
         return y * m0.y_std + m0.y_mean
 
-    def predict_spread(self, X):
-        """The members' mean and their standard deviation per group (log10
-        sensitivity units): where the networks disagree, the data did not
-        pin the prediction down, and the adjoint is the safer source."""
+    def predict_members(self, X):
+        """Every member's prediction (k x n x 12, log10 sensitivities)."""
         import torch
 
         m0 = self.members[0]
         X = np.asarray(X, dtype=np.float64)
         x = torch.from_numpy(((X - m0.x_mean) / m0.x_std).astype(np.float32)).cuda()
-        ys = torch.stack([m.forward_raw(x) for m in self.members]).double()
-        mean = ys.mean(0).cpu().numpy() * m0.y_std + m0.y_mean
-        spread = ys.std(0, unbiased=False).cpu().numpy() * m0.y_std
-        return mean, spread
+        ys = torch.stack([m.forward_raw(x) for m in self.members]).double().cpu().numpy()
+        return ys * m0.y_std + m0.y_mean
+
+    def predict_spread(self, X):
+        """The members' mean and their standard deviation per group (log10
+        sensitivity units): where the networks disagree, the data did not
+        pin the prediction down, and the adjoint is the safer source."""
+        ys = self.predict_members(X)
+        return ys.mean(0), ys.std(0)
 
 
 # ----------------------------------------------------------------- schemes
@@ -437,52 +441,73 @@ def evaluate(mlp, X, Y, M, meta, tol_rel=1e-3, baseline=None):
     return sur, bl
 
 
-FALLBACK_THRESHOLDS = (0.05, 0.1, 0.15, 0.2, 0.3, 0.5)
+FALLBACK_SPREADS = (0.1, 0.2, 0.3, 0.5)
+FALLBACK_SPANS = (0, 1, 2)
 
 
-def evaluate_fallback(pred, spread, Y, M, meta, thresholds=FALLBACK_THRESHOLDS, t_sur=None, t_adj=None,
-                      tol_rel=1e-3):
-    """The surrogate with the adjoint as fallback, on held-out scenes: a
-    scene whose ensemble spread exceeds the threshold in any present group
-    takes the adjoint's sensitivities (its widths are then the adjoint's),
-    the others the ensemble's mean.  Per threshold: the share of scenes
-    that fall back, the share of fields and of scenes within one bit of the
-    adjoint-derived storable widths and, given the two derivation times,
-    the expected speed-up over always running the adjoint,
-    t_adj / (t_sur + share * t_adj)."""
+def _member_span(members_i, m_i, meta_i, tol_rel=1e-3):
+    """Largest spread, over the present groups, of the storable widths the
+    ensemble members' predictions give on their own."""
+    bs = np.array([scheme_bits(y, m_i, meta_i["ranges"], meta_i["loss"], tol_rel) for y in members_i])
+    m = m_i > 0
+    return int((bs.max(0) - bs.min(0))[m].max())
+
+
+def evaluate_fallback(members, Y, M, meta, t_sur=None, t_adj=None, spreads=FALLBACK_SPREADS,
+                      spans=FALLBACK_SPANS, tol_rel=1e-3):
+    """The surrogate with the adjoint as fallback, on held-out scenes.  A
+    scene falls back (takes the adjoint's sensitivities, hence the
+    adjoint's widths) when its ensemble is unsure; the others take the
+    members' mean.  Two rules: "spread", the members' standard deviation
+    in any present group above a threshold (log10 units); "span", the
+    storable widths the members derive on their own differing by more than
+    a number of bits in any present group.  Per rule and threshold: the
+    share of scenes that fall back, the share of fields and of scenes
+    within one bit of the adjoint-derived storable widths and, given the
+    two derivation times, the expected speed-up over always running the
+    adjoint, t_adj / (t_sur + share * t_adj).  members: k x n x 12."""
+    members = np.asarray(members)
+    pred, spread = members.mean(0), members.std(0)
+    n = len(Y)
+    b_adj = [scheme_bits(Y[i], M[i], meta[i]["ranges"], meta[i]["loss"], tol_rel) for i in range(n)]
+    b_sur = [scheme_bits(pred[i], M[i], meta[i]["ranges"], meta[i]["loss"], tol_rel) for i in range(n)]
+    span = [_member_span(members[:, i], M[i], meta[i], tol_rel) for i in range(n)]
+    sd = [float(np.max(np.where(M[i] > 0, spread[i], 0.0))) for i in range(n)]
     out = []
-    for th in thresholds:
-        fb, fields, scenes = [], [], []
-        for i in range(len(Y)):
-            m = M[i] > 0
-            back = bool(np.max(np.where(m, spread[i], 0.0)) > th)
-            b_adj = scheme_bits(Y[i], M[i], meta[i]["ranges"], meta[i]["loss"], tol_rel)
-            b = b_adj if back else scheme_bits(pred[i], M[i], meta[i]["ranges"], meta[i]["loss"], tol_rel)
-            d = np.abs(b - b_adj)[m]
-            fb.append(back)
-            fields.append(float(np.mean(d <= 1)))
-            scenes.append(float(np.all(d <= 1)))
-        row = {"threshold": th, "fallback_share": float(np.mean(fb)), "within_1_bit": float(np.mean(fields)),
-               "scenes_all_within_1_bit": float(np.mean(scenes))}
-        if t_sur is not None and t_adj is not None:
-            row["speedup_vs_adjoint"] = float(t_adj / (t_sur + row["fallback_share"] * t_adj))
-        out.append(row)
+    for rule, ths, score in (("spread", spreads, sd), ("span", spans, span)):
+        for th in ths:
+            fb, fields, scenes = [], [], []
+            for i in range(n):
+                m = M[i] > 0
+                back = score[i] > th
+                d = np.abs((b_adj[i] if back else b_sur[i]) - b_adj[i])[m]
+                fb.append(back)
+                fields.append(float(np.mean(d <= 1)))
+                scenes.append(float(np.all(d <= 1)))
+            row = {"rule": rule, "threshold": th, "fallback_share": float(np.mean(fb)),
+                   "within_1_bit": float(np.mean(fields)), "scenes_all_within_1_bit": float(np.mean(scenes))}
+            if t_sur is not None and t_adj is not None:
+                row["speedup_vs_adjoint"] = float(t_adj / (t_sur + row["fallback_share"] * t_adj))
+            out.append(row)
     return out
 
 
-def derive_scheme(cfg, s0, ensemble, threshold=0.2, tol_rel=1e-3):
+def derive_scheme(cfg, s0, ensemble, max_span=1, tol_rel=1e-3):
     """A bit-width scheme (bits incl. sign per field group, present
     groups) for the scene cfg with initial values s0 on the device: from the
-    ensemble's predicted sensitivities when its members agree within
-    `threshold` (log10 units) in every present group, else from the
-    adjoint's.  Returns (bits, mask, "surrogate" or "adjoint")."""
+    ensemble's mean prediction when the storable widths its members derive
+    on their own agree within `max_span` bits in every present group, else
+    from the adjoint's sensitivities.  Returns (bits, mask, "surrogate" or
+    "adjoint")."""
     n = s0.shape[0]
     st = window_stats(cfg, s0)
-    mean, spread = ensemble.predict_spread(features(cfg, st, n)[None])
+    members = ensemble.predict_members(features(cfg, st, n)[None])[:, 0]
     _, mask = group_sensitivities(cfg, np.ones(st.shape[0]))
     ranges = group_ranges(cfg, st)
-    if np.max(np.where(mask > 0, spread[0], 0.0)) <= threshold:
-        return scheme_bits(mean[0], mask, ranges, window_loss(cfg, st), tol_rel), mask, "surrogate"
+    loss = window_loss(cfg, st)
+    meta = {"ranges": ranges, "loss": loss}
+    if _member_span(members, mask, meta, tol_rel) <= max_span:
+        return scheme_bits(members.mean(0), mask, ranges, loss, tol_rel), mask, "surrogate"
     sens, loss = adjoint_sensitivities(cfg, s0)
     ys, mask = group_sensitivities(cfg, sens)
     return scheme_bits(ys, mask, ranges, loss, tol_rel), mask, "adjoint"
@@ -558,10 +583,11 @@ def main():
     cfg, vals = random_scene(rng, args.n_max // 2, args.n_max, horizon=args.horizon)
     timing_comparison(cfg, vals, mlp, reps=1)  # warm-up (kernel compilation, allocator)
     t_sur, t_adj, b_sur, b_adj = timing_comparison(cfg, vals, mlp)
-    fallback = None
+    fallback, held_out = None, None
     if isinstance(mlp, Ensemble):
-        pred, spread = mlp.predict_spread(Xte)
-        fallback = evaluate_fallback(pred, spread, Yte, Mte, mte, t_sur=t_sur, t_adj=t_adj)
+        members = mlp.predict_members(Xte)
+        fallback = evaluate_fallback(members, Yte, Mte, mte, t_sur=t_sur, t_adj=t_adj)
+        held_out = {"members": members.tolist(), "Y": Yte.tolist(), "M": Mte.tolist(), "meta": mte}
     rep = {"train_scenes": args.train, "test_scenes": args.test, "horizon": args.horizon, "window": WINDOW,
            "ensemble": args.ensemble, "steps": args.steps, "min_width": MIN_WIDTH,
            "dataset_seconds": t_data, "fit_seconds": t_fit, "loss_history": hist, "surrogate": sur,
@@ -569,8 +595,9 @@ def main():
            "scheme_seconds": {"surrogate": t_sur, "adjoint": t_adj,
                                                             "speedup": t_adj / t_sur},
            "timing_scene": {"dim": cfg.dim, "fluid": bool(cfg.use_fluid), "n": int(vals.shape[0]),
-                            "bits_surrogate": b_sur.tolist(), "bits_adjoint": b_adj.tolist()}}
-    print(json.dumps(rep, indent=1))
+                            "bits_surrogate": b_sur.tolist(), "bits_adjoint": b_adj.tolist()},
+           "held_out_predictions": held_out}
+    print(json.dumps({k: v for k, v in rep.items() if k != "held_out_predictions"}, indent=1))
     if args.out:
         with open(args.out, "w") as f:
             json.dump(rep, f, indent=1)

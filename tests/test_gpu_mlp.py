@@ -119,8 +119,9 @@ def test_ensemble_predicts_the_members_mean():
 
 
 def test_derive_scheme_falls_back_to_the_adjoint():
-    """derive_scheme takes the ensemble's prediction when its members agree
-    within the threshold and the adjoint's sensitivities otherwise; the
+    """derive_scheme takes the ensemble's prediction when the widths its
+    members derive agree within max_span bits and the adjoint's sensitivities
+    otherwise; the
     fallback's widths are the adjoint-derived scheme's (to a bit: two
     adjoint runs add their atomic sums in different orders)."""
     import torch
@@ -131,12 +132,12 @@ def test_derive_scheme_falls_back_to_the_adjoint():
     rng = np.random.default_rng(7)
     cfg, vals = SG.random_scene(rng, 10_000, 20_000, horizon=32)
     s0 = torch.from_numpy(vals).to("cuda", torch.float32)
-    b_fb, mask, how = SG.derive_scheme(cfg, s0, e, threshold=-1.0)
+    b_fb, mask, how = SG.derive_scheme(cfg, s0, e, max_span=-1)
     assert how == "adjoint"
     sens, loss = SG.adjoint_sensitivities(cfg, s0)
     ys, m2 = SG.group_sensitivities(cfg, sens)
     st = SG.window_stats(cfg, s0)
     assert np.abs(b_fb - SG.scheme_bits(ys, m2, SG.group_ranges(cfg, st), loss)).max() <= 1
-    b_sur, _, how = SG.derive_scheme(cfg, s0, e, threshold=1e9)
+    b_sur, _, how = SG.derive_scheme(cfg, s0, e, max_span=99)
     assert how == "surrogate"
     assert b_sur.shape == b_fb.shape and np.all(b_sur[mask > 0] >= SG.MIN_WIDTH)

@@ -87,26 +87,31 @@ def test_targets_and_scheme():
 
 
 def test_adjoint_fallback_trades_agreement_for_speed():
-    """evaluate_fallback: scenes whose ensemble spread exceeds the threshold
-    take the adjoint's widths.  With no spread allowed every scene falls
-    back (full agreement, speed-up t_adj / (t_sur + t_adj)); with any spread
-    allowed none does (the ensemble's own agreement); in between, only the
-    uncertain scenes fall back."""
+    """evaluate_fallback: scenes whose ensemble is unsure take the adjoint's
+    widths.  With no disagreement allowed every scene falls back (full
+    agreement, speed-up t_adj / (t_sur + t_adj)); with any allowed, none
+    does (the ensemble's own agreement); in between, only the uncertain
+    scenes fall back, under both rules (members' spread, members' width
+    span)."""
     rng = np.random.default_rng(0)
     n = 40
-    Y = rng.uniform(-12, -2, (n, S.N_OUT))
+    Y = rng.uniform(-2, 2, (n, S.N_OUT))  # widths of about 10 bits: none clamped to the minimum
     M = np.ones((n, S.N_OUT))
     M[:, [2, 5, 8, 11]] = 0  # 2D scenes: third entries empty
     meta = [{"ranges": [1.0] * S.N_OUT, "loss": 1.0} for _ in range(n)]
-    pred = Y.copy()
-    spread = np.full((n, S.N_OUT), 0.01)
+    members = np.stack([Y.copy() for _ in range(4)])
     bad = np.arange(n) % 4 == 0  # a quarter of the scenes: wrong by 3 decades, and the members disagree
-    pred[bad] += 3.0
-    spread[bad, 4] = 0.4
-    rows = S.evaluate_fallback(pred, spread, Y, M, meta, thresholds=(0.0, 0.2, 10.0), t_sur=1.0, t_adj=19.0)
-    assert [r["threshold"] for r in rows] == [0.0, 0.2, 10.0]
-    assert rows[0]["fallback_share"] == 1.0 and rows[0]["scenes_all_within_1_bit"] == 1.0
-    assert rows[0]["speedup_vs_adjoint"] == pytest.approx(19.0 / 20.0)
-    assert rows[1]["fallback_share"] == pytest.approx(0.25) and rows[1]["scenes_all_within_1_bit"] == 1.0
-    assert rows[1]["speedup_vs_adjoint"] == pytest.approx(19.0 / (1.0 + 0.25 * 19.0))
-    assert rows[2]["fallback_share"] == 0.0 and rows[2]["scenes_all_within_1_bit"] == pytest.approx(0.75)
+    members[:, bad] += 3.0
+    members[0, bad, 4] -= 0.8
+    members[1, bad, 4] += 0.8
+    rows = S.evaluate_fallback(members, Y, M, meta, t_sur=1.0, t_adj=19.0, spreads=(-1.0, 0.2, 10.0),
+                               spans=(-1, 1, 99))
+    sp = [r for r in rows if r["rule"] == "spread"]
+    sn = [r for r in rows if r["rule"] == "span"]
+    assert [r["threshold"] for r in sp] == [-1.0, 0.2, 10.0] and [r["threshold"] for r in sn] == [-1, 1, 99]
+    for r0, r1, r2 in (sp, sn):
+        assert r0["fallback_share"] == 1.0 and r0["scenes_all_within_1_bit"] == 1.0
+        assert r0["speedup_vs_adjoint"] == pytest.approx(19.0 / 20.0)
+        assert r1["fallback_share"] == pytest.approx(0.25) and r1["scenes_all_within_1_bit"] == 1.0
+        assert r1["speedup_vs_adjoint"] == pytest.approx(19.0 / (1.0 + 0.25 * 19.0))
+        assert r2["fallback_share"] == 0.0 and r2["scenes_all_within_1_bit"] == pytest.approx(0.75)
