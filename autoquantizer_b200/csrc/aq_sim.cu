@@ -902,19 +902,25 @@ struct SimImpl final : SimBase {
   // into the buffer chunk c's binning read (free once that binning is done)
   // while chunk c steps and comes down from the other buffer, which chunk
   // c + 1's binning then overwrites (after that download).
-  int stream_pass(int do_g2p, int do_p2g, void* gin, void* gout, cudaStream_t st) {
+  // chained: the previous pass of the same chain ran just before; its
+  // last binning is all that the first upload must wait for (with more than
+  // one chunk, the first chunk's host words came down long before), so that
+  // upload overlaps the previous pass's last step and download.
+  int stream_pass(int do_g2p, int do_p2g, void* gin, void* gout, cudaStream_t st, bool chained = false) {
     aq_sim* S_ = s;
     int rc;
+    const int64_t nc = n_chunks();
+    const bool early = chained && nc > 1;
     if (do_p2g && (rc = clear_grid(gout, st))) return rc;
     AQ_CUDA_TRY(cudaEventRecord(S_->ev_start, st));
-    AQ_CUDA_TRY(cudaStreamWaitEvent(S_->up_st, S_->ev_start, 0));
+    if (!early) AQ_CUDA_TRY(cudaStreamWaitEvent(S_->up_st, S_->ev_start, 0));
     AQ_CUDA_TRY(cudaStreamWaitEvent(S_->down_st, S_->ev_start, 0));
-    const int64_t nc = n_chunks();
     for (int64_t c = 0; c < nc; ++c) {
       const int up = 1 - S_->cur;  // the buffer the last binning read
       const int64_t m = chunk_count(c);
-      // (chunk 0: ev_start covers the previous pass, downloads included)
-      if (c > 0) AQ_CUDA_TRY(cudaStreamWaitEvent(S_->up_st, S_->ev_sorted, 0));
+      // (chunk 0: ev_start covers the previous pass, downloads included, or,
+      // chained, ev_sorted of its last binning)
+      if (c > 0 || early) AQ_CUDA_TRY(cudaStreamWaitEvent(S_->up_st, S_->ev_sorted, 0));
       AQ_CUDA_TRY(cudaMemcpyAsync(S_->words[up], chunk_words(c), sizeof(uint64_t) * grouped_words(m, S_->W),
                                   cudaMemcpyHostToDevice, S_->up_st));
       AQ_CUDA_TRY(cudaMemcpyAsync(S_->pid[up], S_->h_pid + c * S_->chunk, sizeof(int32_t) * m,
@@ -950,10 +956,10 @@ struct SimImpl final : SimBase {
     for (int k = 0; k < n; ++k) {
       const int b = 1 - a;
       if (k + 1 < n) {
-        if ((rc = stream_pass(1, 1, S_->grid[a], S_->grid[b], st))) return rc;
+        if ((rc = stream_pass(1, 1, S_->grid[a], S_->grid[b], st, true))) return rc;
         a = b;
       } else {
-        if ((rc = stream_pass(1, 0, S_->grid[a], nullptr, st))) return rc;
+        if ((rc = stream_pass(1, 0, S_->grid[a], nullptr, st, true))) return rc;
         S_->last_grid = a;
       }
       ++S_->step;
