@@ -8,7 +8,7 @@ weights, fp32 accumulation; libaq aq_mlp_* kernels for inference, backward
 and Adam) predicts the log10 sensitivities of 12 field groups from cheap
 statistics of a 16-substep forward window, so a scheme can be derived without
 a backward run; the adjoint (adjoint.py) produces the training labels,
-judges the surrogate's error, and is the fallback: derive_scheme takes the
+measures the surrogate's error, and is the fallback: derive_scheme takes the
 adjoint's sensitivities for a scene whose ensemble members derive widths
 that differ by more than a bit (evaluate_fallback reports the trade of
 fallback share, agreement and speed-up for that rule and for thresholds on
