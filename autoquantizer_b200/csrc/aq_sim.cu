@@ -19,6 +19,7 @@
 #include <cub/device/device_scan.cuh>
 #include <new>
 #include <string>
+#include <vector>
 
 #include "aq_common.cuh"
 #include "aq_jit.h"
@@ -440,6 +441,17 @@ __global__ void k_words_group(const uint64_t* __restrict__ in, uint64_t* __restr
   for (int j = 0; j < W; ++j) out[grec_word(base + i, j, W)] = in[i * W + j];
 }
 
+// Grouped records back to the order of their ids (record i to grouped
+// position pid[i] - base): a streamed chunk from its binned order to
+// particle order.
+__global__ void k_words_unpermute(const uint64_t* __restrict__ in, const int32_t* __restrict__ pid,
+                                  uint64_t* __restrict__ out, int64_t n, int W, int64_t base) {
+  const int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  const int64_t a = pid[i] - base;
+  for (int j = 0; j < W; ++j) out[grec_word(a, j, W)] = in[grec_word(i, j, W)];
+}
+
 __global__ void k_iota(int32_t* p, int64_t n, int64_t base = 0) {
   const int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
   if (i < n) p[i] = (int32_t)(base + i);
@@ -536,6 +548,7 @@ struct SimBase {
   virtual size_t smem_bytes(bool reg_record) const = 0;
   virtual void set_collider(const aq_sim* sim) = 0;
   virtual int setup_kernel(bool col) = 0;
+  virtual int load_chunk(int64_t c, cudaStream_t st) = 0;
 };
 
 }  // namespace aq
@@ -587,18 +600,20 @@ struct aq_sim {
   void* slab = nullptr;      // the one device allocation all buffers above live in
   int ranges_on = 0;
   // streamed (out-of-core) mode, aq_sim_create_streamed: the records of all
-  // n_total particles live in pinned host memory, chunk by chunk in the
-  // device's grouped layout (chunk c: particles c * chunk onward, its words
-  // from h_words + c * grouped_words(chunk, W), its ids from h_pid + c *
-  // chunk); every pass over the particles moves each chunk through the
-  // device buffers, where n is then that chunk's count.  chunk 0: in-core.
+  // n_total particles live in pinned host memory, chunk c (particles
+  // c * chunk onward) from h_words + c * grouped_words(chunk, W), in particle
+  // order in the device's grouped layout, so particle ids never cross the
+  // link; every pass over the particles moves each chunk through the device
+  // buffers, where n is then that chunk's count.  words_dl: the chunk put
+  // back in particle order for its download.  chunk 0: in-core.
   int64_t chunk = 0;
   int64_t n_total = 0;
   uint64_t* h_words = nullptr;
-  int32_t* h_pid = nullptr;
+  uint64_t* words_dl = nullptr;
   // uploads and downloads run on their own streams beside the kernels
   cudaStream_t up_st = nullptr, down_st = nullptr;
-  cudaEvent_t ev_start = nullptr, ev_up = nullptr, ev_sorted = nullptr, ev_stepped = nullptr, ev_down = nullptr;
+  cudaEvent_t ev_start = nullptr, ev_up = nullptr, ev_sorted = nullptr, ev_ready = nullptr, ev_down = nullptr;
+  std::vector<cudaEvent_t> ev_chunk_down;  // per chunk: its last download (its host words are final)
   int64_t step = 0;
   int last_grid = 0;  // grid[] holding the P2G sums of the latest substep
   int since_sort = 0;
@@ -885,63 +900,74 @@ struct SimImpl final : SimBase {
   int64_t chunk_count(int64_t c) const { return std::min(s->chunk, s->n_total - c * s->chunk); }
   uint64_t* chunk_words(int64_t c) const { return s->h_words + c * grouped_words(s->chunk, s->W); }
 
-  // chunk c from host memory into the current device buffers (loss)
-  int load_chunk(int64_t c, cudaStream_t st) {
+  // chunk c from host memory into the current device buffers, ids set to
+  // its particles' (particle order); the loss and aq_sim_stream_get_words
+  int load_chunk(int64_t c, cudaStream_t st) override {
     s->n = chunk_count(c);
     AQ_CUDA_TRY(cudaMemcpyAsync(s->words[s->cur], chunk_words(c), sizeof(uint64_t) * grouped_words(s->n, s->W),
                                 cudaMemcpyHostToDevice, st));
-    AQ_CUDA_TRY(cudaMemcpyAsync(s->pid[s->cur], s->h_pid + c * s->chunk, sizeof(int32_t) * s->n,
-                                cudaMemcpyHostToDevice, st));
+    k_iota<<<grid_for(s->n, 256), 256, 0, st>>>(s->pid[s->cur], s->n, c * s->chunk);
+    AQ_CUDA_TRY(cudaGetLastError());
     return AQ_OK;
   }
 
-  // One pass of k_step over every chunk: upload, bin (the chunk's own
-  // items), step, download.  The P2G target is cleared once for the pass;
-  // all chunks add into it and read the same complete G2P source.  Kernels
-  // run on st, uploads on up_st, downloads on down_st: chunk c + 1 goes up
-  // into the buffer chunk c's binning read (free once that binning is done)
-  // while chunk c steps and comes down from the other buffer, which chunk
-  // c + 1's binning then overwrites (after that download).
-  // chained: the previous pass of the same chain ran just before; its
-  // last binning is all that the first upload must wait for (with more than
-  // one chunk, the first chunk's host words came down long before), so that
-  // upload overlaps the previous pass's last step and download.
-  int stream_pass(int do_g2p, int do_p2g, void* gin, void* gout, cudaStream_t st, bool chained = false) {
+  // One pass of k_step over every chunk: upload (particle order), bin (the
+  // chunk's own items), step, put back in particle order, download.  The
+  // P2G target is cleared once for the pass; all chunks add into it and
+  // read the same complete G2P source.  Kernels run on st, uploads on
+  // up_st, downloads on down_st, over three buffers: chunk c + 1 goes up
+  // into the buffer chunk c's binning read, its binning writes the buffer
+  // chunk c stepped in (after chunk c was put back in order from it), and
+  // chunk c comes down from words_dl, which chunk c + 1's put-back waits
+  // for; so the uploads, the kernels and the downloads of neighbouring
+  // chunks overlap.
+  // chained: the previous pass of the same chain ran just before: the first
+  // upload waits only for its last binning and its own chunk's download
+  // (done by then unless there are fewer than three chunks), so it overlaps
+  // that pass's last step and download.  last: the chain ends
+  // with this pass, whose downloads st then waits for (within a chain only
+  // the next put-back waits for them).
+  int stream_pass(int do_g2p, int do_p2g, void* gin, void* gout, cudaStream_t st, bool chained, bool last) {
     aq_sim* S_ = s;
     int rc;
     const int64_t nc = n_chunks();
-    const bool early = chained && nc > 1;
+    const bool early = chained;
     if (do_p2g && (rc = clear_grid(gout, st))) return rc;
     AQ_CUDA_TRY(cudaEventRecord(S_->ev_start, st));
     if (!early) AQ_CUDA_TRY(cudaStreamWaitEvent(S_->up_st, S_->ev_start, 0));
     AQ_CUDA_TRY(cudaStreamWaitEvent(S_->down_st, S_->ev_start, 0));
     for (int64_t c = 0; c < nc; ++c) {
       const int up = 1 - S_->cur;  // the buffer the last binning read
-      const int64_t m = chunk_count(c);
-      // (chunk 0: ev_start covers the previous pass, downloads included, or,
-      // chained, ev_sorted of its last binning)
+      const int64_t m = chunk_count(c), base = c * S_->chunk;
+      // the buffer: free once the last binning read it (chunk 0 of a pass
+      // that is not chained: ev_start); the host words: final once the
+      // chunk's own download of the previous pass is done
       if (c > 0 || early) AQ_CUDA_TRY(cudaStreamWaitEvent(S_->up_st, S_->ev_sorted, 0));
+      AQ_CUDA_TRY(cudaStreamWaitEvent(S_->up_st, S_->ev_chunk_down[c], 0));
       AQ_CUDA_TRY(cudaMemcpyAsync(S_->words[up], chunk_words(c), sizeof(uint64_t) * grouped_words(m, S_->W),
                                   cudaMemcpyHostToDevice, S_->up_st));
-      AQ_CUDA_TRY(cudaMemcpyAsync(S_->pid[up], S_->h_pid + c * S_->chunk, sizeof(int32_t) * m,
-                                  cudaMemcpyHostToDevice, S_->up_st));
       AQ_CUDA_TRY(cudaEventRecord(S_->ev_up, S_->up_st));
+      k_iota<<<grid_for(m, 256), 256, 0, st>>>(S_->pid[up], m, base);
+      AQ_CUDA_TRY(cudaGetLastError());
       AQ_CUDA_TRY(cudaStreamWaitEvent(st, S_->ev_up, 0));
-      if (c > 0) AQ_CUDA_TRY(cudaStreamWaitEvent(st, S_->ev_down, 0));  // the binning's target is going down
       S_->cur = up;
       S_->n = m;
       if ((rc = sort(st))) return rc;  // words[up] -> words[1 - up], cur = 1 - up
       AQ_CUDA_TRY(cudaEventRecord(S_->ev_sorted, st));
       if ((rc = launch_step(do_g2p, do_p2g, gin, gout, st, false))) return rc;
-      AQ_CUDA_TRY(cudaEventRecord(S_->ev_stepped, st));
-      AQ_CUDA_TRY(cudaStreamWaitEvent(S_->down_st, S_->ev_stepped, 0));
-      AQ_CUDA_TRY(cudaMemcpyAsync(chunk_words(c), S_->words[S_->cur], sizeof(uint64_t) * grouped_words(m, S_->W),
-                                  cudaMemcpyDeviceToHost, S_->down_st));
-      AQ_CUDA_TRY(cudaMemcpyAsync(S_->h_pid + c * S_->chunk, S_->pid[S_->cur], sizeof(int32_t) * m,
+      AQ_CUDA_TRY(cudaStreamWaitEvent(st, S_->ev_down, 0));  // words_dl may still be going down
+      k_words_unpermute<<<grid_for(m, 256), 256, 0, st>>>(S_->words[S_->cur], S_->pid[S_->cur], S_->words_dl, m,
+                                                          S_->W, base);
+      AQ_CUDA_TRY(cudaGetLastError());
+      S_->launches += 2;
+      AQ_CUDA_TRY(cudaEventRecord(S_->ev_ready, st));
+      AQ_CUDA_TRY(cudaStreamWaitEvent(S_->down_st, S_->ev_ready, 0));
+      AQ_CUDA_TRY(cudaMemcpyAsync(chunk_words(c), S_->words_dl, sizeof(uint64_t) * grouped_words(m, S_->W),
                                   cudaMemcpyDeviceToHost, S_->down_st));
       AQ_CUDA_TRY(cudaEventRecord(S_->ev_down, S_->down_st));
+      AQ_CUDA_TRY(cudaEventRecord(S_->ev_chunk_down[c], S_->down_st));
     }
-    AQ_CUDA_TRY(cudaStreamWaitEvent(st, S_->ev_down, 0));  // the host store is complete when st gets here
+    if (last) AQ_CUDA_TRY(cudaStreamWaitEvent(st, S_->ev_down, 0));  // the host store is complete when st gets here
     return AQ_OK;
   }
 
@@ -952,14 +978,14 @@ struct SimImpl final : SimBase {
   int stream_substeps(int n, cudaStream_t st) {
     aq_sim* S_ = s;
     int rc, a = 0;
-    if ((rc = stream_pass(0, 1, nullptr, S_->grid[a], st))) return rc;
+    if ((rc = stream_pass(0, 1, nullptr, S_->grid[a], st, false, false))) return rc;
     for (int k = 0; k < n; ++k) {
       const int b = 1 - a;
       if (k + 1 < n) {
-        if ((rc = stream_pass(1, 1, S_->grid[a], S_->grid[b], st, true))) return rc;
+        if ((rc = stream_pass(1, 1, S_->grid[a], S_->grid[b], st, true, false))) return rc;
         a = b;
       } else {
-        if ((rc = stream_pass(1, 0, S_->grid[a], nullptr, st, true))) return rc;
+        if ((rc = stream_pass(1, 0, S_->grid[a], nullptr, st, true, true))) return rc;
         S_->last_grid = a;
       }
       ++S_->step;
@@ -1096,8 +1122,10 @@ static void free_sim(aq_sim* s) {
   }
   if (s->slab) cudaFree(s->slab);
   if (s->h_words) cudaFreeHost(s->h_words);
-  if (s->h_pid) cudaFreeHost(s->h_pid);
-  for (cudaEvent_t ev : {s->ev_start, s->ev_up, s->ev_sorted, s->ev_stepped, s->ev_down})
+  if (s->words_dl) cudaFree(s->words_dl);
+  for (cudaEvent_t ev : {s->ev_start, s->ev_up, s->ev_sorted, s->ev_ready, s->ev_down})
+    if (ev) cudaEventDestroy(ev);
+  for (cudaEvent_t ev : s->ev_chunk_down)
     if (ev) cudaEventDestroy(ev);
   if (s->up_st) cudaStreamDestroy(s->up_st);
   if (s->down_st) cudaStreamDestroy(s->down_st);
@@ -1290,23 +1318,30 @@ int aq_sim_create_streamed(const aq_params* P, const aq_layout* L, int64_t chunk
   const int64_t nc = (n_total + chunk - 1) / chunk;
   const size_t wbytes = sizeof(uint64_t) * (size_t)(nc * grouped_words(chunk, s->W));
   cudaError_t e = cudaMallocHost((void**)&s->h_words, wbytes);
-  if (e == cudaSuccess) e = cudaMallocHost((void**)&s->h_pid, sizeof(int32_t) * (size_t)(nc * chunk));
   if (e != cudaSuccess) {
     set_last_cuda_error(e, "cudaMallocHost");
     free_sim(s);
     return AQ_E_NOMEM;
   }
+  e = cudaMalloc((void**)&s->words_dl, sizeof(uint64_t) * (size_t)(grouped_words(chunk, s->W) + 2));
+  if (e != cudaSuccess) {
+    set_last_cuda_error(e, "cudaMalloc");
+    free_sim(s);
+    return AQ_E_NOMEM;
+  }
   e = cudaStreamCreateWithFlags(&s->up_st, cudaStreamNonBlocking);
   if (e == cudaSuccess) e = cudaStreamCreateWithFlags(&s->down_st, cudaStreamNonBlocking);
-  for (cudaEvent_t* ev : {&s->ev_start, &s->ev_up, &s->ev_sorted, &s->ev_stepped, &s->ev_down})
+  for (cudaEvent_t* ev : {&s->ev_start, &s->ev_up, &s->ev_sorted, &s->ev_ready, &s->ev_down})
     if (e == cudaSuccess) e = cudaEventCreateWithFlags(ev, cudaEventDisableTiming);
+  s->ev_chunk_down.assign((size_t)nc, nullptr);
+  for (int64_t c = 0; c < nc && e == cudaSuccess; ++c)
+    e = cudaEventCreateWithFlags(&s->ev_chunk_down[c], cudaEventDisableTiming);
   if (e != cudaSuccess) {
     set_last_cuda_error(e, "cudaStreamCreate/cudaEventCreate");
     free_sim(s);
     return AQ_E_CUDA;
   }
   memset(s->h_words, 0, wbytes);
-  for (int64_t i = 0; i < n_total; ++i) s->h_pid[i] = (int32_t)i;
   s->chunk = chunk;
   s->n_total = n_total;
   *out = s;
@@ -1327,7 +1362,6 @@ int aq_sim_stream_set_words(aq_sim* s, const uint64_t* h_words, void* stream) {
     AQ_CUDA_TRY(cudaGetLastError());
     AQ_CUDA_TRY(cudaMemcpyAsync(s->h_words + c * grouped_words(s->chunk, s->W), s->words[s->cur],
                                 sizeof(uint64_t) * grouped_words(m, s->W), cudaMemcpyDeviceToHost, st));
-    for (int64_t j = 0; j < m; ++j) s->h_pid[base + j] = (int32_t)(base + j);
     s->launches += 1;
   }
   AQ_CUDA_TRY(cudaStreamSynchronize(st));
@@ -1343,9 +1377,8 @@ int aq_sim_stream_get_words(aq_sim* s, uint64_t* h_words, void* stream) {
   uint64_t* tmp = s->words[1 - s->cur];
   for (int64_t c = 0; c < nc; ++c) {
     const int64_t base = c * s->chunk, m = std::min(s->chunk, s->n_total - base);
-    AQ_CUDA_TRY(cudaMemcpyAsync(s->words[s->cur], s->h_words + c * grouped_words(s->chunk, s->W),
-                                sizeof(uint64_t) * grouped_words(m, s->W), cudaMemcpyHostToDevice, st));
-    AQ_CUDA_TRY(cudaMemcpyAsync(s->pid[s->cur], s->h_pid + base, sizeof(int32_t) * m, cudaMemcpyHostToDevice, st));
+    int rc;
+    if ((rc = s->impl->load_chunk(c, st))) return rc;  // particle order, ids base, base + 1, ...
     k_words_ungroup<<<grid_for(m, 256), 256, 0, st>>>(s->words[s->cur], s->pid[s->cur], tmp, m, s->W, base);
     AQ_CUDA_TRY(cudaGetLastError());
     AQ_CUDA_TRY(cudaMemcpyAsync(h_words + base * s->W, tmp, sizeof(uint64_t) * m * s->W, cudaMemcpyDeviceToHost, st));

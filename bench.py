@@ -486,7 +486,7 @@ def streamed_run(q, cfg32, vals, n, steps, parts, ws, cfg_cr=None):
     from autoquantizer_b200.streamed import StreamedSolver
 
     out = {"mode": "records in pinned host memory, %d chunks through the device per pass "
-                   "(aq_sim_create_streamed); every pass uploads and downloads every record and its id" % parts,
+                   "(aq_sim_create_streamed); every pass uploads and downloads every record" % parts,
            "chunk": n // parts, "steps": steps}
     f = MPMSolver(cfg32)
     f.set_particles(vals)
@@ -508,7 +508,7 @@ def streamed_run(q, cfg32, vals, n, steps, parts, ws, cfg_cr=None):
         v, ms_ = job_rate(n * steps, e0.elapsed_time(e1), ws)
         rb = sol.bytes_per_particle()
         out[name] = {"value": v, "unit": UNIT, "ms_per_step": ms_ / steps, "record_bytes": rb,
-                     "host_bytes_per_substep": 2 * (rb + 4) * n, "status_flags": st.status()[0]}
+                     "host_bytes_per_substep": 2 * rb * n, "status_flags": st.status()[0]}
         st.close()
     del f
     out["quantized_speedup"] = out["quantized"]["value"] / out["fp32_state"]["value"]

@@ -219,9 +219,10 @@ int aq_sim_count(const aq_sim* sim, int64_t* h_n, int64_t* h_capacity);
  * aq_sim_loss) moves them through the device in chunks of at most `chunk`
  * records (upload, binning of the chunk, the substep kernel, download); the
  * grids stay on the device and collect every chunk.  For scenes whose
- * records do not fit in device memory: device memory then holds two chunk
- * buffers and the grids, and the host link bounds the speed, in proportion
- * to the record bytes.  Dense grids only (sparse = 0).  Records enter and
+ * records do not fit in device memory: device memory then holds three
+ * chunk buffers and the grids, and the host link bounds the speed, in
+ * proportion to the record bytes (the host keeps each chunk in particle
+ * order, so no particle ids cross the link).  Dense grids only (sparse = 0).  Records enter and
  * leave through aq_sim_stream_set_words / aq_sim_stream_get_words (host
  * pointers, particle order, n x n_words); aq_sim_set_state, get_state,
  * set_words, get_words and field_stats return AQ_E_STATE on a streamed

@@ -49,11 +49,13 @@ def test_words_round_trip_through_host_chunks():
     st.close()
 
 
-def test_streamed_quantized_2d_matches_in_core():
-    """The quantized, dithered 2D dam break (8,192 particles, 128^2) in three
-    chunks of 3,000 records, 4 substeps after 8 in-core ones."""
+@pytest.mark.parametrize("chunk", [3000, 4096, 8192])
+def test_streamed_quantized_2d_matches_in_core(chunk):
+    """The quantized, dithered 2D dam break (8,192 particles, 128^2) in
+    three, two or one chunks, 4 substeps after 8 in-core ones (the passes
+    of a chain overlap whatever the chunk count)."""
     cfg, vals = scenes.dam_break_2d(n=8192, n_grid=128)
-    s, st = _pair(cfg, vals, chunk=3000, warm=8)
+    s, st = _pair(cfg, vals, chunk=chunk, warm=8)
     assert st.step_count() == s.step_count() == 8
     s.substeps(4)
     st.substeps(4)
