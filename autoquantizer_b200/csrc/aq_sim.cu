@@ -912,7 +912,8 @@ struct SimImpl final : SimBase {
   }
 
   // One pass of k_step over every chunk: upload (particle order), bin (the
-  // chunk's own items), step, put back in particle order, download.  The
+  // chunk's own items), step, put back in particle order, download (not
+  // after a P2G-only step, which changes no record).  The
   // P2G target is cleared once for the pass; all chunks add into it and
   // read the same complete G2P source.  Kernels run on st, uploads on
   // up_st, downloads on down_st, over three buffers: chunk c + 1 goes up
@@ -949,17 +950,19 @@ struct SimImpl final : SimBase {
       AQ_CUDA_TRY(cudaEventRecord(S_->ev_up, S_->up_st));
       k_iota<<<grid_for(m, 256), 256, 0, st>>>(S_->pid[up], m, base);
       AQ_CUDA_TRY(cudaGetLastError());
+      S_->launches += 1;
       AQ_CUDA_TRY(cudaStreamWaitEvent(st, S_->ev_up, 0));
       S_->cur = up;
       S_->n = m;
       if ((rc = sort(st))) return rc;  // words[up] -> words[1 - up], cur = 1 - up
       AQ_CUDA_TRY(cudaEventRecord(S_->ev_sorted, st));
       if ((rc = launch_step(do_g2p, do_p2g, gin, gout, st, false))) return rc;
+      if (!do_g2p) continue;  // a P2G-only pass leaves the records as they are: nothing to take down
       AQ_CUDA_TRY(cudaStreamWaitEvent(st, S_->ev_down, 0));  // words_dl may still be going down
       k_words_unpermute<<<grid_for(m, 256), 256, 0, st>>>(S_->words[S_->cur], S_->pid[S_->cur], S_->words_dl, m,
                                                           S_->W, base);
       AQ_CUDA_TRY(cudaGetLastError());
-      S_->launches += 2;
+      S_->launches += 1;
       AQ_CUDA_TRY(cudaEventRecord(S_->ev_ready, st));
       AQ_CUDA_TRY(cudaStreamWaitEvent(S_->down_st, S_->ev_ready, 0));
       AQ_CUDA_TRY(cudaMemcpyAsync(chunk_words(c), S_->words_dl, sizeof(uint64_t) * grouped_words(m, S_->W),

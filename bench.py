@@ -622,7 +622,7 @@ def main():
     ap.add_argument("--no-cr", action="store_true", help="skip the compression-rate-0.5 scheme run")
     ap.add_argument("--reference-budget-s", type=float, default=90.0,
                     help="--impl reference: the whole scene if warm-up + timed substeps fit this many seconds")
-    ap.add_argument("--stream-steps", type=int, default=8,
+    ap.add_argument("--stream-steps", type=int, default=16,
                     help="substeps timed in the streamed (out-of-core) mode; 0 skips it")
     ap.add_argument("--stream-parts", type=int, default=4, help="chunks per pass in the streamed mode")
     ap.add_argument("--x-bound", type=float, default=1e-4, help="requested position RMS error bound")
