@@ -24,6 +24,33 @@ import numpy as np
 from . import _lib
 
 
+def encode_values(solver, batch):
+    """The packed records (n x n_words, particle order) of a solver's
+    particle values as it holds them before a simulator runs (host staging
+    array or device tensor), encoded on the device `batch` particles at a
+    time with the codes a simulator's aq_sim_set_state gives them
+    (dithering keyed on the particle ids at the initial-state step)."""
+    import torch
+
+    L = solver.layout()
+    n, W = int(solver.current_idx), L.n_words
+    out = np.empty((n, W), dtype=np.uint64)
+    dev = solver._dev if (solver._dev is not None and solver._host is None) else None
+    for a in range(0, n, batch):
+        b = min(n, a + batch)
+        if dev is not None:
+            v = dev[a:b].to(torch.float64).contiguous()
+        else:
+            v = torch.from_numpy(np.ascontiguousarray(solver._staging()[a:b])).cuda()
+        ids = torch.arange(a, b, dtype=torch.int32, device="cuda")
+        w = torch.empty((b - a, W), dtype=torch.int64, device="cuda")
+        _lib.check(_lib.lib().aq_encode(C.byref(L), C.c_void_p(v.data_ptr()), 1, C.c_void_p(w.data_ptr()), b - a,
+                                        C.c_void_p(ids.data_ptr()), int(solver.param.seed), -1, None,
+                                        _lib.stream_ptr()), "aq_encode")
+        out[a:b] = w.cpu().numpy().view(np.uint64)
+    return out
+
+
 class StreamedSolver:
     """A streamed copy of `solver`'s scene: its parameters, record layout,
     current records and substep count (the dithering generator's step
@@ -34,7 +61,10 @@ class StreamedSolver:
             raise ValueError("StreamedSolver: the SDF collider is not streamed")
         if getattr(solver.param, "sparse_grid", False):
             raise ValueError("StreamedSolver: streamed chunks bin on a dense grid")
-        words = solver.words()
+        if solver._sim is not None and not solver._dirty:
+            words = solver.words()  # a running simulator: its current records
+        else:  # no simulator (a scene set up but not run): encode chunk by chunk, none in device memory whole
+            words = encode_values(solver, chunk)
         step = solver.step_count()
         self.dim = solver.dim
         self.n_particles = int(solver.current_idx)

@@ -39,8 +39,13 @@ def _pair(cfg, vals, chunk, warm=0):
 
 
 def test_words_round_trip_through_host_chunks():
+    """A scene set up but not run is encoded chunk by chunk, with no
+    in-core simulator, to the codes the in-core simulator gives it
+    (dithered layout: the draws are keyed on the same particle ids), and
+    records go through the host chunks and back unchanged."""
     cfg, vals = scenes.dam_break_2d(n=5000, n_grid=64)
     s, st = _pair(cfg, vals, chunk=1234)
+    assert s._sim is None
     assert st.chunks() == (1234, 5000)
     w = s.words()
     assert np.array_equal(st.words(), w)
