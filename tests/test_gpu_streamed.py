@@ -99,5 +99,6 @@ def test_streamed_simulator_refuses_device_state_calls():
     assert rc == -5
     w = torch.empty((2048, s.layout().n_words), dtype=torch.int64, device="cuda")
     assert _lib.lib().aq_sim_get_words(st._sim, C.c_void_p(w.data_ptr()), _lib.stream_ptr()) == -5
+    s.substeps(0)  # an in-core simulator: the streamed entry points refuse it
     assert _lib.lib().aq_sim_stream_get_words(s._sim, C.c_void_p(w.data_ptr()), _lib.stream_ptr()) == -5
     st.close()
