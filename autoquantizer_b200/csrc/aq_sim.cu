@@ -83,23 +83,48 @@ __global__ void __launch_bounds__(SCATTER_T) k_scatter(const uint64_t* __restric
   const int64_t c0 = (int64_t)(key >> 6) * 64;
   const int myc = key & 63;
   // records before this one: min(count, rk) of every cell, plus one more
-  // for every earlier cell that has an rk-th record.  The block's 65
-  // offsets are read as int4 vectors (start is 256-byte aligned, c0 a
-  // multiple of 64).
-  const int4* st4 = reinterpret_cast<const int4*>(start + c0);
-  int4 v = __ldg(st4);
-  const int64_t b0 = v.x;
+  // for every earlier cell that has an rk-th record; with mask_r the cells
+  // holding more than r records, that is the sum of popc(mask_r) over
+  // r < rk plus popc(mask_rk) below cell myc.
+  int64_t b0;
   int t = 0;
-#pragma unroll 4
-  for (int q = 0; q < 16; ++q) {
-    const int4 nv = q < 15 ? __ldg(st4 + q + 1) : make_int4(__ldg(start + c0 + 64), 0, 0, 0);
-    const int ss[5] = {v.x, v.y, v.z, v.w, nv.x};
-#pragma unroll
-    for (int j = 0; j < 4; ++j) {
-      const int k = 4 * q + j, nk = ss[j + 1] - ss[j];
-      t += min(nk, rk) + ((k < myc && nk > rk) ? 1 : 0);
+  const unsigned am = __activemask();
+  const int64_t c0_first = __shfl_sync(am, c0, 0);
+  if (am == 0xffffffffu && __all_sync(am, c0 == c0_first)) {
+    // the whole warp in one block (the usual case: records come in the
+    // previous binning's block order): the warp builds mask_r rank by rank
+    // from two cells per lane, one ballot pair per rank
+    const int* sc = start + c0;
+    const int n_lo = __ldg(sc + lane + 1) - __ldg(sc + lane);
+    const int n_hi = __ldg(sc + lane + 33) - __ldg(sc + lane + 32);
+    b0 = __ldg(sc);
+    const int rmax = (int)__reduce_max_sync(am, (unsigned)rk);
+    const unsigned long long below = (1ull << myc) - 1ull;
+    int acc = 0;
+    for (int r = 0; r <= rmax; ++r) {
+      const unsigned long long m =
+          (unsigned long long)__ballot_sync(am, n_lo > r) | ((unsigned long long)__ballot_sync(am, n_hi > r) << 32);
+      if (r == rk) t = acc + __popcll(m & below);
+      acc += __popcll(m);
     }
-    v = nv;
+  } else {
+    // lanes of several blocks (or a partial warp): each lane alone.  The
+    // block's 65 offsets are read as int4 vectors (start is 256-byte
+    // aligned, c0 a multiple of 64).
+    const int4* st4 = reinterpret_cast<const int4*>(start + c0);
+    int4 v = __ldg(st4);
+    b0 = v.x;
+#pragma unroll 4
+    for (int q = 0; q < 16; ++q) {
+      const int4 nv = q < 15 ? __ldg(st4 + q + 1) : make_int4(__ldg(start + c0 + 64), 0, 0, 0);
+      const int ss[5] = {v.x, v.y, v.z, v.w, nv.x};
+#pragma unroll
+      for (int j = 0; j < 4; ++j) {
+        const int k = 4 * q + j, nk = ss[j + 1] - ss[j];
+        t += min(nk, rk) + ((k < myc && nk > rk) ? 1 : 0);
+      }
+      v = nv;
+    }
   }
   const int64_t dst = b0 + t;
   const uint64_t* g = win + i0 * W;  // the group's words (i0 is a multiple of 32)
