@@ -635,9 +635,16 @@ struct aq_sim {
   int64_t n_total = 0;
   uint64_t* h_words = nullptr;
   uint64_t* words_dl = nullptr;
+  // uploads alternate between two buffers (the slab's first record buffer
+  // and words_up2), so an upload never waits for the binning of the chunk
+  // before; the slab's second record buffer takes the binned chunk
+  uint64_t* words_up[2] = {nullptr, nullptr};
+  uint64_t* words_binned = nullptr;
+  int up_par = 0;
+  cudaEvent_t ev_read[2] = {nullptr, nullptr};  // the binning that last read words_up[k]
   // uploads and downloads run on their own streams beside the kernels
   cudaStream_t up_st = nullptr, down_st = nullptr;
-  cudaEvent_t ev_start = nullptr, ev_up = nullptr, ev_sorted = nullptr, ev_ready = nullptr, ev_down = nullptr;
+  cudaEvent_t ev_start = nullptr, ev_up = nullptr, ev_ready = nullptr, ev_down = nullptr;
   std::vector<cudaEvent_t> ev_chunk_down;  // per chunk: its last download (its host words are final)
   int64_t step = 0;
   int last_grid = 0;  // grid[] holding the P2G sums of the latest substep
@@ -938,49 +945,52 @@ struct SimImpl final : SimBase {
 
   // One pass of k_step over every chunk: upload (particle order), bin (the
   // chunk's own items), step, put back in particle order, download (not
-  // after a P2G-only step, which changes no record).  The
-  // P2G target is cleared once for the pass; all chunks add into it and
-  // read the same complete G2P source.  Kernels run on st, uploads on
-  // up_st, downloads on down_st, over three buffers: chunk c + 1 goes up
-  // into the buffer chunk c's binning read, its binning writes the buffer
-  // chunk c stepped in (after chunk c was put back in order from it), and
-  // chunk c comes down from words_dl, which chunk c + 1's put-back waits
-  // for; so the uploads, the kernels and the downloads of neighbouring
-  // chunks overlap.
-  // chained: the previous pass of the same chain ran just before: the first
-  // upload waits only for its last binning and its own chunk's download
-  // (done by then unless there are fewer than three chunks), so it overlaps
-  // that pass's last step and download.  last: the chain ends
-  // with this pass, whose downloads st then waits for (within a chain only
-  // the next put-back waits for them).
+  // after a P2G-only step, which changes no record).  The P2G target is
+  // cleared once for the pass; all chunks add into it and read the same
+  // complete G2P source.  Kernels run on st, uploads on up_st, downloads on
+  // down_st, over four buffers: chunk c goes up into words_up[c's parity],
+  // free once the binning of chunk c - 2 read it; its binning writes
+  // words_binned, where it steps (after chunk c - 1 was put back in order
+  // from there); it is put back in order into words_dl once chunk c - 1 has
+  // come down from there.  So the uploads, the kernels and the downloads of
+  // neighbouring chunks overlap, and an upload waits for no kernel of the
+  // chunk before it.
+  // chained: the previous pass of the same chain ran just before: uploads
+  // wait only for the binnings that read their buffers and for their own
+  // chunks' downloads of that pass, so the first upload overlaps that
+  // pass's last kernels and download.  last: the chain ends with this pass,
+  // whose downloads st then waits for (within a chain only the next
+  // put-back waits for them).
   int stream_pass(int do_g2p, int do_p2g, void* gin, void* gout, cudaStream_t st, bool chained, bool last) {
     aq_sim* S_ = s;
     int rc;
     const int64_t nc = n_chunks();
-    const bool early = chained;
     if (do_p2g && (rc = clear_grid(gout, st))) return rc;
     AQ_CUDA_TRY(cudaEventRecord(S_->ev_start, st));
-    if (!early) AQ_CUDA_TRY(cudaStreamWaitEvent(S_->up_st, S_->ev_start, 0));
+    // not chained: every upload after whatever st did before this pass
+    if (!chained) AQ_CUDA_TRY(cudaStreamWaitEvent(S_->up_st, S_->ev_start, 0));
     AQ_CUDA_TRY(cudaStreamWaitEvent(S_->down_st, S_->ev_start, 0));
     for (int64_t c = 0; c < nc; ++c) {
-      const int up = 1 - S_->cur;  // the buffer the last binning read
+      const int par = S_->up_par;
+      S_->up_par ^= 1;
+      uint64_t* X = S_->words_up[par];
       const int64_t m = chunk_count(c), base = c * S_->chunk;
-      // the buffer: free once the last binning read it (chunk 0 of a pass
-      // that is not chained: ev_start); the host words: final once the
-      // chunk's own download of the previous pass is done
-      if (c > 0 || early) AQ_CUDA_TRY(cudaStreamWaitEvent(S_->up_st, S_->ev_sorted, 0));
-      AQ_CUDA_TRY(cudaStreamWaitEvent(S_->up_st, S_->ev_chunk_down[c], 0));
-      AQ_CUDA_TRY(cudaMemcpyAsync(S_->words[up], chunk_words(c), sizeof(uint64_t) * grouped_words(m, S_->W),
+      AQ_CUDA_TRY(cudaStreamWaitEvent(S_->up_st, S_->ev_read[par], 0));      // the buffer is free
+      AQ_CUDA_TRY(cudaStreamWaitEvent(S_->up_st, S_->ev_chunk_down[c], 0));  // the host words are final
+      AQ_CUDA_TRY(cudaMemcpyAsync(X, chunk_words(c), sizeof(uint64_t) * grouped_words(m, S_->W),
                                   cudaMemcpyHostToDevice, S_->up_st));
       AQ_CUDA_TRY(cudaEventRecord(S_->ev_up, S_->up_st));
-      k_iota<<<grid_for(m, 256), 256, 0, st>>>(S_->pid[up], m, base);
+      // bin from X (ids: the chunk's particles in order) into words_binned
+      S_->words[0] = X;
+      S_->words[1] = S_->words_binned;
+      S_->cur = 0;
+      k_iota<<<grid_for(m, 256), 256, 0, st>>>(S_->pid[0], m, base);
       AQ_CUDA_TRY(cudaGetLastError());
       S_->launches += 1;
       AQ_CUDA_TRY(cudaStreamWaitEvent(st, S_->ev_up, 0));
-      S_->cur = up;
       S_->n = m;
-      if ((rc = sort(st))) return rc;  // words[up] -> words[1 - up], cur = 1 - up
-      AQ_CUDA_TRY(cudaEventRecord(S_->ev_sorted, st));
+      if ((rc = sort(st))) return rc;  // words[0] -> words[1], cur = 1
+      AQ_CUDA_TRY(cudaEventRecord(S_->ev_read[par], st));
       if ((rc = launch_step(do_g2p, do_p2g, gin, gout, st, false))) return rc;
       if (!do_g2p) continue;  // a P2G-only pass leaves the records as they are: nothing to take down
       AQ_CUDA_TRY(cudaStreamWaitEvent(st, S_->ev_down, 0));  // words_dl may still be going down
@@ -1151,7 +1161,8 @@ static void free_sim(aq_sim* s) {
   if (s->slab) cudaFree(s->slab);
   if (s->h_words) cudaFreeHost(s->h_words);
   if (s->words_dl) cudaFree(s->words_dl);
-  for (cudaEvent_t ev : {s->ev_start, s->ev_up, s->ev_sorted, s->ev_ready, s->ev_down})
+  if (s->words_up[1]) cudaFree(s->words_up[1]);
+  for (cudaEvent_t ev : {s->ev_start, s->ev_up, s->ev_read[0], s->ev_read[1], s->ev_ready, s->ev_down})
     if (ev) cudaEventDestroy(ev);
   for (cudaEvent_t ev : s->ev_chunk_down)
     if (ev) cudaEventDestroy(ev);
@@ -1352,14 +1363,17 @@ int aq_sim_create_streamed(const aq_params* P, const aq_layout* L, int64_t chunk
     return AQ_E_NOMEM;
   }
   e = cudaMalloc((void**)&s->words_dl, sizeof(uint64_t) * (size_t)(grouped_words(chunk, s->W) + 2));
+  if (e == cudaSuccess) e = cudaMalloc((void**)&s->words_up[1], sizeof(uint64_t) * (size_t)(grouped_words(chunk, s->W) + 2));
   if (e != cudaSuccess) {
     set_last_cuda_error(e, "cudaMalloc");
     free_sim(s);
     return AQ_E_NOMEM;
   }
+  s->words_up[0] = s->words[0];
+  s->words_binned = s->words[1];
   e = cudaStreamCreateWithFlags(&s->up_st, cudaStreamNonBlocking);
   if (e == cudaSuccess) e = cudaStreamCreateWithFlags(&s->down_st, cudaStreamNonBlocking);
-  for (cudaEvent_t* ev : {&s->ev_start, &s->ev_up, &s->ev_sorted, &s->ev_ready, &s->ev_down})
+  for (cudaEvent_t* ev : {&s->ev_start, &s->ev_up, &s->ev_read[0], &s->ev_read[1], &s->ev_ready, &s->ev_down})
     if (e == cudaSuccess) e = cudaEventCreateWithFlags(ev, cudaEventDisableTiming);
   s->ev_chunk_down.assign((size_t)nc, nullptr);
   for (int64_t c = 0; c < nc && e == cudaSuccess; ++c)

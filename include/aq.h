@@ -219,7 +219,7 @@ int aq_sim_count(const aq_sim* sim, int64_t* h_n, int64_t* h_capacity);
  * aq_sim_loss) moves them through the device in chunks of at most `chunk`
  * records (upload, binning of the chunk, the substep kernel, download); the
  * grids stay on the device and collect every chunk.  For scenes whose
- * records do not fit in device memory: device memory then holds three
+ * records do not fit in device memory: device memory then holds four
  * chunk buffers and the grids, and the host link bounds the speed, in
  * proportion to the record bytes (the host keeps each chunk in particle
  * order, so no particle ids cross the link).  Dense grids only (sparse = 0).  Records enter and
