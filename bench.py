@@ -508,7 +508,9 @@ def streamed_run(q, cfg32, vals, n, steps, parts, ws, cfg_cr=None):
         v, ms_ = job_rate(n * steps, e0.elapsed_time(e1), ws)
         rb = sol.bytes_per_particle()
         out[name] = {"value": v, "unit": UNIT, "ms_per_step": ms_ / steps, "record_bytes": rb,
-                     "host_bytes_per_substep": 2 * rb * n, "status_flags": st.status()[0]}
+                     "host_bytes_per_substep": 2 * rb * n,
+                     "host_link_gbs": 2 * rb * n / (ms_ / steps * 1e-3) / 1e9,  # both directions together
+                     "status_flags": st.status()[0]}
         st.close()
     del f
     out["quantized_speedup"] = out["quantized"]["value"] / out["fp32_state"]["value"]
