@@ -372,3 +372,28 @@ def test_fluid_3d_scaling_solve_reads_the_fixed_range_file(tmp_path):
     out = D.solve(exp, c, str(tmp_path), D.CR, 0.5)
     case = [k for k in SCIPY_GOLD["cases"] if k["key"] == FS and k["form"] == "mem" and k["eps"] == 0.5][0]
     assert out["bits"] == case["bits"]
+
+
+@pytest.mark.parametrize("task,cid", [(0, 0), (1, 0), (1, 1), (1, 2), (1, 3), (1, 4), (1, 5), (1, 6), (1, 7)])
+def test_fluid_3d_scaling_initial_conditions(tmp_path, task, cid):
+    """init() of run_mpm_fluid_3d_scaling.py:222-275 for the scaling task and
+    every initial-condition configuration: the blocks start at the walls lb
+    (configurations 5 and 6 start empty), inside the domain, with the
+    configuration's particle count (split in two for configuration 3)."""
+    from autoquantizer_b200.mpm_solver import MPMSolver
+
+    exp, c = _scaling_config(tmp_path, id=cid, task=task, n_particles=4000)
+    mpm = MPMSolver(c)
+    exp.init(mpm)
+    if cid in (5, 6) and task == 1:
+        assert mpm.current_idx == 0
+        return
+    assert mpm.current_idx == 4000
+    x = mpm._staging()[:4000, :3]
+    dx = 1.0 / c.n_grid
+    assert np.all(x >= (np.array(c.lb) + 0.5) * dx - 1e-12)
+    assert np.all(x < 1.0)
+    if cid == 1 and task == 1:  # the block starts at the middle of the walls in x
+        assert x[:, 0].min() >= (c.lb[0] + c.ub[0]) * 0.5 * dx - 1e-12
+    if cid == 3 and task == 1:  # two blocks, one against each z wall
+        assert (x[:, 2] < 0.5).sum() == 2000 and (x[:, 2] > 0.5).sum() == 2000
