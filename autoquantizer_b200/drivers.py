@@ -9,7 +9,8 @@ block.
 
 Flags follow the reference drivers (run_mpm_elastic_2d.py:18-50): -a
 gradients, -r ranges, -f solve + forward, -e epsilon, -m mode (0 compression
-rate, 1 error bound).  Additions: --root (folder holding grads/ and ranges/,
+rate, 1 error bound); with -f, --optimality TASK -b S1 -b2 S2 perturbs the
+solved widths as run_mpm_optimality_check.py does before the runs.  Additions: --root (folder holding grads/ and ranges/,
 default the working directory), -N (forward runs), --timesteps (shorter
 horizons), --json (one summary line).
 
@@ -28,6 +29,9 @@ Experiments:
   fluid_3d    run_mpm_fluid_3d.py — two fluid slabs stirred by the rotating
               SDF propeller collider (init_sdf_value; the autodiff path's
               collider schedule for -a and -r).
+  dithering_2d  run_mpm_dithering_exp.py — the 2D elastic material in four
+              cubes on a fixed scheme; -f runs it unquantized, quantized with
+              dithering and without.
   fluid_3d_scaling  run_mpm_fluid_3d_scaling.py — a fluid block (or, for
               configurations 5 and 6, two water jets) in a walled box, from
               one of the reference's JSON configurations (-c); scheme from
@@ -131,6 +135,79 @@ class Elastic2D(Experiment):
         else:
             bits, _ = LagrangianEB(grads=grads * ranges ** 2, ref=self.f64_data, tol_rel=eps)
         return bits + 1, ranges
+
+
+class Dithering2D(Elastic2D):
+    """run_mpm_dithering_exp.py: the 2D elastic material (E 50, 80,000
+    particles, 128^2, 8193 timesteps, f64) in four lattice cubes at
+    (0.125 + 0.2 i, 0.75), 0.15 x 0.15, a fixed scheme (widths 19, 19, 13,
+    13, 9, 10, 10, 9, 14, 14, 14, 15 on the elastic_2d experiment's ranges,
+    positions 1, the others doubled, :119-132); -f runs it unquantized (the
+    f64 reference), quantized with dithering and quantized without (the
+    driver's three modes, :98-113).  The driver sets config.dt = 5e-5 in
+    init_dithering (:79), after the solver has read its time step
+    (mpm_solver.py:44): its runs use dt 2e-4, and so do these."""
+
+    name = "dithering_2d"
+    file_name = "elastic_2d.npy"  # ranges/elastic_2d: the elastic_2d experiment's
+    modes = ()
+    BITS = [19, 19, 13, 13, 9, 10, 10, 9, 14, 14, 14, 15]
+
+    def config(self, kind="forward"):
+        c = super().config(kind)
+        c.id = "dithering"
+        c.quant_bits = np.array(self.BITS)
+        return c
+
+    def init(self, mpm):
+        mpm.initialize()
+        n = mpm.param.n_particles // 4
+        for i in range(4):
+            mpm.add_cube((0.125 + i * 0.2, 0.75), (0.15, 0.15), n)
+
+
+def dithering_experiment(exp, cfg, root):
+    """The three runs of run_mpm_dithering_exp.py on the experiment's fixed
+    scheme and the elastic_2d ranges: the loss of each and the relative
+    error of the quantized ones against the unquantized run."""
+    import copy
+
+    ranges = np.array(np.load(os.path.join(root, "ranges", "elastic_2d", exp.file_name)), dtype=np.float64)
+    ranges[:2] = 1.0
+    ranges[2:] *= 2.0
+    cfg.quant_ranges = ranges
+    out = {"bits": list(exp.BITS), "ranges": ranges.tolist()}
+    ref = float(run(exp, copy.deepcopy(cfg), 1, quant=False)[0])
+    out["loss_f64"] = ref
+    for name, dith in (("dithering", True), ("no_dithering", False)):
+        c = copy.deepcopy(cfg)
+        c.use_dithering = dith
+        loss = float(run(exp, c, 1, quant=True)[0])
+        out["loss_" + name] = loss
+        out["rel_err_" + name] = abs(loss - ref) / abs(ref)
+    return out
+
+
+def perturb_bits(bits, dim, task, s1, s2=None, rng=None):
+    """The widths of run_mpm_optimality_check.py's checks (:196-232) from
+    solved ones: task 0 takes s1 bits off every field, task 1 off half of
+    the fields chosen at random, task 2 moves s1 bits from each position
+    component to the velocity's and s2 from each entry of C to F's."""
+    b = np.array(bits, dtype=np.int64).copy()
+    n = len(b)
+    if task in (0, 1):
+        order = (rng or np.random.default_rng(0)).permutation(n)
+        for k in order[: n if task == 0 else n // 2]:
+            b[k] -= s1
+    elif task == 2:
+        s2 = s1 if s2 is None else s2
+        b[:dim] -= s1
+        b[dim:2 * dim] += s1
+        b[2 * dim:2 * dim + dim * dim] -= s2
+        b[2 * dim + dim * dim:2 * dim + 2 * dim * dim] += s2
+    else:
+        raise ValueError("optimality task %r is not 0, 1 or 2" % (task,))
+    return b
 
 
 class Fluid2D(Experiment):
@@ -548,7 +625,7 @@ class Fluid3DScaling(Experiment):
         return bits + 1, ranges
 
 
-EXPERIMENTS = {e.name: e for e in (Elastic2D, Fluid2D, FallingBlock3D, Letters3D, Propeller3D,
+EXPERIMENTS = {e.name: e for e in (Elastic2D, Dithering2D, Fluid2D, FallingBlock3D, Letters3D, Propeller3D,
                                     Fluid3DScaling)}
 
 
@@ -646,6 +723,12 @@ def main(argv=None):
     ap.add_argument("--inputs", default="inputs", help="folder of the 3D experiments' meshes and collider volumes")
     ap.add_argument("-c", "--config", default=None,
                     help="fluid_3d_scaling: one of the reference's JSON configurations (mpm_exps/configs/...)")
+    ap.add_argument("--optimality", type=int, default=None, metavar="TASK",
+                    help="with -f: perturb the solved widths as run_mpm_optimality_check.py does "
+                         "(0: -b bits off every field, 1: off half of them, 2: move -b bits x->v, -b2 bits C->F)")
+    ap.add_argument("-b", "--search-bits", type=int, default=1)
+    ap.add_argument("-b2", "--search-bits-2", type=int, default=1)
+    ap.add_argument("--seed", type=int, default=0, help="fields chosen by --optimality 1")
     ap.add_argument("--timesteps", type=int, default=None)
     ap.add_argument("--json", action="store_true")
     args = ap.parse_args(argv)
@@ -660,10 +743,19 @@ def main(argv=None):
         out = ad(exp, cfg, args.root)
     elif args.ranges:
         out = detect_range(exp, cfg, args.root)
+    elif args.forward and isinstance(exp, Dithering2D):
+        out = dithering_experiment(exp, cfg, args.root)
     elif args.forward:
         if args.mode not in exp.modes:
             ap.error("%s has no mode %d" % (exp.name, args.mode))
         out = solve(exp, cfg, args.root, args.mode, args.epsilon)
+        if args.optimality is not None:
+            b = perturb_bits(out["bits"], cfg.dim, args.optimality, args.search_bits, args.search_bits_2,
+                             np.random.default_rng(args.seed))
+            if np.any(b < 1) or np.any(b > 32):
+                ap.error("perturbed widths %s fall outside [1, 32]" % b.tolist())
+            cfg.quant_bits = b
+            out["bits_solved"], out["bits"] = out["bits"], b.tolist()
         loss = run(exp, cfg, args.runs)
         out.update({"loss_mean": float(loss.mean()), "loss_std": float(loss.std()),
                     "loss_max": float(loss.max()), "loss_min": float(loss.min()), "losses": loss.tolist()})

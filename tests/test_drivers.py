@@ -397,3 +397,40 @@ def test_fluid_3d_scaling_initial_conditions(tmp_path, task, cid):
         assert x[:, 0].min() >= (c.lb[0] + c.ub[0]) * 0.5 * dx - 1e-12
     if cid == 3 and task == 1:  # two blocks, one against each z wall
         assert (x[:, 2] < 0.5).sum() == 2000 and (x[:, 2] > 0.5).sum() == 2000
+
+
+def test_optimality_check_perturbations():
+    """run_mpm_optimality_check.py:196-232: task 0 takes S bits off every
+    field, task 1 off half of them (chosen at random), task 2 moves S1 bits
+    from x to v and S2 from C to F (totals kept)."""
+    bits = np.array([22, 22, 16, 16, 9, 11, 11, 9, 18, 17, 17, 18])
+    b0 = D.perturb_bits(bits, 2, 0, 2)
+    assert (bits - b0).tolist() == [2] * 12
+    b1 = D.perturb_bits(bits, 2, 1, 3, rng=np.random.default_rng(5))
+    d = bits - b1
+    assert sorted(d.tolist()) == [0] * 6 + [3] * 6
+    assert not np.array_equal(d, bits - D.perturb_bits(bits, 2, 1, 3, rng=np.random.default_rng(6)))
+    b2 = D.perturb_bits(bits, 2, 2, 2, 1)
+    assert (b2 - bits).tolist() == [-2, -2, 2, 2, -1, -1, -1, -1, 1, 1, 1, 1]
+    assert b2.sum() == bits.sum()
+    with pytest.raises(ValueError):
+        D.perturb_bits(bits, 2, 3, 1)
+
+
+def test_dithering_experiment_scene():
+    """run_mpm_dithering_exp.py's scene: four 0.15-wide lattice cubes at
+    (0.125 + 0.2 i, 0.75) of n/4 particles each, on its fixed scheme."""
+    from autoquantizer_b200.mpm_solver import MPMSolver
+
+    exp = D.Dithering2D()
+    c = exp.config()
+    assert c.quant_bits.tolist() == D.Dithering2D.BITS and c.dt == 2e-4 and c.precision == "f64"
+    c.n_particles = 4 * 400
+    mpm = MPMSolver(c)
+    exp.init(mpm)
+    assert mpm.current_idx == 1600
+    x = mpm._staging()[:1600, :2]
+    for i in range(4):
+        blk = x[400 * i:400 * (i + 1)]
+        assert blk[:, 0].min() >= 0.125 + 0.2 * i - 1e-12 and blk[:, 0].max() < 0.125 + 0.2 * i + 0.15
+        assert blk[:, 1].min() >= 0.75 - 1e-12 and blk[:, 1].max() < 0.9

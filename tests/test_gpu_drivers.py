@@ -208,3 +208,21 @@ def test_fluid_3d_scaling_jets_fill_the_box(tmp_path):
     assert mpm.status()[0] == 0
     x = mpm.state_values()[: mpm.current_idx, :3]
     assert np.all((x > 0) & (x < 1))
+
+
+def test_dithering_experiment_runs_all_three_modes(tmp_path):
+    """run_mpm_dithering_exp.py's three runs on its fixed scheme (the
+    elastic_2d ranges from the shipped file), over 512 substeps: the
+    unquantized f64 run, quantized with and without dithering; both
+    quantized losses stay within 1 % of the unquantized one."""
+    os.makedirs(tmp_path / "ranges" / "elastic_2d")
+    np.save(tmp_path / "ranges" / "elastic_2d" / "elastic_2d.npy",
+            np.array(GOLD["ranges"]["elastic_2d/elastic_2d.npy"]))
+    exp = D.Dithering2D()
+    cfg = exp.config()
+    cfg.n_timesteps = 513
+    out = D.dithering_experiment(exp, cfg, str(tmp_path))
+    print("dithering experiment:", out["loss_f64"], out["rel_err_dithering"], out["rel_err_no_dithering"])
+    assert out["loss_f64"] > 0
+    assert out["rel_err_dithering"] < 1e-2 and out["rel_err_no_dithering"] < 1e-2
+    assert out["loss_dithering"] != out["loss_no_dithering"]
