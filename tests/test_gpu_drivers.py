@@ -213,8 +213,11 @@ def test_fluid_3d_scaling_jets_fill_the_box(tmp_path):
 def test_dithering_experiment_runs_all_three_modes(tmp_path):
     """run_mpm_dithering_exp.py's three runs on its fixed scheme (the
     elastic_2d ranges from the shipped file), over 512 substeps: the
-    unquantized f64 run, quantized with and without dithering; both
-    quantized losses stay within 1 % of the unquantized one."""
+    unquantized f64 run, quantized with and without dithering.  With
+    dithering the loss stays within 1 % of the unquantized one (measured:
+    2.3e-4); without it, rounding every velocity update the same way
+    (gravity adds about one velocity step per substep) biases the motion,
+    and the loss is off by far more (measured: 162 %)."""
     os.makedirs(tmp_path / "ranges" / "elastic_2d")
     np.save(tmp_path / "ranges" / "elastic_2d" / "elastic_2d.npy",
             np.array(GOLD["ranges"]["elastic_2d/elastic_2d.npy"]))
@@ -224,5 +227,5 @@ def test_dithering_experiment_runs_all_three_modes(tmp_path):
     out = D.dithering_experiment(exp, cfg, str(tmp_path))
     print("dithering experiment:", out["loss_f64"], out["rel_err_dithering"], out["rel_err_no_dithering"])
     assert out["loss_f64"] > 0
-    assert out["rel_err_dithering"] < 1e-2 and out["rel_err_no_dithering"] < 1e-2
-    assert out["loss_dithering"] != out["loss_no_dithering"]
+    assert out["rel_err_dithering"] < 1e-2
+    assert out["rel_err_no_dithering"] > 10 * out["rel_err_dithering"]
