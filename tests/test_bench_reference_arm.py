@@ -21,3 +21,5 @@ def test_reference_arm_prints_one_line():
     assert d["cpu_baseline"]["value"] == d["value"] and d["cpu_baseline"]["cores"] >= 1
     assert d["e2e"]["value"] == d["value"] and d["e2e"]["h2d_bytes_per_step"] == 0
     assert d["config"]["workload"].startswith("mixed_boxes_3d")
+    # four substeps of the whole scene fit the default budget: the arm times the whole scene
+    assert d["config"]["same_config"] is True and d["config"]["sample"].startswith("the whole scene")
