@@ -132,3 +132,28 @@ def test_every_entry_point_is_mapped_to_a_reference_interface():
     missing = [f for f in declared if f not in exact and not any(f.startswith(p) for p in families)]
     assert not missing, missing
     assert not exact - set(declared), exact - set(declared)
+
+
+def test_new_entry_points_reject_bad_arguments_before_any_cuda_call():
+    """The streamed-mode and append entry points validate their arguments
+    first: null handles and pointers, a chunk below one record, a sparse
+    grid for a streamed simulator and an empty scene give AQ_E_ARG."""
+    L = _lib.lib()
+    P = _lib.Params()
+    P.dim, P.res[0], P.res[1], P.res[2], P.n_particles = 3, 32, 32, 32, 1000
+    P.dx, P.dt = 1.0 / 32, 1e-4
+    lay = _lib.Layout()
+    sim = C.c_void_p()
+    assert L.aq_sim_create_streamed(None, C.byref(lay), 100, C.byref(sim)) == -1
+    assert L.aq_sim_create_streamed(C.byref(P), C.byref(lay), 0, C.byref(sim)) == -1
+    P.sparse = 1
+    assert L.aq_sim_create_streamed(C.byref(P), C.byref(lay), 100, C.byref(sim)) == -1
+    P.sparse, P.n_particles = 0, 0
+    assert L.aq_sim_create_streamed(C.byref(P), C.byref(lay), 100, C.byref(sim)) == -1
+    n, cap = C.c_int64(), C.c_int64()
+    assert L.aq_sim_append(None, None, 0, 10, None) == -1
+    assert L.aq_sim_set_count(None, 5) == -1
+    assert L.aq_sim_count(None, C.byref(n), C.byref(cap)) == -1
+    assert L.aq_sim_stream_set_words(None, None, None) == -1
+    assert L.aq_sim_stream_get_words(None, None, None) == -1
+    assert L.aq_sim_stream_chunks(None, C.byref(n), C.byref(cap)) == -1
