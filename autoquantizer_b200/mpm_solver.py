@@ -683,6 +683,7 @@ class MPMSolver:
         n = len(x)
         if n > self.n_particles:
             raise ValueError("load_states: %d particles exceed n_particles=%d" % (n, self.n_particles))
+        self._pull()  # a running simulator holds the current values (particles appended on the device too)
         vals = np.array(self._staging()[:n], copy=True)
         vals[:, slice(*self.slot_range("x"))] = x
         for name in ("v", "C", "F" if self.has_F else "J"):
